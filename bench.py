@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Particle-steps/s of milupHPC's right-hand side + integrator on one B200.
+
+A step is one integration step (RHS: bounding box, keys, radix sort, tree,
+centres of mass / multipoles, Barnes-Hut walk; plus the FP64 leapfrog update)
+over the workload's synthetic particles, which stay resident in HBM.  The
+default workload is the 16.7M-particle Plummer sphere (Hilbert keys, leapfrog
+dt = 0.01, eps = 0.01) run with the mixed-precision walk at the opening
+parameter that meets p99 relative force error <= 1e-3 against FP64 direct
+summation.  `--impl reference` times the reference algorithm (FP64,
+computeForces_v2 semantics, at the opening parameter that meets the same
+error bar) as restated by the CPU oracle on the host cores.
+
+Multi-GPU (torchrun, one process per GPU): replicas only — every rank runs
+an independent copy of the workload; time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # Plummer at scale, precision form: N = 2^24, Hilbert keys, leapfrog dt 0.01
+    "plummer16m": dict(kind="gravity", n=1 << 24, sfc=1, dt=0.01, eps2=1e-4, theta=0.5, theta_mixed=0.3,
+                       theta_plain_matched=0.1, seed=1),
+    # the reference's own single-rank case: N = 131072, Lebesgue, leapfrog dt 0.025
+    "plummer131k": dict(kind="gravity", n=131072, sfc=0, dt=0.025, eps2=1e-4, theta=0.5, theta_mixed=0.3,
+                        theta_plain_matched=0.1, seed=1),
+}
+
+FLOP_MONO = 19   # flop per accepted particle-node monopole interaction
+FLOP_QUAD = 34   # extra flop of the quadrupole term of an accepted cell
+
+
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active," \
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown," \
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [a.strip() for a in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fp32_peak_tflops(torch):
+    """Measured FP32 FMA throughput of this GPU (CUDA cores): libmhpc's own
+    dependent-FMA kernel, best of 3, used as the gravity walk's roofline."""
+    from miluphpc_b200 import _lib
+    import ctypes
+    L = _lib.load()
+    best = 0.0
+    for _ in range(3):
+        t = ctypes.c_double(0)
+        _lib.check(L.mhpc_fp32_peak(ctypes.byref(t)), "fp32_peak")
+        best = max(best, t.value)
+    return best
+
+
+def plummer_state(wl, rank):
+    from miluphpc_b200 import ics
+    return ics.plummer(wl["n"], seed=wl["seed"] + 1000 * rank)
+
+
+def make_sim(wl, state, variant):
+    from miluphpc_b200 import _lib
+    from miluphpc_b200.miluphpc import Miluphpc
+    kw = dict(gravity=1, sph=0, integrator=2, time_step=wl["dt"], smoothing=wl["eps2"], sfc=wl["sfc"],
+              theta=wl["theta"], theta_mixed=wl["theta_mixed"])
+    if variant == "mixed":
+        kw["precision"] = 1
+    elif variant == "plain_matched":
+        kw["theta"] = wl["theta_plain_matched"]
+    cfg = _lib.default_config(**kw)
+    return Miluphpc(cfg, state)
+
+
+def force_error(sim, torch, eps2, ntarget=4096, seed=7):
+    from miluphpc_b200.miluphpc import direct_gravity
+    n = sim.n
+    rng = np.random.default_rng(seed)
+    tg = np.sort(rng.choice(n, min(ntarget, n), replace=False)).astype(np.int32)
+    tgt = torch.as_tensor(tg, device=sim.device)
+    dx, dy, dz = direct_gravity(sim.t["x"][:n], sim.t["y"][:n], sim.t["z"][:n], sim.t["mass"][:n], tgt, eps2)
+    g = [sim.t[k][:n][tgt.long()] for k in ("g_ax", "g_ay", "g_az")]
+    num = torch.sqrt((g[0] - dx) ** 2 + (g[1] - dy) ** 2 + (g[2] - dz) ** 2)
+    den = torch.sqrt(dx ** 2 + dy ** 2 + dz ** 2)
+    e = (num / den).cpu().numpy()
+    return {"p50": float(np.median(e)), "p99": float(np.percentile(e, 99)), "max": float(e.max()),
+            "targets": int(len(tg))}
+
+
+def run_ours(args, wl):
+    import torch
+    import torch.distributed as dist
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    state = plummer_state(wl, rank)
+    n = wl["n"]
+    sim = make_sim(wl, state, args.variant)
+    step = 0
+    for _ in range(args.warmup):
+        sim.integrate(step)
+        step += 1
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    grav_ms, inter, quad = [], 0.0, 0.0
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        sim.integrate(step)
+        st = sim.stats()
+        grav_ms.append(st["ms_stage"]["gravity"])
+        inter += st["gravity_interactions"]
+        quad += st["gravity_quad_interactions"]
+        step += 1
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = n * world * args.steps / (ms_max / 1e3)
+    last = sim.stats()
+    ferr = force_error(sim, torch, wl["eps2"])
+    # end to end through the public C ABI with host buffers (pinned)
+    e2e = run_e2e(args, wl, sim, state, torch, step)
+    out = None
+    if rank == 0:
+        flops = (inter * FLOP_MONO + quad * FLOP_QUAD) / args.steps
+        gms = float(np.mean(grav_ms))
+        achieved = flops / (gms / 1e3) / 1e12
+        peak = fp32_peak_tflops(torch)
+        traffic = load_traffic(args.workload, args.variant)
+        roof = {"kernel": "k_grav_mixed" if args.variant == "mixed" else "k_grav_v2", "bound": "fp32",
+                "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
+                "frac": round(achieved / peak, 4) if peak > 0 else None, "traffic": traffic,
+                "peak_source": "measured on this GPU by mhpc_fp32_peak (dependent FFMA chains)",
+                "work_unit": "%d flop per accepted monopole interaction + %d per quadrupole term" % (FLOP_MONO, FLOP_QUAD),
+                "kernel_ms_per_launch": round(gms, 3), "interactions_per_launch": inter / args.steps}
+        cpu = cpu_baseline(wl, args) if not args.no_cpu_baseline else None
+        out = {
+            "metric": "particle-steps/s on 1 B200: mixed/learned vs plain at rel. force err <=1e-3",
+            "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.variant == "mixed" else "f64",
+            "data": "synthetic (seeded Plummer sampler, no dataset)",
+            "config": {"workload": args.workload, "n_particles": n, "variant": args.variant,
+                       "theta": wl["theta_mixed"] if args.variant == "mixed" else
+                       (wl["theta_plain_matched"] if args.variant == "plain_matched" else wl["theta"]),
+                       "sfc": "hilbert" if wl["sfc"] else "lebesgue", "integrator": "leapfrog", "dt": wl["dt"],
+                       "eps2": wl["eps2"], "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (positions alone %.0f MB)" % (n * 24 / 1e6)},
+            "force_error": ferr,
+            "stages_ms_last_step": {k: round(v, 3) for k, v in last["ms_stage"].items()},
+            "tree_cells": last["cells"],
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": args.steps * launches_per_step(args.variant),
+            "clocks": clk,
+        }
+    sim.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def launches_per_step(variant):
+    # per RHS: bbox, bbox_finish, keys, hist, hist_scan, 8 onesweep, gather,
+    # lcp, count, 4 scan, copy_total, zero_cells, nodes, upward, walk
+    rhs = 2 + 1 + 2 + 8 + 1 + 2 + 4 + 3 + 1 + 1
+    if variant == "mixed":
+        rhs += 1  # mixed node conversion
+    return rhs + 2  # leapfrog updateX, updateV
+
+
+def run_e2e(args, wl, sim, state, torch, step0):
+    """Same steps through mhpc_integrate_host: host (pinned) state copied in
+    and the new state + accelerations copied out every step."""
+    import ctypes
+    from miluphpc_b200 import _lib
+    n = sim.n
+    fields_in = ["x", "y", "z", "mass", "vx", "vy", "vz", "g_ax", "g_ay", "g_az"]
+    host = {}
+    for f in fields_in:
+        host[f] = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        host[f].copy_(sim.t[f][:n].cpu())
+    hp = _lib.Particles()
+    hp.n = n
+    hp.num_nodes = n
+    for f in fields_in:
+        setattr(hp, f, ctypes.cast(ctypes.c_void_p(host[f].data_ptr()), _lib.P_d))
+    L = _lib.load()
+    dt = ctypes.c_double()
+    steps = max(2, min(args.steps, 5))
+    # one untimed call allocates the context's device mirror
+    _lib.check(L.mhpc_integrate_host(sim.ctx, ctypes.byref(hp), step0, ctypes.byref(dt)), "integrate_host")
+    t0 = time.perf_counter()
+    for k in range(steps):
+        _lib.check(L.mhpc_integrate_host(sim.ctx, ctypes.byref(hp), step0 + 1 + k, ctypes.byref(dt)),
+                   "integrate_host")
+    el = time.perf_counter() - t0
+    h2d = 10 * 8 * n
+    d2h = 9 * 8 * n
+    return {"value": n * steps / el, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "steps": steps}
+
+
+def load_traffic(workload, variant):
+    """DRAM bytes per launch of the walk from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        d = json.load(open(p))
+        return d.get("%s/%s" % (workload, variant))
+    except Exception:
+        return None
+
+
+def cpu_baseline(wl, args, sample_groups=None):
+    """The reference algorithm (FP64 v2 walk at the accuracy-matched theta,
+    with keys, sort, tree and COM) restated by the oracle, timed on the host
+    cores: full keys/sort/tree/COM on all particles, the walk on a sample of
+    warp groups, scaled to the full workload."""
+    from oracle import oracle as O
+    from miluphpc_b200 import ics
+    n = wl["n"]
+    P = ics.plummer(n, seed=wl["seed"])
+    theta = wl["theta_plain_matched"]
+    t0 = time.perf_counter()
+    bb = O.bbox(P["x"], P["y"], P["z"])
+    k = O.keys(P["x"], P["y"], P["z"], bb, wl["sfc"])
+    _, perm = O.sort(k)
+    t1 = time.perf_counter()
+    T = O.Tree(P["x"], P["y"], P["z"], P["mass"], bb)
+    t2 = time.perf_counter()
+    ngroups = (n + 31) // 32
+    stride = max(1, ngroups // (sample_groups or args.cpu_sample_groups))
+    O.gravity_v2_sample(T, perm, 0.5 * (bb[1] - bb[0]), theta, wl["eps2"], stride)
+    t3 = time.perf_counter()
+    walk_full = (t3 - t2) * stride
+    total = (t2 - t0) + walk_full
+    return {"value": n / total, "unit": "particle-steps/s", "cores": O.num_threads(), "kind": "port",
+            "sample": "keys+sort+tree+COM on all %d particles (%.1f s), v2 walk (theta %.2f) on every %d-th of "
+                      "%d warp groups (%.1f s) scaled x%d" % (n, t2 - t0, theta, stride, ngroups, t3 - t2, stride),
+            "seconds": t3 - t0}
+
+
+def run_reference(args, wl):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return None
+    per_step = []
+    cb = None
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        pass
+    for s in range(max(1, args.steps)):
+        cb = cpu_baseline(wl, args, sample_groups=args.cpu_sample_groups)
+        per_step.append(cb["value"])
+    value = float(np.median(per_step))
+    return {
+        "impl": "reference",
+        "metric": "particle-steps/s on 1 B200: mixed/learned vs plain at rel. force err <=1e-3",
+        "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded Plummer sampler, no dataset)",
+        "config": {"workload": args.workload, "n_particles": wl["n"], "variant": "reference v2 FP64 (oracle port)",
+                   "theta": wl["theta_plain_matched"], "sfc": "hilbert" if wl["sfc"] else "lebesgue"},
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cb["cores"], "kind": "port",
+                         "sample": cb["sample"]},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="plummer16m", choices=sorted(WORKLOADS))
+    ap.add_argument("--variant", default="mixed", choices=["mixed", "plain", "plain_matched"])
+    ap.add_argument("--cpu-sample-groups", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        out = run_reference(args, wl)
+    else:
+        out = run_ours(args, wl)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,263 @@
+/*
+ * mhpc.h — C ABI of the B200-native right-hand side of milupHPC.
+ *
+ * The library replaces the single-rank path of Miluphpc::rhs()
+ * (include/miluphpc.h:478, src/miluphpc.cpp:387-562 of milupHPC) and the
+ * integrator kernels that call it.  Every entry point takes plain pointers and
+ * sizes; device pointers are CUDA device addresses, `stream` is a
+ * cudaStream_t passed as void* (NULL = the legacy default stream).  All
+ * functions return an mhpc status code (MHPC_OK = 0) and never abort the
+ * process or trap the GPU.  Work is stream-ordered; functions that must read
+ * a device result on the host (status words, counters) synchronise `stream`
+ * and say so.
+ */
+#ifndef MHPC_H
+#define MHPC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+/* Replaces host exit(1) (src/miluphpc.cpp:974-981), device assert(0)
+ * (include/cuda_utils/cuda_utilities.cuh:41-73) and gpuErrorcheck aborts. */
+enum mhpc_status {
+    MHPC_OK = 0,
+    MHPC_ERR_ARG = 1,         /* null pointer, negative size, bad enum */
+    MHPC_ERR_CUDA = 2,        /* CUDA runtime error (launch, copy, alloc) */
+    MHPC_ERR_CAPACITY = 3,    /* n larger than the context's capacity */
+    MHPC_ERR_NODE_POOL = 4,   /* tree cells exceed the node pool */
+    MHPC_ERR_DEPTH = 5,       /* a traversal exceeded its depth / stack bound */
+    MHPC_ERR_NEIGHBOURS = 6,  /* a particle has more than max_num_interactions */
+    MHPC_ERR_NAN = 7,         /* non-finite position or non-positive density */
+    MHPC_ERR_CONFIG = 8,      /* .info / .cfg file missing or malformed */
+    MHPC_ERR_NO_DEVICE = 9,   /* no CUDA device */
+    MHPC_ERR_TIMEOUT = 10,    /* a bounded device-side wait ran out */
+    MHPC_ERR_UNSUPPORTED = 11 /* option not implemented in this build */
+};
+
+const char* mhpc_status_string(int status);
+int mhpc_version(void);
+
+/* ------------------------------------------------------------ parameters */
+/* Run-time form of SimulationParameters (include/parameter.h:122-159) plus
+ * the compile-time physics switches of include/parameter.h:25-108, which are
+ * run-time flags here. */
+typedef struct mhpc_config {
+    /* .info keys (src/main.cpp:165-237) */
+    int integrator;            /* 0 explicit Euler, 1 predictor-corrector Euler, 2 leapfrog */
+    double time_step;
+    double max_time_step;
+    double time_end;
+    int sfc;                   /* 0 Lebesgue, 1 Hilbert */
+    double theta;              /* Barnes-Hut opening parameter (squared-ratio form of v2) */
+    double smoothing;          /* gravitational softening eps^2, added to r^2 */
+    int smoothing_kernel;      /* 0 spiky, 1 cubic spline, 2 wendlandc2, 3 wendlandc4, 4 wendlandc6 */
+    int gravity_force_version; /* 0 warp-voted walk (computeForces_v2), 2 per-particle (computeForces_v1) */
+    int sph_frnn_version;      /* 0 (fixedRadiusNN) */
+    int calculate_energy;
+    int calculate_angular_momentum;
+    int calculate_center_of_mass;
+    int remove_particles;
+    int remove_particles_criterion;
+    double remove_particles_dimension;
+    /* parameter.h switches */
+    int gravity;               /* GRAVITY_SIM */
+    int sph;                   /* SPH_SIM */
+    int integrate_energy;      /* INTEGRATE_ENERGY */
+    int integrate_density;     /* INTEGRATE_DENSITY */
+    int integrate_sml;         /* INTEGRATE_SML */
+    int variable_sml;          /* VARIABLE_SML */
+    int si_units;              /* SI_UNITS (G = 6.67430e-11 when set) */
+    int max_num_interactions;  /* MAX_NUM_INTERACTIONS (180) */
+    int nb_tolerance;          /* TOLERANCE_WANTED_NUMBER_OF_INTERACTIONS (5) */
+    int max_sml_iterations;    /* MAX_VARIABLE_SML_ITERATIONS (5) */
+    /* additions of this library */
+    int precision;             /* 0 plain FP64 (reference semantics), 1 mixed FP32 split + quadrupoles */
+    double theta_mixed;        /* opening parameter of the mixed walk (same squared-ratio meaning) */
+    int learned_h;             /* 1: MLP smoothing-length predictor with plain fallback */
+    int softening_mode;        /* 0 global eps^2, 1 eps_i = softening_h_factor * h_i (plus eps^2) */
+    double softening_h_factor;
+    double node_pool_factor;   /* tree cell pool = node_pool_factor * capacity + 20000 */
+} mhpc_config;
+
+/* Material (include/materials/material.cuh:123-150), one entry of the
+ * materials list of a .cfg file. */
+typedef struct mhpc_material {
+    int id;
+    int interactions;          /* variable-h target neighbour count */
+    double sml;                /* initial smoothing length = kernel support radius */
+    double alpha, beta;        /* artificial_viscosity */
+    int eos_type;              /* 0 polytropic, 1 Murnaghan, 3 isothermal, 9 ideal gas, 12 locally isothermal */
+    double polytropic_K, polytropic_gamma, rho_0, bulk_modulus, n, shear_modulus;
+} mhpc_material;
+
+void mhpc_config_default(mhpc_config* cfg);
+/* ConfigParser + src/main.cpp:165-237: read a .info (Boost property-tree
+ * INFO syntax: `key value`, `;` comments, `{}` blocks ignored) file. */
+int mhpc_config_from_info(const char* path, mhpc_config* cfg);
+/* MaterialHandler(const char*) (src/materials/material_handler.cpp:58-150):
+ * read a libconfig `materials = ( {...}, ... );` file.  Writes at most `cap`
+ * entries indexed by ID and the number found to *count. */
+int mhpc_materials_from_cfg(const char* path, mhpc_material* out, int cap, int* count);
+
+/* ------------------------------------------------------------- particles */
+/* Mirror of the Particles SoA (include/particles.cuh; allocation
+ * src/particle_handler.cpp:8-60,148-170).  Device pointers, FP64 state.
+ * x, y, z, mass have num_nodes entries; when num_nodes >= n + cells the
+ * cells' centres of mass are written after the particles, as in the
+ * reference.  Pointers marked optional may be NULL. */
+typedef struct mhpc_particles {
+    int n;                     /* numParticlesLocal */
+    int num_nodes;             /* length of x, y, z, mass (>= n) */
+    double *x, *y, *z, *mass;
+    double *vx, *vy, *vz;
+    double *ax, *ay, *az;              /* SPH acceleration */
+    double *g_ax, *g_ay, *g_az;        /* gravitational acceleration */
+    double *g_ax_old, *g_ay_old, *g_az_old; /* leapfrog only */
+    double *sml, *rho, *p, *cs, *e;
+    double *drhodt, *dedt, *dsmldt;
+    int *noi;                  /* optional: neighbour counts */
+    int *nnl;                  /* optional: n * max_num_interactions neighbour list (original indices) */
+    int *material_id;          /* optional: NULL = material 0 for all */
+    int *level;                /* optional: num_nodes tree levels */
+} mhpc_particles;
+
+/* ------------------------------------------------ stateless building blocks */
+/* TreeNS::Kernel::computeBoundingBox (src/subdomain_key_tree/tree.cu:302-437)
+ * after Kernel::resetArrays (src/device_rhs.cu:24-33): cubic box that always
+ * contains the origin.  bbox_dev receives 6 doubles {minX,maxX,minY,maxY,
+ * minZ,maxZ} in device memory. */
+int mhpc_bbox(const double* x, const double* y, const double* z, int n, double* bbox_dev,
+              void* stream);
+/* SubDomainKeyTreeNS::Kernel::getParticleKeys (src/subdomain_key_tree/
+ * subdomain.cu:849-894) / Tree::getParticleKey (tree.cu:157-240): 21-level
+ * Lebesgue (curve 0) or Hilbert (curve 1) keys from a device bbox. */
+int mhpc_keys(const double* x, const double* y, const double* z, int n, const double* bbox_dev,
+              int curve, uint64_t* keys, void* stream);
+/* HelperNS::sortArray (src/helper.cu:150-166) with TreeNS::prepareSorting
+ * (tree.cu:1404-1413): stable ascending sort of 64-bit keys with int values
+ * (vals_in NULL = 0..n-1).  Scratch is caller-provided device memory of
+ * mhpc_sort_scratch_bytes(n) bytes; the inputs are not modified. */
+size_t mhpc_sort_scratch_bytes(int n);
+int mhpc_sort_pairs(const uint64_t* keys_in, const int* vals_in, uint64_t* keys_out,
+                    int* vals_out, int n, void* scratch, size_t scratch_bytes, void* stream);
+
+/* ------------------------------------------------------------ the context */
+typedef struct mhpc_ctx mhpc_ctx;
+
+/* Allocates every workspace buffer for up to `capacity` particles once
+ * (replaces the handlers' cudaMalloc, src/particle_handler.cpp:148+ and
+ * src/subdomain_key_tree/tree_handler.cpp:6-36); no call below allocates. */
+int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg,
+                    const mhpc_material* materials, int num_materials);
+int mhpc_ctx_destroy(mhpc_ctx* ctx);
+int mhpc_ctx_set_stream(mhpc_ctx* ctx, void* stream);
+int mhpc_ctx_set_config(mhpc_ctx* ctx, const mhpc_config* cfg);
+
+/* Miluphpc::rhs(step, selfGravity, assignParticlesToProcess)
+ * (include/miluphpc.h:478, src/miluphpc.cpp:387-562) on one GPU: bbox, keys,
+ * sort, tree, centres of mass, gravity (if cfg->gravity && self_gravity),
+ * SPH neighbour search, density, sound speed, pressure and internal forces
+ * (if cfg->sph).  Results land in the SoA.  Synchronises the stream once at
+ * the end to read the device status word; *ms_out (optional) receives the
+ * device time of the call. */
+int mhpc_rhs(mhpc_ctx* ctx, const mhpc_particles* p, int step, int self_gravity, float* ms_out);
+/* Same without the final synchronisation: the status is read by
+ * mhpc_ctx_status().  Capturable into a CUDA graph. */
+int mhpc_rhs_async(mhpc_ctx* ctx, const mhpc_particles* p, int step, int self_gravity);
+int mhpc_ctx_status(mhpc_ctx* ctx);
+
+/* One integrator step (src/integrator/leapfrog.cpp:21-117,
+ * explicit_euler.cpp:17-99, predictor_corrector_euler.cpp:47-151) with the
+ * integrator of cfg: calls the RHS and the FP64 update kernels.  step 0 runs
+ * the extra initial RHS of the leapfrog.  dt_out (optional) receives the
+ * step size used. */
+int mhpc_integrate(mhpc_ctx* ctx, const mhpc_particles* p, int step, double* dt_out);
+/* The same step with HOST (pinned or pageable) state arrays: copies the state
+ * in, runs the step, copies the state and accelerations out.  Uses the
+ * context's device mirror (allocated on first use). */
+int mhpc_integrate_host(mhpc_ctx* ctx, mhpc_particles* host, int step, double* dt_out);
+
+/* Sub-stages (the reference's Launch:: wrappers), stream-ordered, no sync. */
+int mhpc_stage_tree(mhpc_ctx* ctx, const mhpc_particles* p);    /* bbox+keys+sort+tree+COM */
+int mhpc_stage_gravity(mhpc_ctx* ctx, const mhpc_particles* p); /* needs stage_tree */
+int mhpc_stage_sph(mhpc_ctx* ctx, const mhpc_particles* p);     /* needs stage_tree */
+
+/* Parity exports (synchronise the stream). */
+/* Sorted keys and the permutation tree->sorted (device pointers, n entries). */
+int mhpc_export_sorted(mhpc_ctx* ctx, uint64_t* keys_dev, int* perm_dev);
+/* Tree in the reference layout: child[8*num_nodes] (host), cells numbered
+ * from n in pre-order, root children in child[0..7], leaves = original
+ * particle indices; level[num_nodes] (host, optional); node COMs into the
+ * host arrays x,y,z,m (num_nodes each, optional).  Returns the cell count in
+ * *cells. */
+int mhpc_export_tree(mhpc_ctx* ctx, int num_nodes, int* child, int* level, double* x, double* y,
+                     double* z, double* m, int* cells);
+
+/* Statistics of the last RHS (synchronises the stream). */
+typedef struct mhpc_stats {
+    int n;
+    int cells;                 /* tree cells */
+    int max_level;
+    int key_collisions;        /* particles sharing a full 63-bit key with another */
+    double bbox[6];
+    double radius;
+    double gravity_interactions; /* accepted particle-node interactions (walk) */
+    double gravity_nodes_visited;
+    double gravity_quad_interactions; /* accepted cells evaluated with a quadrupole term (mixed walk) */
+    int max_noi;               /* largest neighbour count */
+    double mean_noi;
+    int sml_sweeps;            /* variable-h sweeps run */
+    int sml_out_of_band;       /* particles whose final count misses the band */
+    int predictor_used;        /* particles whose learned h was accepted */
+    int predictor_fallback;    /* particles that fell back to the plain iteration */
+    float ms_stage[12];        /* bbox_keys, sort, tree, com, gravity, frnn, sml, density, forces, integrate, mlp, other */
+} mhpc_stats;
+int mhpc_get_stats(mhpc_ctx* ctx, mhpc_stats* out);
+
+/* FP64 diagnostics (src/miluphpc.cpp:577-677, Physics::Kernel
+ * src/subdomain_key_tree/subdomain.cu:2423-2644): out[0] kinetic energy,
+ * out[1] internal energy sum m e, out[2..4] linear momentum, out[5..7]
+ * angular momentum, out[8..10] centre of mass.  Synchronises. */
+int mhpc_diagnostics(mhpc_ctx* ctx, const mhpc_particles* p, double* out11);
+
+/* FP64 direct summation for verification: accelerations of `nt` target
+ * particles (original indices, device) from all n particles with softening
+ * eps2; outputs are device arrays of nt doubles. */
+int mhpc_direct_gravity(const double* x, const double* y, const double* z, const double* m, int n,
+                        const int* targets, int nt, double eps2, double* gax, double* gay,
+                        double* gaz, void* stream);
+
+/* Measured FP32 FMA throughput of the current device in TFLOP/s (dependent
+ * FFMA chains on every SM; the roofline denominator of the FP32 walk).
+ * Allocates and frees a small buffer; synchronises. */
+int mhpc_fp32_peak(double* tflops);
+
+/* ------------------------------------------------ learned smoothing length */
+/* MLP 12 -> 64 -> 64 -> 1 (SiLU), BF16 weights, FP32 accumulation, trained
+ * on the GPU by the library's own tensor-core kernels.  Not in the
+ * reference. */
+int mhpc_mlp_reset(mhpc_ctx* ctx, uint64_t seed);
+/* Adds the (features, converged h) pairs of the last plain variable-h
+ * iteration to the training buffer and runs `iters` Adam steps; *loss_out
+ * (optional) receives the last mini-batch loss.  Synchronises. */
+int mhpc_mlp_train(mhpc_ctx* ctx, int iters, float lr, float* loss_out);
+/* Forward pass on `rows` feature rows (device, rows x 12 float) into out
+ * (device, rows float), and the FP32 gradient of the mean-squared loss
+ * against target (device, rows float) w.r.t. all weights into grad (device,
+ * mhpc_mlp_num_params() floats) when grad is not NULL. */
+int mhpc_mlp_num_params(void);
+int mhpc_mlp_forward_backward(mhpc_ctx* ctx, const float* feats, int rows, const float* target,
+                              float* out, float* grad, float* loss_out);
+/* Copy the FP32 master weights out (host, mhpc_mlp_num_params() floats) or in. */
+int mhpc_mlp_get_params(mhpc_ctx* ctx, float* host_params);
+int mhpc_mlp_set_params(mhpc_ctx* ctx, const float* host_params);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MHPC_H */

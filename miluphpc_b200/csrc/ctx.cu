@@ -1,0 +1,671 @@
+// Context, orchestration and the C ABI of libmhpc.
+//
+// mhpc_rhs follows the single-rank sequence of Miluphpc::rhs()
+// (src/miluphpc.cpp:387-562): bounding box, keys, sort, tree, centres of mass,
+// gravity, SPH.  Differences by design: the work is stream-ordered with no
+// device synchronisation between stages (the reference synchronises after
+// every kernel, include/cuda_utils/cuda_launcher.cuh:114-141), the MPI
+// domain-list / LET kernels that do no work on one rank are not run, and all
+// workspace is allocated once in mhpc_ctx_create.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "gravity.cuh"
+#include "integrate.cuh"
+#include "mlp.cuh"
+#include "sph.cuh"
+#include "tree.cuh"
+
+enum Stage { EV_START, EV_KEYS, EV_SORT, EV_TREE, EV_COM, EV_GRAV, EV_SML, EV_FRNN, EV_DENS, EV_FORCES, EV_END, EV_COUNT };
+
+struct mhpc_ctx {
+    int cap = 0, cell_cap = 0, cap_nodes = 0, maxnb = 180;
+    int device = 0;
+    mhpc_config cfg;
+    mhpc_material mats[MHPC_MAX_MATERIALS];
+    int nmat = 1;
+    cudaStream_t stream = nullptr;
+    DevStatus* st = nullptr;
+    DevStatus* h_st = nullptr;
+    long long* ord = nullptr;
+    double* bbox = nullptr;
+    uint64_t* keys = nullptr;
+    uint64_t* skey = nullptr;
+    int* perm = nullptr;
+    void* sort_scratch = nullptr;
+    size_t sort_bytes = 0;
+    void* scan_scratch = nullptr;
+    double *sx = nullptr, *sy = nullptr, *sz = nullptr, *sm = nullptr, *sh = nullptr;
+    double *svx = nullptr, *svy = nullptr, *svz = nullptr, *se = nullptr, *srho = nullptr, *sp = nullptr,
+           *scs = nullptr;
+    int* smat = nullptr;
+    TreeDev T;
+    int* nbr = nullptr;
+    int* noi = nullptr;
+    double* hold = nullptr;
+    int *vh_done = nullptr, *vh_nit = nullptr, *vh_count = nullptr;
+    double* diag_part = nullptr;
+    double* diag_out = nullptr;
+    cudaEvent_t ev[EV_COUNT];
+    bool ev_recorded[EV_COUNT];
+    bool first_rhs_done = false;
+    int last_n = 0;
+    // device mirror for mhpc_integrate_host
+    mhpc_particles mirror;
+    bool mirror_ready = false;
+    std::vector<void*> allocs;
+    MlpState* mlp = nullptr;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(mhpc_ctx* c, T** p, size_t count) {
+    if (count == 0) count = 1;
+    void* q = nullptr;
+    if (cudaMalloc(&q, sizeof(T) * count) != cudaSuccess) return MHPC_ERR_CUDA;
+    c->allocs.push_back(q);
+    *p = (T*)q;
+    return MHPC_OK;
+}
+
+#define TRY(x)                 \
+    do {                       \
+        int _r = (x);          \
+        if (_r) return _r;     \
+    } while (0)
+
+MatDev to_dev(const mhpc_material& m, int si_units) {
+    MatDev d;
+    d.eos_type = m.eos_type;
+    d.interactions = m.interactions;
+    d.alpha = m.alpha;
+    d.beta = m.beta;
+    d.K = m.polytropic_K;
+    d.gamma = m.polytropic_gamma;
+    d.rho0 = m.rho_0;
+    d.bulk = m.bulk_modulus;
+    d.n_exp = m.n;
+    d.shear = m.shear_modulus;
+    // initializeSoundSpeed (src/sph/soundspeed.cu:4-36)
+    d.cs_init = 0.0;
+    if (m.eos_type == 1 && m.rho_0 > 0) d.cs_init = std::sqrt(m.bulk_modulus / m.rho_0);
+    if (m.eos_type == 3) d.cs_init = si_units ? 203.0 : 203.0 / 2.998e8;
+    return d;
+}
+
+SphParams sph_params(const mhpc_ctx* c, int n) {
+    SphParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.n = n;
+    P.maxnb = c->maxnb;
+    P.kernel = c->cfg.smoothing_kernel;
+    P.avg_h = (c->cfg.variable_sml || c->cfg.integrate_sml) ? 1 : 0;
+    P.integrate_energy = c->cfg.integrate_energy;
+    P.integrate_sml = c->cfg.integrate_sml;
+    P.integrate_density = c->cfg.integrate_density;
+    P.num_materials = c->nmat;
+    P.mixed = c->cfg.precision == 1;
+    for (int i = 0; i < c->nmat && i < MHPC_MAX_MATERIALS; ++i) P.mat[i] = to_dev(c->mats[i], c->cfg.si_units);
+    return P;
+}
+
+void record(mhpc_ctx* c, int e) {
+    cudaEventRecord(c->ev[e], c->stream);
+    c->ev_recorded[e] = true;
+}
+
+int check_particles(const mhpc_ctx* c, const mhpc_particles* p) {
+    if (!p) return MHPC_ERR_ARG;
+    if (p->n < 0) return MHPC_ERR_ARG;
+    if (p->n > c->cap) return MHPC_ERR_CAPACITY;
+    if (p->n == 0) return MHPC_OK;
+    if (!p->x || !p->y || !p->z || !p->mass) return MHPC_ERR_ARG;
+    if (c->cfg.gravity && (!p->g_ax || !p->g_ay || !p->g_az)) return MHPC_ERR_ARG;
+    if (c->cfg.sph && (!p->sml || !p->rho || !p->p || !p->cs || !p->ax || !p->ay || !p->az || !p->vx || !p->vy ||
+                       !p->vz || !p->e))
+        return MHPC_ERR_ARG;
+    return MHPC_OK;
+}
+
+int stage_tree(mhpc_ctx* c, const mhpc_particles* p) {
+    const int n = p->n;
+    cudaStream_t s = c->stream;
+    TRY(launch_bbox(p->x, p->y, p->z, n, c->ord, c->st, s));
+    TRY(launch_bbox_finish(c->ord, c->bbox, s));
+    TRY(launch_keys(p->x, p->y, p->z, n, c->ord, c->cfg.sfc, c->keys, nullptr, s));
+    record(c, EV_KEYS);
+    TRY(sort_pairs_u64(c->keys, nullptr, c->skey, c->perm, n, c->sort_scratch, c->sort_bytes, c->st, s));
+    record(c, EV_SORT);
+    GatherList L;
+    std::memset(&L, 0, sizeof(L));
+    const double* src[] = {p->x, p->y, p->z, p->mass};
+    double* dst[] = {c->sx, c->sy, c->sz, c->sm};
+    for (int a = 0; a < 4; ++a) { L.src[a] = src[a]; L.dst[a] = dst[a]; }
+    L.count = 4;
+    if (c->cfg.sph || (c->cfg.gravity && c->cfg.softening_h_factor > 0.0 && p->sml)) {
+        L.src[L.count] = p->sml; L.dst[L.count++] = c->sh;
+    }
+    if (c->cfg.sph) {
+        const double* s2[] = {p->vx, p->vy, p->vz, p->e, p->rho, p->p, p->cs};
+        double* d2[] = {c->svx, c->svy, c->svz, c->se, c->srho, c->sp, c->scs};
+        for (int a = 0; a < 7; ++a) { L.src[L.count] = s2[a]; L.dst[L.count++] = d2[a]; }
+        if (p->material_id) { L.isrc = p->material_id; L.idst = c->smat; }
+    }
+    TRY(launch_gather(n, c->perm, L, s));
+    c->T.n = n;
+    TRY(tree_build(c->T, c->skey, c->scan_scratch, c->st, s));
+    record(c, EV_TREE);
+    const int want_quad = c->cfg.gravity && c->cfg.precision == 1;
+    TRY(tree_upward(c->T, c->sx, c->sy, c->sz, c->sm, want_quad, c->st, s));
+    if (want_quad) TRY(tree_mixed_nodes(c->T, c->ord, c->cfg.theta_mixed, c->st, s));
+    record(c, EV_COM);
+    return MHPC_OK;
+}
+
+int stage_gravity(mhpc_ctx* c, const mhpc_particles* p) {
+    GravParams G;
+    std::memset(&G, 0, sizeof(G));
+    G.n = p->n;
+    G.eps2 = c->cfg.smoothing;
+    G.h_factor = (c->cfg.softening_mode == 1) ? c->cfg.softening_h_factor : 0.0;
+    G.G = c->cfg.si_units ? 6.67430e-11 : 1.0;
+    G.ord = c->ord;
+    if (c->cfg.precision == 1) {
+        G.theta = c->cfg.theta_mixed;
+        TRY(gravity_mixed(c->T, G, c->sx, c->sy, c->sz, c->sh, c->perm, p->g_ax, p->g_ay, p->g_az, c->st,
+                          c->stream));
+    } else {
+        G.theta = c->cfg.theta;
+        TRY(gravity_v2(c->T, G, c->sx, c->sy, c->sz, c->sh, c->perm, p->g_ax, p->g_ay, p->g_az, c->st,
+                       c->stream));
+    }
+    record(c, EV_GRAV);
+    return MHPC_OK;
+}
+
+int stage_sph(mhpc_ctx* c, const mhpc_particles* p) {
+    const int n = p->n;
+    cudaStream_t s = c->stream;
+    SphParams P = sph_params(c, n);
+    if (c->cfg.variable_sml) {
+        CUDA_TRY(cudaMemsetAsync(c->vh_done, 0, sizeof(int) * n, s));
+        CUDA_TRY(cudaMemsetAsync(c->vh_nit, 0xff, sizeof(int) * n, s));  // nit starts at -1
+        int target = c->mats[0].interactions > 0 ? c->mats[0].interactions : 50;
+        if (c->cfg.learned_h && c->mlp) TRY(mlp_predict_h(c->mlp, c, n));
+        TRY(sph_variable_h(c->T, P, c->sx, c->sy, c->sz, c->sh, c->hold, c->vh_done, c->vh_nit, c->vh_count,
+                           target, c->cfg.nb_tolerance, c->cfg.max_sml_iterations, c->cfg.max_sml_iterations + 2,
+                           c->st, s));
+        GatherList L;
+        std::memset(&L, 0, sizeof(L));
+        L.count = 1;
+        L.src[0] = c->sh;
+        L.dst[0] = p->sml;
+        TRY(launch_scatter(n, c->perm, L, s));
+    }
+    record(c, EV_SML);
+    SphSorted S;
+    S.x = c->sx; S.y = c->sy; S.z = c->sz; S.m = c->sm; S.h = c->sh;
+    S.vx = c->svx; S.vy = c->svy; S.vz = c->svz; S.e = c->se;
+    S.mat = p->material_id ? c->smat : nullptr;
+    S.rho = c->srho; S.p = c->sp; S.cs = c->scs;
+    TRY(sph_frnn(c->T, P, S, c->nbr, c->noi, c->st, s));
+    record(c, EV_FRNN);
+    TRY(sph_density_eos(P, S, c->nbr, c->noi, c->perm, p->rho, p->p, p->cs, c->st, s));
+    record(c, EV_DENS);
+    TRY(sph_forces(P, S, c->nbr, c->noi, c->perm, p->ax, p->ay, p->az, p->drhodt, p->dedt, p->dsmldt, c->st, s));
+    if (p->nnl || p->noi) TRY(sph_export_nnl(P, c->nbr, c->noi, c->perm, p->nnl, p->noi, s));
+    if (c->cfg.learned_h && c->mlp) TRY(mlp_collect(c->mlp, c, n));
+    record(c, EV_FORCES);
+    return MHPC_OK;
+}
+
+int rhs_async(mhpc_ctx* c, const mhpc_particles* p, int self_gravity) {
+    TRY(check_particles(c, p));
+    for (int e = 0; e < EV_COUNT; ++e) c->ev_recorded[e] = false;
+    c->last_n = p->n;
+    if (p->n == 0) return MHPC_OK;
+    CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevStatus), c->stream));
+    record(c, EV_START);
+    TRY(stage_tree(c, p));
+    if (c->cfg.gravity && self_gravity) TRY(stage_gravity(c, p));
+    if (c->cfg.sph) TRY(stage_sph(c, p));
+    record(c, EV_END);
+    c->first_rhs_done = true;
+    return MHPC_OK;
+}
+
+int read_status(mhpc_ctx* c) {
+    CUDA_TRY(cudaMemcpyAsync(c->h_st, c->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return c->h_st->code;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+const char* mhpc_status_string(int s) {
+    switch (s) {
+        case MHPC_OK: return "ok";
+        case MHPC_ERR_ARG: return "invalid argument";
+        case MHPC_ERR_CUDA: return "CUDA runtime error";
+        case MHPC_ERR_CAPACITY: return "particle count exceeds context capacity";
+        case MHPC_ERR_NODE_POOL: return "tree node pool exhausted";
+        case MHPC_ERR_DEPTH: return "traversal depth exceeded";
+        case MHPC_ERR_NEIGHBOURS: return "too many neighbours (max_num_interactions)";
+        case MHPC_ERR_NAN: return "non-finite position or non-positive density";
+        case MHPC_ERR_CONFIG: return "configuration file missing or malformed";
+        case MHPC_ERR_NO_DEVICE: return "no CUDA device";
+        case MHPC_ERR_TIMEOUT: return "bounded device wait ran out";
+        case MHPC_ERR_UNSUPPORTED: return "unsupported option";
+        default: return "unknown status";
+    }
+}
+
+int mhpc_version(void) { return 1; }
+
+int mhpc_bbox(const double* x, const double* y, const double* z, int n, double* bbox_dev, void* stream) {
+    if (n < 0 || !bbox_dev || (n > 0 && (!x || !y || !z))) return MHPC_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    // the ordered-integer (min, max) pair is reduced in the first 16 bytes of
+    // the caller's 48-byte output and expanded in place
+    long long* ord = reinterpret_cast<long long*>(bbox_dev);
+    TRY(launch_bbox(x, y, z, n, ord, nullptr, s));
+    TRY(launch_bbox_finish(ord, bbox_dev, s));
+    return MHPC_OK;
+}
+
+int mhpc_keys(const double* x, const double* y, const double* z, int n, const double* bbox_dev, int curve,
+              uint64_t* keys, void* stream) {
+    if (n < 0 || !bbox_dev || !keys || curve < 0 || curve > 1 || (n > 0 && (!x || !y || !z))) return MHPC_ERR_ARG;
+    return launch_keys_box(x, y, z, n, bbox_dev, curve, keys, (cudaStream_t)stream);
+}
+
+size_t mhpc_sort_scratch_bytes(int n) { return n < 0 ? 0 : sort_scratch_bytes(n) + 256; }
+
+// The last 256 bytes of the scratch hold a status word: nonzero (MHPC_ERR_TIMEOUT)
+// if a bounded look-back wait ran out.
+int mhpc_sort_pairs(const uint64_t* keys_in, const int* vals_in, uint64_t* keys_out, int* vals_out, int n,
+                    void* scratch, size_t scratch_bytes, void* stream) {
+    if (n < 0 || !scratch) return MHPC_ERR_ARG;
+    if (scratch_bytes < mhpc_sort_scratch_bytes(n)) return MHPC_ERR_ARG;
+    cudaStream_t s = (cudaStream_t)stream;
+    DevStatus* st = reinterpret_cast<DevStatus*>((char*)scratch + sort_scratch_bytes(n));
+    CUDA_TRY(cudaMemsetAsync(st, 0, sizeof(DevStatus), s));
+    return sort_pairs_u64(keys_in, vals_in, keys_out, vals_out, n, scratch, sort_scratch_bytes(n), st, s);
+}
+
+int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const mhpc_material* materials,
+                    int num_materials) {
+    if (!out || capacity <= 0 || !cfg || num_materials < 0 || num_materials > MHPC_MAX_MATERIALS)
+        return MHPC_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return MHPC_ERR_NO_DEVICE;
+    mhpc_ctx* c = new mhpc_ctx();
+    c->cfg = *cfg;
+    cudaGetDevice(&c->device);
+    c->cap = capacity;
+    c->maxnb = cfg->max_num_interactions > 0 ? cfg->max_num_interactions : 180;
+    double f = cfg->node_pool_factor > 0 ? cfg->node_pool_factor : 1.0;
+    c->cell_cap = (int)std::min(2147483000.0 - capacity, f * capacity + 20000.0);
+    c->cap_nodes = capacity + c->cell_cap;
+    if (num_materials == 0) {
+        std::memset(c->mats, 0, sizeof(c->mats));
+        c->mats[0].polytropic_gamma = 5.0 / 3.0;
+        c->mats[0].eos_type = 9;
+        c->mats[0].interactions = 60;
+        c->nmat = 1;
+    } else {
+        for (int i = 0; i < num_materials; ++i) c->mats[i] = materials[i];
+        c->nmat = num_materials;
+    }
+    int rc = MHPC_OK;
+    const size_t n = capacity, M = c->cap_nodes;
+#define A(p, cnt) \
+    if (!rc) rc = dalloc(c, &(p), (cnt))
+    A(c->st, 1);
+    A(c->ord, 2);
+    A(c->bbox, 6);
+    A(c->keys, n);
+    A(c->skey, n);
+    A(c->perm, n);
+    c->sort_bytes = sort_scratch_bytes(capacity);
+    {
+        char* q = nullptr;
+        A(q, c->sort_bytes);
+        c->sort_scratch = q;
+        char* r = nullptr;
+        A(r, scan_scratch_bytes(capacity) + 256);
+        c->scan_scratch = r;
+    }
+    A(c->sx, n); A(c->sy, n); A(c->sz, n); A(c->sm, n); A(c->sh, n);
+    TreeDev& T = c->T;
+    T.n = 0;
+    T.cap_nodes = c->cap_nodes;
+    A(T.dl, n); A(T.cnt, n); A(T.off, n + 1); A(T.leaf_node, n);
+    A(T.link, M); A(T.first, M); A(T.last, M); A(T.parent, M); A(T.nchild, M); A(T.arrive, M);
+    A(T.com, M); A(T.bmin, M); A(T.bmax, M);
+    A(T.root_nchild, 1); A(T.nodes, 1);
+    if (cfg->gravity) {
+        A(T.quad0, M); A(T.quad1, M); A(T.mpos, M); A(T.mlo, M);
+    }
+    if (cfg->sph) {
+        A(c->svx, n); A(c->svy, n); A(c->svz, n); A(c->se, n); A(c->srho, n); A(c->sp, n); A(c->scs, n);
+        A(c->smat, n);
+        size_t groups = (n + 31) / 32;
+        A(c->nbr, groups * 32 * (size_t)c->maxnb);
+        A(c->noi, n);
+        A(c->hold, n); A(c->vh_done, n); A(c->vh_nit, n); A(c->vh_count, n);
+    }
+    A(c->diag_part, diagnostics_scratch_doubles());
+    A(c->diag_out, 16);
+#undef A
+    if (!rc && cudaMallocHost(&c->h_st, sizeof(DevStatus)) != cudaSuccess) rc = MHPC_ERR_CUDA;
+    for (int e = 0; e < EV_COUNT && !rc; ++e)
+        if (cudaEventCreate(&c->ev[e]) != cudaSuccess) rc = MHPC_ERR_CUDA;
+    if (!rc && cfg->learned_h) rc = mlp_create(&c->mlp, capacity);
+    if (rc) {
+        mhpc_ctx_destroy(c);
+        return rc;
+    }
+    CUDA_TRY(cudaMemset(c->st, 0, sizeof(DevStatus)));
+    *out = c;
+    return MHPC_OK;
+}
+
+int mhpc_ctx_destroy(mhpc_ctx* c) {
+    if (!c) return MHPC_ERR_ARG;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    cudaDeviceSynchronize();
+    for (void* p : c->allocs) cudaFree(p);
+    if (c->h_st) cudaFreeHost(c->h_st);
+    for (int e = 0; e < EV_COUNT; ++e)
+        if (c->ev[e]) cudaEventDestroy(c->ev[e]);
+    if (c->mlp) mlp_destroy(c->mlp);
+    if (c->mirror_ready) {
+        double** ptrs[] = {&c->mirror.x, &c->mirror.y, &c->mirror.z, &c->mirror.mass, &c->mirror.vx, &c->mirror.vy,
+                           &c->mirror.vz, &c->mirror.ax, &c->mirror.ay, &c->mirror.az, &c->mirror.g_ax,
+                           &c->mirror.g_ay, &c->mirror.g_az, &c->mirror.g_ax_old, &c->mirror.g_ay_old,
+                           &c->mirror.g_az_old, &c->mirror.sml, &c->mirror.rho, &c->mirror.p, &c->mirror.cs,
+                           &c->mirror.e, &c->mirror.drhodt, &c->mirror.dedt, &c->mirror.dsmldt};
+        for (auto pp : ptrs)
+            if (*pp) cudaFree(*pp);
+    }
+    delete c;
+    return MHPC_OK;
+}
+
+int mhpc_ctx_set_stream(mhpc_ctx* c, void* stream) {
+    if (!c) return MHPC_ERR_ARG;
+    c->stream = (cudaStream_t)stream;
+    return MHPC_OK;
+}
+
+int mhpc_ctx_set_config(mhpc_ctx* c, const mhpc_config* cfg) {
+    if (!c || !cfg) return MHPC_ERR_ARG;
+    if ((cfg->sph && !c->cfg.sph) || (cfg->gravity && !c->cfg.gravity) ||
+        (cfg->learned_h && !c->mlp) || cfg->max_num_interactions != c->maxnb)
+        return MHPC_ERR_ARG;  // would need buffers the context did not allocate
+    c->cfg = *cfg;
+    return MHPC_OK;
+}
+
+int mhpc_rhs_async(mhpc_ctx* c, const mhpc_particles* p, int step, int self_gravity) {
+    (void)step;
+    if (!c) return MHPC_ERR_ARG;
+    return rhs_async(c, p, self_gravity);
+}
+
+int mhpc_ctx_status(mhpc_ctx* c) {
+    if (!c) return MHPC_ERR_ARG;
+    return read_status(c);
+}
+
+int mhpc_rhs(mhpc_ctx* c, const mhpc_particles* p, int step, int self_gravity, float* ms_out) {
+    if (!c) return MHPC_ERR_ARG;
+    TRY(mhpc_rhs_async(c, p, step, self_gravity));
+    int code = read_status(c);
+    if (ms_out) {
+        *ms_out = 0.f;
+        if (c->ev_recorded[EV_START] && c->ev_recorded[EV_END])
+            cudaEventElapsedTime(ms_out, c->ev[EV_START], c->ev[EV_END]);
+    }
+    return code;
+}
+
+int mhpc_stage_tree(mhpc_ctx* c, const mhpc_particles* p) {
+    if (!c) return MHPC_ERR_ARG;
+    TRY(check_particles(c, p));
+    if (p->n == 0) return MHPC_OK;
+    CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevStatus), c->stream));
+    c->last_n = p->n;
+    return stage_tree(c, p);
+}
+
+int mhpc_stage_gravity(mhpc_ctx* c, const mhpc_particles* p) {
+    if (!c || !c->cfg.gravity) return MHPC_ERR_ARG;
+    TRY(check_particles(c, p));
+    if (p->n == 0) return MHPC_OK;
+    return stage_gravity(c, p);
+}
+
+int mhpc_stage_sph(mhpc_ctx* c, const mhpc_particles* p) {
+    if (!c || !c->cfg.sph) return MHPC_ERR_ARG;
+    TRY(check_particles(c, p));
+    if (p->n == 0) return MHPC_OK;
+    return stage_sph(c, p);
+}
+
+int mhpc_integrate(mhpc_ctx* c, const mhpc_particles* p, int step, double* dt_out) {
+    if (!c) return MHPC_ERR_ARG;
+    TRY(check_particles(c, p));
+    const double dt = c->cfg.time_step;
+    cudaStream_t s = c->stream;
+    if (dt_out) *dt_out = dt;
+    if (p->n == 0) return MHPC_OK;
+    switch (c->cfg.integrator) {
+        case 2: {  // Leapfrog::integrate (src/integrator/leapfrog.cpp:21-117)
+            if (!p->g_ax_old || !p->g_ay_old || !p->g_az_old) return MHPC_ERR_ARG;
+            if (step == 0 && !c->first_rhs_done) {
+                TRY(rhs_async(c, p, 1));
+                int code = read_status(c);
+                if (code) return code;
+            }
+            TRY(launch_leapfrog_x(*p, dt, s));
+            TRY(rhs_async(c, p, 1));
+            TRY(launch_leapfrog_v(*p, dt, s));
+        } break;
+        case 0: {  // ExplicitEuler::integrate (src/integrator/explicit_euler.cpp:17-99)
+            TRY(rhs_async(c, p, 1));
+            TRY(launch_euler(*p, dt, c->cfg.gravity, c->cfg.sph, c->cfg.integrate_density, c->cfg.integrate_energy,
+                             c->cfg.integrate_sml, s));
+        } break;
+        default:
+            return MHPC_ERR_UNSUPPORTED;
+    }
+    return read_status(c);
+}
+
+int mhpc_integrate_host(mhpc_ctx* c, mhpc_particles* h, int step, double* dt_out) {
+    if (!c || !h) return MHPC_ERR_ARG;
+    if (h->n > c->cap || h->n < 0) return MHPC_ERR_CAPACITY;
+    const size_t n = c->cap;
+    mhpc_particles& m = c->mirror;
+    if (!c->mirror_ready) {
+        std::memset(&m, 0, sizeof(m));
+        double** ptrs[] = {&m.x, &m.y, &m.z, &m.mass, &m.vx, &m.vy, &m.vz, &m.g_ax, &m.g_ay, &m.g_az,
+                           &m.g_ax_old, &m.g_ay_old, &m.g_az_old};
+        for (auto pp : ptrs) CUDA_TRY(cudaMalloc(pp, sizeof(double) * n));
+        if (c->cfg.sph) {
+            double** p2[] = {&m.ax, &m.ay, &m.az, &m.sml, &m.rho, &m.p, &m.cs, &m.e, &m.drhodt, &m.dedt, &m.dsmldt};
+            for (auto pp : p2) CUDA_TRY(cudaMalloc(pp, sizeof(double) * n));
+        }
+        c->mirror_ready = true;
+    }
+    m.n = h->n;
+    m.num_nodes = h->n;
+    cudaStream_t s = c->stream;
+    const size_t b = sizeof(double) * h->n;
+    // state in (positions, velocities, masses; leapfrog carries g_a between steps)
+    struct Pair { double* d; double* hh; };
+    std::vector<Pair> in = {{m.x, h->x}, {m.y, h->y}, {m.z, h->z}, {m.mass, h->mass},
+                            {m.vx, h->vx}, {m.vy, h->vy}, {m.vz, h->vz}};
+    if (c->cfg.integrator == 2) {
+        in.push_back({m.g_ax, h->g_ax}); in.push_back({m.g_ay, h->g_ay}); in.push_back({m.g_az, h->g_az});
+    }
+    if (c->cfg.sph) {
+        in.push_back({m.sml, h->sml}); in.push_back({m.e, h->e}); in.push_back({m.rho, h->rho});
+        in.push_back({m.p, h->p}); in.push_back({m.cs, h->cs});
+    }
+    for (auto& q : in)
+        if (q.hh) CUDA_TRY(cudaMemcpyAsync(q.d, q.hh, b, cudaMemcpyHostToDevice, s));
+    // leapfrog: step 0 computes the initial accelerations; later steps carry
+    // the caller's g_a of the previous step
+    if (c->cfg.integrator == 2) c->first_rhs_done = step != 0;
+    int rc = mhpc_integrate(c, &m, step, dt_out);
+    if (rc) return rc;
+    std::vector<Pair> outp = {{m.x, h->x}, {m.y, h->y}, {m.z, h->z}, {m.vx, h->vx}, {m.vy, h->vy}, {m.vz, h->vz}};
+    if (c->cfg.gravity) {
+        outp.push_back({m.g_ax, h->g_ax}); outp.push_back({m.g_ay, h->g_ay}); outp.push_back({m.g_az, h->g_az});
+    }
+    if (c->cfg.sph) {
+        outp.push_back({m.sml, h->sml}); outp.push_back({m.e, h->e}); outp.push_back({m.rho, h->rho});
+        outp.push_back({m.p, h->p}); outp.push_back({m.cs, h->cs});
+        outp.push_back({m.ax, h->ax}); outp.push_back({m.ay, h->ay}); outp.push_back({m.az, h->az});
+    }
+    for (auto& q : outp)
+        if (q.hh) CUDA_TRY(cudaMemcpyAsync(q.hh, q.d, b, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return MHPC_OK;
+}
+
+int mhpc_export_sorted(mhpc_ctx* c, uint64_t* keys_dev, int* perm_dev) {
+    if (!c) return MHPC_ERR_ARG;
+    const int n = c->last_n;
+    if (keys_dev) CUDA_TRY(cudaMemcpyAsync(keys_dev, c->skey, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, c->stream));
+    if (perm_dev) CUDA_TRY(cudaMemcpyAsync(perm_dev, c->perm, sizeof(int) * n, cudaMemcpyDeviceToDevice, c->stream));
+    return read_status(c);
+}
+
+int mhpc_export_tree(mhpc_ctx* c, int num_nodes, int* child, int* level, double* x, double* y, double* z, double* m,
+                     int* cells_out) {
+    if (!c || !child) return MHPC_ERR_ARG;
+    int code = read_status(c);
+    if (code) return code;
+    const int n = c->last_n;
+    int total = 0;
+    CUDA_TRY(cudaMemcpy(&total, c->T.nodes, sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<int2> link(total);
+    std::vector<int> first(total);
+    std::vector<double4> com(total);
+    std::vector<int> perm(n);
+    std::vector<uint64_t> skey(n);
+    CUDA_TRY(cudaMemcpy(link.data(), c->T.link, sizeof(int2) * total, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(first.data(), c->T.first, sizeof(int) * total, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(com.data(), c->T.com, sizeof(double4) * total, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(perm.data(), c->perm, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    std::vector<double> px(n), py(n), pz(n);
+    CUDA_TRY(cudaMemcpy(px.data(), c->sx, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(py.data(), c->sy, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(pz.data(), c->sz, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    long long ord[2];
+    CUDA_TRY(cudaMemcpy(ord, c->ord, sizeof(ord), cudaMemcpyDeviceToHost));
+    const double lo = ord_to_dbl(ord[0]), hi = ord_to_dbl(ord[1]);
+    // cell ids: n + ordinal in pre-order
+    std::vector<int> id(total, -1);
+    int cells = 0;
+    for (int i = 0; i < total; ++i) id[i] = (link[i].y & ND_LEAF) ? perm[first[i]] : n + cells++;
+    if (cells_out) *cells_out = cells;
+    if (n + cells > num_nodes) return MHPC_ERR_CAPACITY;
+    for (long i = 0; i < 8L * num_nodes; ++i) child[i] = -1;
+    if (level) for (int i = 0; i < num_nodes; ++i) level[i] = -1;
+    // octant of a sorted particle at level L (1-based), reference bit rule
+    auto octant = [&](int sidx, int L) {
+        double mn[3] = {lo, lo, lo}, mx[3] = {hi, hi, hi};
+        double p[3] = {px[sidx], py[sidx], pz[sidx]};
+        int son = 0;
+        for (int l = 0; l < L; ++l) {
+            son = 0;
+            for (int d = 0; d < 3; ++d) {
+                volatile double mid = 0.5 * (mn[d] + mx[d]);
+                if (p[d] < mid) { son += 1 << d; mx[d] = mid; } else mn[d] = mid;
+            }
+        }
+        return son;
+    };
+    for (int i = 0; i < total; ++i) {
+        const int L = link[i].y & 0xff;
+        const int self = id[i];
+        if (level) level[self] = L;
+        if (!(link[i].y & ND_LEAF)) {
+            if (x) x[self] = com[i].x;
+            if (y) y[self] = com[i].y;
+            if (z) z[self] = com[i].z;
+            if (m) m[self] = com[i].w;
+            for (int ch = i + 1; ch < link[i].x; ch = link[ch].x) {
+                const int slot = octant(first[ch], L + 1);
+                child[8 * self + slot] = id[ch];
+            }
+        }
+        if (L == 1) child[octant(first[i], 1)] = self;
+    }
+    return MHPC_OK;
+}
+
+int mhpc_get_stats(mhpc_ctx* c, mhpc_stats* o) {
+    if (!c || !o) return MHPC_ERR_ARG;
+    std::memset(o, 0, sizeof(*o));
+    int code = read_status(c);
+    o->n = c->last_n;
+    if (c->last_n > 0) {
+        int total = 0;
+        CUDA_TRY(cudaMemcpy(&total, c->T.nodes, sizeof(int), cudaMemcpyDeviceToHost));
+        o->cells = total - c->last_n;
+        CUDA_TRY(cudaMemcpy(o->bbox, c->bbox, sizeof(double) * 6, cudaMemcpyDeviceToHost));
+        o->radius = 0.5 * (o->bbox[1] - o->bbox[0]);
+    }
+    DevStatus& h = *c->h_st;
+    o->max_level = h.max_level;
+    o->key_collisions = h.key_collisions;
+    o->gravity_interactions = (double)h.interactions;
+    o->gravity_nodes_visited = (double)h.nodes_visited;
+    o->gravity_quad_interactions = (double)h.quad_interactions;
+    o->max_noi = h.max_noi;
+    o->sml_out_of_band = h.sml_out_of_band;
+    o->predictor_used = h.predictor_used;
+    o->predictor_fallback = h.predictor_fallback;
+    const int pairs[12][2] = {{EV_START, EV_KEYS}, {EV_KEYS, EV_SORT}, {EV_SORT, EV_TREE}, {EV_TREE, EV_COM},
+                              {EV_COM, EV_GRAV},   {EV_SML, EV_FRNN}, {EV_COM, EV_SML},   {EV_FRNN, EV_DENS},
+                              {EV_DENS, EV_FORCES}, {-1, -1},         {-1, -1},           {EV_START, EV_END}};
+    for (int k = 0; k < 12; ++k) {
+        int a = pairs[k][0], b = pairs[k][1];
+        if (a >= 0 && c->ev_recorded[a] && c->ev_recorded[b]) cudaEventElapsedTime(&o->ms_stage[k], c->ev[a], c->ev[b]);
+    }
+    if (c->ev_recorded[EV_GRAV] && c->ev_recorded[EV_SML]) {
+        // gravity ran before SPH: the SML stage starts at EV_GRAV
+        cudaEventElapsedTime(&o->ms_stage[6], c->ev[EV_GRAV], c->ev[EV_SML]);
+    }
+    return code;
+}
+
+int mhpc_diagnostics(mhpc_ctx* c, const mhpc_particles* p, double* out) {
+    if (!c || !p || !out) return MHPC_ERR_ARG;
+    TRY(check_particles(c, p));
+    TRY(launch_diagnostics(*p, c->cfg.sph, c->diag_part, c->diag_out, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(out, c->diag_out, sizeof(double) * 11, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return MHPC_OK;
+}
+
+int mhpc_direct_gravity(const double* x, const double* y, const double* z, const double* m, int n, const int* targets,
+                        int nt, double eps2, double* gax, double* gay, double* gaz, void* stream) {
+    if (n < 0 || nt < 0 || (nt > 0 && (!x || !y || !z || !m || !targets || !gax || !gay || !gaz))) return MHPC_ERR_ARG;
+    return launch_direct(x, y, z, m, n, targets, nt, eps2, gax, gay, gaz, (cudaStream_t)stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,21 @@
+#pragma once
+#include "tree.cuh"
+
+struct GravParams {
+    int n;
+    double eps2;          // global softening eps^2 (config `smoothing`)
+    double h_factor;      // softening tied to h: eps_i = h_factor * h_i (0 = off)
+    double G;             // gravitational constant (1 unless SI units)
+    double theta;         // opening parameter
+    const long long* ord; // device bounding box (ordered-int min, max); radius = (max - min) / 2
+};
+
+// Plain FP64 walk with the reference's computeForces_v2 semantics.
+int gravity_v2(const TreeDev& T, const GravParams& P, const double* sx, const double* sy, const double* sz,
+               const double* sh, const int* perm, double* gax, double* gay, double* gaz, DevStatus* st,
+               cudaStream_t s);
+// Mixed FP32 walk: hi/lo node positions relative to the group centre, group
+// bounding-box criterion, monopole + quadrupole, FP64 flush of FP32 partial sums.
+int gravity_mixed(const TreeDev& T, const GravParams& P, const double* sx, const double* sy, const double* sz,
+                  const double* sh, const int* perm, double* gax, double* gay, double* gaz, DevStatus* st,
+                  cudaStream_t s);

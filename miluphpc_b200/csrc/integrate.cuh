@@ -1,0 +1,24 @@
+#pragma once
+#include "common.cuh"
+
+#define MHPC_GATHER_MAX 16
+
+// dst[a][s] = src[a][perm[s]] (gather) or dst[a][perm[s]] = src[a][s] (scatter)
+struct GatherList {
+    int count;
+    const double* src[MHPC_GATHER_MAX];
+    double* dst[MHPC_GATHER_MAX];
+    const int* isrc;  // optional int array gathered alongside
+    int* idst;
+};
+
+int launch_gather(int n, const int* perm, const GatherList& L, cudaStream_t s);
+int launch_scatter(int n, const int* perm, const GatherList& L, cudaStream_t s);
+int launch_leapfrog_x(const mhpc_particles& p, double dt, cudaStream_t s);
+int launch_leapfrog_v(const mhpc_particles& p, double dt, cudaStream_t s);
+int launch_euler(const mhpc_particles& p, double dt, int gravity, int sph, int int_rho, int int_e, int int_sml,
+                 cudaStream_t s);
+int launch_diagnostics(const mhpc_particles& p, int sph, double* part, double* out, cudaStream_t s);
+size_t diagnostics_scratch_doubles();
+int launch_direct(const double* x, const double* y, const double* z, const double* m, int n, const int* tg, int nt,
+                  double eps2, double* gax, double* gay, double* gaz, cudaStream_t s);

@@ -1,0 +1,366 @@
+// SPH: fixed-radius neighbour search, variable smoothing length, density /
+// sound speed / pressure, and internal (hydro) forces.
+//
+// Neighbour search: the reference walks the tree once per particle with a
+// per-thread stack (SPH::fixedRadiusNN, src/sph/sph.cu:93-281).  Here a warp
+// walks once for 32 consecutive SFC-sorted particles: nodes whose particle
+// bounding box overlaps the group's search box (group box grown by each
+// lane's h) are opened, overlapping leaves and small cells are staged as
+// candidates in shared memory, and each lane then tests the staged
+// candidates with the reference's pair rule d^2 < h_i^2 && d^2 < h_j^2
+// (j != i), d^2 formed without FMA contraction like the reference build.  The
+// walk is conservative, so the neighbour set equals the brute-force set.
+#include "sph.cuh"
+
+namespace {
+
+constexpr int kBlock = 128;
+constexpr int kWarps = kBlock / 32;
+constexpr int kCap = 512;     // staged candidates per warp
+constexpr int kSmall = 16;    // cells with at most this many particles are staged whole
+
+// ------------------------------------------------------------ kernels W
+// SmoothingKernel::{spiky, cubicSpline, wendlandc2, wendlandc4, wendlandc6}
+// (src/sph/kernel.cu:14-183), 3-D forms, support radius = h.
+__device__ __forceinline__ void skernel(int type, double r, double h, double& W, double& dWdr) {
+    const double q = r / h;
+    W = 0.0;
+    dWdr = 0.0;
+    switch (type) {
+        case 0: {  // spiky
+            if (q <= 1.0 && q >= 0.0) {
+                const double a = 1.0 - q;
+                W = 15. / (M_PI * h * h * h) * a * a * a;
+                dWdr = -45 / (M_PI * h * h * h * h) * a * a;
+            }
+        } break;
+        case 1: {  // cubic spline
+            const double f = 8. / M_PI * 1. / (h * h * h);
+            if (q > 1) {
+            } else if (q > 0.5) {
+                const double a = 1. - q;
+                W = 2. * f * a * a * a;
+                dWdr = -6. * f * 1. / h * a * a;
+            } else {
+                W = f * (6. * q * q * q - 6. * q * q + 1.);
+                dWdr = 6. * f / h * (3 * q * q - 2 * q);
+            }
+        } break;
+        case 2: {  // Wendland C2
+            if (r <= h) {
+                const double a = 1 - q;
+                W = 21. / (2 * M_PI * h * h * h) * a * a * a * a * (1 + 4 * q) * (q < 1);
+                dWdr = -210. / (M_PI * h * h * h * h) * q * a * a * a * (q < 1);
+            }
+        } break;
+        case 3: {  // Wendland C4 (derivative as written in the reference)
+            if (r <= h) {
+                const double a = 1 - q, a5 = a * a * a * a * a;
+                W = 495. / (32. * M_PI * h * h * h) * a5 * a * (1. + 6. * q + 35. / 3. * q * q) * (q < 1);
+                dWdr = -1485. / (16. * M_PI * h * h * h * h) * a5 * (1. - 35. * q * q + 105. * q * q * q) * (q < 1);
+            }
+        } break;
+        default: {  // Wendland C6
+            if (r <= h) {
+                const double a = 1 - q, a7 = a * a * a * a * a * a * a;
+                W = 1365. / (64. * M_PI * h * h * h) * a7 * a * (1. + 8. * q + 25. * q * q + 32 * q * q * q) * (q < 1);
+                dWdr = -15015. / (32. * M_PI * h * h * h * h) * q * a7 * (1. + 7 * q + 16 * q * q) * (q < 1);
+            }
+        } break;
+    }
+}
+
+__device__ __forceinline__ double d2_exact(double dx, double dy, double dz) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+__device__ __forceinline__ size_t nb_index(long s, int k, int maxnb) {
+    return ((size_t)(s >> 5) * maxnb + k) * 32 + (s & 31);
+}
+
+// ------------------------------------------------------------ FRNN walk
+// mode 0: write lists (h_i = h[i], h_j = h[j]); mode 1: count only for lanes
+// with done[i] == 0, with h_i = h[i], h_j = h[j] (the variable-h sweep passes
+// the sweep's snapshot as h).
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) k_frnn(TreeDev T, int n, int maxnb, const double* __restrict__ sx,
+                                                 const double* __restrict__ sy, const double* __restrict__ sz,
+                                                 const double* __restrict__ sh, const int* __restrict__ done,
+                                                 int* __restrict__ nbr, int* __restrict__ noi, DevStatus* st) {
+    __shared__ int cand[kWarps][kCap];
+    if (st->code) return;
+    const int M = *T.nodes;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long g = ((long)blockIdx.x * kBlock + threadIdx.x) >> 5;
+    const long s = g * 32 + lane;
+    const bool valid = s < n;
+    bool active = valid && (MODE == 0 || done[s] == 0);
+    if (!__any_sync(MHPC_FULL, active)) return;
+    double px = 0, py = 0, pz = 0, hi = 0;
+    if (valid) { px = sx[s]; py = sy[s]; pz = sz[s]; hi = sh[s]; }
+    const double hi2 = hi * hi;
+    double lx = active ? px - hi : 1e300, ly = active ? py - hi : 1e300, lz = active ? pz - hi : 1e300;
+    double ux = active ? px + hi : -1e300, uy = active ? py + hi : -1e300, uz = active ? pz + hi : -1e300;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lx = fmin(lx, __shfl_xor_sync(MHPC_FULL, lx, o));
+        ly = fmin(ly, __shfl_xor_sync(MHPC_FULL, ly, o));
+        lz = fmin(lz, __shfl_xor_sync(MHPC_FULL, lz, o));
+        ux = fmax(ux, __shfl_xor_sync(MHPC_FULL, ux, o));
+        uy = fmax(uy, __shfl_xor_sync(MHPC_FULL, uy, o));
+        uz = fmax(uz, __shfl_xor_sync(MHPC_FULL, uz, o));
+    }
+    const float qlx = __double2float_rd(lx), qly = __double2float_rd(ly), qlz = __double2float_rd(lz);
+    const float qux = __double2float_ru(ux), quy = __double2float_ru(uy), quz = __double2float_ru(uz);
+    int k = 0;       // neighbours found by this lane
+    int cnt = 0;     // staged candidates (warp-uniform)
+    int* C = cand[w];
+    auto flush = [&]() {
+        __syncwarp();
+        if (active) {
+            for (int c = 0; c < cnt; ++c) {
+                const int j = C[c];
+                if (j == s) continue;
+                const double dx = px - __ldg(sx + j), dy = py - __ldg(sy + j), dz = pz - __ldg(sz + j);
+                const double d = d2_exact(dx, dy, dz);
+                const double hj = __ldg(sh + j);
+                if (d < hi2 && d < hj * hj) {
+                    if (MODE == 0 && k < maxnb) nbr[nb_index(s, k, maxnb)] = j;
+                    ++k;
+                }
+            }
+        }
+        __syncwarp();
+        cnt = 0;
+    };
+    int nd = 0;
+    while (nd < M) {
+        const int2 lk = __ldg(T.link + nd);
+        const float4 bl = __ldg(T.bmin + nd), bh = __ldg(T.bmax + nd);
+        const bool overlap = !(bh.x < qlx || bl.x > qux || bh.y < qly || bl.y > quy || bh.z < qlz || bl.z > quz);
+        if (!overlap) { nd = lk.x; continue; }
+        const int f = __ldg(T.first + nd);
+        int len = 0;
+        if (lk.y & ND_LEAF) len = 1;
+        else {
+            const int l = __ldg(T.last + nd);
+            if (l - f + 1 <= kSmall) len = l - f + 1;
+        }
+        if (len == 0) { ++nd; continue; }
+        if (cnt + len > kCap) flush();
+        if (lane < len) C[cnt + lane] = f + lane;
+        cnt += len;
+        nd = lk.x;
+    }
+    flush();
+    if (active) {
+        noi[s] = k;
+        if (MODE == 0 && k > maxnb) set_status(st, MHPC_ERR_NEIGHBOURS, (int)s);
+        if (MODE == 0) atomicMax(&st->max_noi, k);
+    }
+}
+
+// ------------------------------------------------------- variable h update
+// Convergence rule and update of fixedRadiusNN_variableSML
+// (src/sph/sph.cu:911-933): stop when nit > max_iter or |n - target| < tol,
+// provided n < maxnb; otherwise h *= 0.5 (1 + (target / max(n,1))^(1/3)).
+__global__ void k_vh_update(int n, const int* __restrict__ count, double* h, int* done, int* nit, int target, int tol,
+                            int max_iter, int maxnb) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (done[i]) continue;
+        const int it = ++nit[i];
+        const int c = count[i];
+        if ((it > max_iter || abs(c - target) < tol) && c < maxnb) {
+            done[i] = 1;
+        } else {
+            const int cc = c < 1 ? 1 : c;
+            h[i] *= 0.5 * (1.0 + pow((double)target / (double)cc, 1. / 3.));
+        }
+    }
+}
+
+__global__ void k_copy(int n, const double* __restrict__ a, double* b) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
+}
+
+// --------------------------------------------------- density + EOS (fused)
+// calculateDensity (src/sph/density.cu:8-72), then calculateSoundSpeed
+// (src/sph/soundspeed.cu:38-97) and calculatePressure (src/sph/pressure.cu:5-87)
+// in the reference's order: the ideal-gas sound speed uses the pressure of
+// the previous call.
+__global__ void __launch_bounds__(kBlock) k_density_eos(SphParams P, SphSorted S, const int* __restrict__ nbr,
+                                                        const int* __restrict__ noi, const int* __restrict__ perm,
+                                                        double* rho_out, double* p_out, double* cs_out,
+                                                        DevStatus* st) {
+    if (st->code) return;
+    const long s = (long)blockIdx.x * kBlock + threadIdx.x;
+    if (s >= P.n) return;
+    const double xi = S.x[s], yi = S.y[s], zi = S.z[s], hi = S.h[s];
+    double rho;
+    if (P.integrate_density) {
+        rho = S.rho[s];
+    } else {
+        double W, dWdr;
+        skernel(P.kernel, 0.0, hi, W, dWdr);
+        rho = S.m[s] * W;
+        const int k = min(noi[s], P.maxnb);
+        for (int q = 0; q < k; ++q) {
+            const int j = nbr[nb_index(s, q, P.maxnb)];
+            const double hb = P.avg_h ? 0.5 * (hi + __ldg(S.h + j)) : hi;
+            const double dx = xi - __ldg(S.x + j), dy = yi - __ldg(S.y + j), dz = zi - __ldg(S.z + j);
+            const double r = sqrt(dx * dx + dy * dy + dz * dz);
+            skernel(P.kernel, r, hb, W, dWdr);
+            rho += __ldg(S.m + j) * W;
+        }
+        if (!(rho > 0.0)) set_status(st, MHPC_ERR_NAN, (int)s);
+    }
+    const int mid = S.mat ? S.mat[s] : 0;
+    const MatDev& M = P.mat[mid];
+    double p = S.p[s], cs = S.cs[s];
+    switch (M.eos_type) {
+        case 0: cs = sqrt(M.K * pow(rho, M.gamma - 1.0)); break;
+        case 9: cs = sqrt(M.gamma * p / rho); break;
+        case 12: cs = 0.0; break;
+        default: break;
+    }
+    switch (M.eos_type) {
+        case 0: p = M.K * pow(rho, M.gamma); break;
+        case 1: p = (M.bulk / M.n_exp) * (pow(rho / M.rho0, M.n_exp) - 1.0); break;
+        case 3: p = 41255.407 * rho; break;
+        case 9: p = (M.gamma - 1) * rho * S.e[s]; break;
+        case 12: p = cs * cs * rho; break;
+        default: break;
+    }
+    S.rho[s] = rho;
+    S.p[s] = p;
+    S.cs[s] = cs;
+    const int o = perm[s];
+    rho_out[o] = rho;
+    p_out[o] = p;
+    cs_out[o] = cs;
+}
+
+// ------------------------------------------------------------- forces
+// SPH::Kernel::internalForces, hydro part, SPH_EQU_VERSION 1
+// (src/sph/internal_forces.cu:372-552).
+__global__ void __launch_bounds__(kBlock) k_forces(SphParams P, SphSorted S, const int* __restrict__ nbr,
+                                                   const int* __restrict__ noi, const int* __restrict__ perm,
+                                                   double* ax_o, double* ay_o, double* az_o, double* drhodt_o,
+                                                   double* dedt_o, double* dsmldt_o, DevStatus* st) {
+    if (st->code) return;
+    const long s = (long)blockIdx.x * kBlock + threadIdx.x;
+    if (s >= P.n) return;
+    const double xi = S.x[s], yi = S.y[s], zi = S.z[s], hi = S.h[s];
+    const double vxi = S.vx[s], vyi = S.vy[s], vzi = S.vz[s];
+    const double rhoi = S.rho[s], pi = S.p[s], csi = S.cs[s];
+    const int mid = S.mat ? S.mat[s] : 0;
+    const double alpha = P.mat[mid].alpha, beta = P.mat[mid].beta;
+    const double pri = pi / (rhoi * rhoi);
+    double a0 = 0, a1 = 0, a2 = 0, drho = 0, de = 0, dh = 0;
+    const int k = min(noi[s], P.maxnb);
+    for (int q = 0; q < k; ++q) {
+        const int j = nbr[nb_index(s, q, P.maxnb)];
+        const double hj = __ldg(S.h + j);
+        const double hb = P.avg_h ? 0.5 * (hi + hj) : hi;
+        const double dx = xi - __ldg(S.x + j), dy = yi - __ldg(S.y + j), dz = zi - __ldg(S.z + j);
+        const double rr = dx * dx + dy * dy + dz * dz;
+        const double r = sqrt(rr);
+        double W, dWdr;
+        skernel(P.kernel, r, hb, W, dWdr);
+        const double g = dWdr / r;
+        const double gx = g * dx, gy = g * dy, gz = g * dz;
+        const double dvx = vxi - __ldg(S.vx + j), dvy = vyi - __ldg(S.vy + j), dvz = vzi - __ldg(S.vz + j);
+        const double vvnablaW = dvx * gx + dvy * gy + dvz * gz;
+        const double vr = dvx * dx + dvy * dy + dvz * dz;
+        const double rhoj = __ldg(S.rho + j), mj = __ldg(S.m + j);
+        double pij = 0.0;
+        if (vr < 0) {
+            const double csbar = 0.5 * (csi + __ldg(S.cs + j));
+            const double smooth = 0.5 * (hi + hj);
+            const double mu = smooth * vr / (rr + smooth * smooth * 1e-2);
+            const double rhobar = 0.5 * (rhoi + rhoj);
+            pij = (beta * mu - alpha * csbar) * mu / rhobar;
+        }
+        const double pf = -mj * (pri + __ldg(S.p + j) / (rhoj * rhoj));
+        const double ajx = pf * gx, ajy = pf * gy, ajz = pf * gz;
+        const double vf = mj * (-pij);
+        a0 += ajx + vf * gx;
+        a1 += ajy + vf * gy;
+        a2 += ajz + vf * gz;
+        drho += rhoi / rhoj * mj * vvnablaW;
+        if (P.integrate_sml) dh -= 1. / 3. * hi * mj / rhoj * vvnablaW;
+        if (P.integrate_energy) de += 0.5 * mj * pij * vvnablaW - 0.5 * (ajx * dvx + ajy * dvy + ajz * dvz);
+    }
+    const int o = perm[s];
+    ax_o[o] = a0;
+    ay_o[o] = a1;
+    az_o[o] = a2;
+    if (drhodt_o) drhodt_o[o] = drho;
+    if (dedt_o) dedt_o[o] = P.integrate_energy ? de : 0.0;
+    if (dsmldt_o) dsmldt_o[o] = P.integrate_sml ? dh : 0.0;
+}
+
+__global__ void k_export_nnl(int n, int maxnb, const int* __restrict__ nbr, const int* __restrict__ noi,
+                             const int* __restrict__ perm, int* nnl, int* noi_out) {
+    for (long s = blockIdx.x * (long)blockDim.x + threadIdx.x; s < n; s += (long)gridDim.x * blockDim.x) {
+        const int o = perm[s];
+        const int k = noi[s];
+        if (noi_out) noi_out[o] = k;
+        if (nnl) {
+            const int kk = min(k, maxnb);
+            for (int q = 0; q < maxnb; ++q)
+                nnl[(size_t)o * maxnb + q] = q < kk ? perm[nbr[nb_index(s, q, maxnb)]] : -1;
+        }
+    }
+}
+
+}  // namespace
+
+int sph_frnn(const TreeDev& T, const SphParams& P, const SphSorted& S, int* nbr, int* noi, DevStatus* st,
+             cudaStream_t s) {
+    if (P.n <= 0) return MHPC_OK;
+    long blocks = (((long)P.n + 31) / 32 * 32 + kBlock - 1) / kBlock;
+    k_frnn<0><<<(int)blocks, kBlock, 0, s>>>(T, P.n, P.maxnb, S.x, S.y, S.z, S.h, nullptr, nbr, noi, st);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int sph_variable_h(const TreeDev& T, const SphParams& P, const double* x, const double* y, const double* z,
+                   double* h, double* hold, int* done, int* nit, int* count, int target, int tol, int max_iter,
+                   int sweeps, DevStatus* st, cudaStream_t s) {
+    if (P.n <= 0) return MHPC_OK;
+    long blocks = (((long)P.n + 31) / 32 * 32 + kBlock - 1) / kBlock;
+    int g = grid_for(P.n, 256, 148 * 16);
+    for (int it = 0; it < sweeps; ++it) {
+        k_copy<<<g, 256, 0, s>>>(P.n, h, hold);
+        k_frnn<1><<<(int)blocks, kBlock, 0, s>>>(T, P.n, P.maxnb, x, y, z, hold, done, nullptr, count, st);
+        k_vh_update<<<g, 256, 0, s>>>(P.n, count, h, done, nit, target, tol, max_iter, P.maxnb);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int sph_density_eos(const SphParams& P, const SphSorted& S, const int* nbr, const int* noi, const int* perm,
+                    double* rho_out, double* p_out, double* cs_out, DevStatus* st, cudaStream_t s) {
+    if (P.n <= 0) return MHPC_OK;
+    k_density_eos<<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(P, S, nbr, noi, perm, rho_out, p_out, cs_out, st);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int sph_forces(const SphParams& P, const SphSorted& S, const int* nbr, const int* noi, const int* perm, double* ax,
+               double* ay, double* az, double* drhodt, double* dedt, double* dsmldt, DevStatus* st, cudaStream_t s) {
+    if (P.n <= 0) return MHPC_OK;
+    k_forces<<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(P, S, nbr, noi, perm, ax, ay, az, drhodt, dedt, dsmldt,
+                                                           st);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int sph_export_nnl(const SphParams& P, const int* nbr, const int* noi, const int* perm, int* nnl, int* noi_out,
+                   cudaStream_t s) {
+    if (P.n <= 0) return MHPC_OK;
+    k_export_nnl<<<grid_for(P.n, 256, 148 * 16), 256, 0, s>>>(P.n, P.maxnb, nbr, noi, perm, nnl, noi_out);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}

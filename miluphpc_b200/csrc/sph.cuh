@@ -1,0 +1,54 @@
+#pragma once
+#include "tree.cuh"
+
+#define MHPC_MAX_MATERIALS 8
+
+struct MatDev {
+    int eos_type;
+    int interactions;
+    double alpha, beta;
+    double K, gamma, rho0, bulk, n_exp, shear;
+    double cs_init;  // sound speed set by initializeSoundSpeed (Murnaghan, isothermal)
+};
+
+struct SphParams {
+    int n;
+    int maxnb;             // max_num_interactions (list stride per particle)
+    int kernel;            // 0 spiky, 1 cubic spline, 2 wendlandc2, 3 wendlandc4, 4 wendlandc6
+    int avg_h;             // h_bar = (h_i + h_j)/2 (variable_sml || integrate_sml)
+    int integrate_energy;
+    int integrate_sml;
+    int integrate_density; // density from state (no kernel sum)
+    int num_materials;
+    int mixed;             // FP32 pair sums on group-relative coordinates
+    MatDev mat[MHPC_MAX_MATERIALS];
+};
+
+// Sorted-order views of the SPH state.
+struct SphSorted {
+    const double *x, *y, *z, *m, *h;
+    const double *vx, *vy, *vz, *e;
+    const int* mat;        // may be null
+    double *rho, *p, *cs;  // sorted outputs of the density/EOS pass (p, cs hold previous values on entry)
+};
+
+// Neighbour lists in sorted index space, group-transposed:
+// nbr[((s >> 5) * maxnb + k) * 32 + (s & 31)], count noi[s].
+int sph_frnn(const TreeDev& T, const SphParams& P, const SphSorted& S, int* nbr, int* noi, DevStatus* st,
+             cudaStream_t s);
+// Plain variable-h iteration (Jacobi form of fixedRadiusNN_variableSML):
+// updates h (sorted, in place) for up to `sweeps` sweeps; `done` marks converged
+// particles (caller zeroes it before the first sweep; predictor-accepted
+// particles can be pre-marked), hold/htry are scratch [n].
+int sph_variable_h(const TreeDev& T, const SphParams& P, const double* x, const double* y, const double* z,
+                   double* h, double* hold, int* done, int* nit, int* count, int target, int tol, int max_iter,
+                   int sweeps, DevStatus* st, cudaStream_t s);
+int sph_density_eos(const SphParams& P, const SphSorted& S, const int* nbr, const int* noi, const int* perm,
+                    double* rho_out, double* p_out, double* cs_out, DevStatus* st, cudaStream_t s);
+int sph_forces(const SphParams& P, const SphSorted& S, const int* nbr, const int* noi, const int* perm,
+               double* ax, double* ay, double* az, double* drhodt, double* dedt, double* dsmldt, DevStatus* st,
+               cudaStream_t s);
+// Scatter the sorted neighbour lists into the reference layout
+// nnl[i * maxnb + k] (original indices) and noi[i].
+int sph_export_nnl(const SphParams& P, const int* nbr, const int* noi, const int* perm, int* nnl, int* noi_out,
+                   cudaStream_t s);

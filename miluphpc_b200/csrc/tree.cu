@@ -1,0 +1,275 @@
+// Tree construction from sorted keys and the bottom-up moment pass.
+//
+// Node set: equal, as a set of (key prefix, level), to the reference's
+// buildTree result (src/subdomain_key_tree/tree.cu:768-1082); node numbering
+// is depth-first pre-order instead of atomic insertion order.  Centres of mass
+// follow calculateCentersOfMass (tree.cu:1416-1497): m = sum of child masses,
+// x = sum(x_c m_c) / m over the children in curve order, computed with
+// explicitly rounded FP64 multiplies and adds (the reference builds with
+// -fmad=false) so that Lebesgue-ordered results match it bit for bit.  The
+// reference runs one launch per level (21 launches, miluphpc.cpp:1205-1210);
+// here one launch climbs from every leaf and the last child to arrive at a
+// cell computes it.
+#include "tree.cuh"
+
+namespace {
+
+__device__ __forceinline__ int dl_at(const unsigned char* dl, int i) { return i >= 0 ? (int)dl[i] : 0; }
+
+__global__ void __launch_bounds__(256) k_lcp(const uint64_t* __restrict__ k, int n, unsigned char* dl, int* cnt,
+                                             DevStatus* st) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int d = 0;
+        if (i + 1 < n) {
+            uint64_t x = __ldg(k + i) ^ __ldg(k + i + 1);
+            d = x == 0 ? MHPC_MAX_LEVEL : (__clzll((long long)x) - 1) / 3;
+            if (d > MHPC_MAX_LEVEL) d = MHPC_MAX_LEVEL;
+            if (x == 0) atomicAdd(&st->key_collisions, 1);
+        }
+        dl[i] = (unsigned char)d;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_count(const unsigned char* __restrict__ dl, int n, int* cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        int dp = dl_at(dl, i - 1), dc = dl[i];
+        cnt[i] = (dc > dp ? dc - dp : 0) + 1;
+    }
+}
+
+// last j in [a, n) whose key shares the prefix (key >> sh) == pref
+__device__ int gallop_fwd(const uint64_t* __restrict__ k, int a, int n, uint64_t pref, int sh) {
+    int lo = a, hi, step = 1;
+    for (;;) {
+        long h = (long)lo + step;
+        if (h >= n || (__ldg(k + h) >> sh) != pref) { hi = (int)(h < n ? h : n); break; }
+        lo = (int)h;
+        step <<= 1;
+    }
+    while (hi - lo > 1) {
+        int mid = lo + ((hi - lo) >> 1);
+        if ((__ldg(k + mid) >> sh) == pref) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// first j in [0, a] whose key shares the prefix
+__device__ int gallop_back(const uint64_t* __restrict__ k, int a, uint64_t pref, int sh) {
+    int hi = a, lo, step = 1;
+    for (;;) {
+        long l = (long)hi - step;
+        if (l < 0 || (__ldg(k + l) >> sh) != pref) { lo = (int)(l < 0 ? -1 : l); break; }
+        hi = (int)l;
+        step <<= 1;
+    }
+    while (hi - lo > 1) {
+        int mid = lo + ((hi - lo) >> 1);
+        if ((__ldg(k + mid) >> sh) == pref) hi = mid; else lo = mid;
+    }
+    return hi;
+}
+
+__device__ __forceinline__ int cell_node(const int* off, const unsigned char* dl, int a, int L) {
+    return off[a] + (L - dl_at(dl, a - 1) - 1);
+}
+
+__global__ void __launch_bounds__(256) k_nodes(TreeDev T, const uint64_t* __restrict__ k, DevStatus* st) {
+    const int n = T.n;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+        const int dp = dl_at(T.dl, a - 1), dc = T.dl[a];
+        const int c = dc > dp ? dc - dp : 0;
+        const int o = T.off[a];
+        const uint64_t ka = __ldg(k + a);
+        for (int j = 0; j < c; ++j) {
+            const int L = dp + 1 + j;
+            const int node = o + j;
+            if (node >= T.cap_nodes) { set_status(st, MHPC_ERR_NODE_POOL, node); break; }
+            const int sh = 3 * (MHPC_MAX_LEVEL - L);
+            const int b = gallop_fwd(k, a, n, ka >> sh, sh);
+            int par;
+            if (j > 0) par = node - 1;
+            else if (L - 1 == 0) par = -1;
+            else {
+                const int sh2 = 3 * (MHPC_MAX_LEVEL - (L - 1));
+                const int a2 = gallop_back(k, a, ka >> sh2, sh2);
+                par = cell_node(T.off, T.dl, a2, L - 1);
+            }
+            T.link[node] = make_int2(T.off[b + 1], L);
+            T.first[node] = a;
+            T.last[node] = b;
+            T.parent[node] = par;
+            T.arrive[node] = 0;
+            if (par >= T.cap_nodes) set_status(st, MHPC_ERR_NODE_POOL, par);
+            else if (par >= 0) atomicAdd(&T.nchild[par], 1);
+            else atomicAdd(T.root_nchild, 1);
+        }
+        const int node = o + c;
+        if (node >= T.cap_nodes) { set_status(st, MHPC_ERR_NODE_POOL, node); continue; }
+        const int P = dp > dc ? dp : dc;
+        int par;
+        if (P == 0) par = -1;
+        else if (dc > dp) par = node - 1;
+        else {
+            const int sh2 = 3 * (MHPC_MAX_LEVEL - P);
+            const int a2 = gallop_back(k, a, ka >> sh2, sh2);
+            par = cell_node(T.off, T.dl, a2, P);
+        }
+        T.link[node] = make_int2(node + 1, (P + 1) | ND_LEAF);
+        T.first[node] = a;
+        T.last[node] = a;
+        T.parent[node] = par;
+        T.nchild[node] = 0;
+        T.leaf_node[a] = node;
+        if (par >= T.cap_nodes) set_status(st, MHPC_ERR_NODE_POOL, par);
+            else if (par >= 0) atomicAdd(&T.nchild[par], 1);
+            else atomicAdd(T.root_nchild, 1);
+        if (P + 1 > MHPC_MAX_LEVEL) atomicMax(&st->max_level, P + 1);
+    }
+}
+
+__global__ void k_zero_cells(TreeDev T) {
+    // nchild of cells must be zero before k_nodes counts; cells are the
+    // non-leaf nodes, whose ids are unknown before the scan, so clear all.
+    int total = *T.nodes;
+    if (total > T.cap_nodes) total = T.cap_nodes;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        T.nchild[i] = 0;
+        T.arrive[i] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *T.root_nchild = 0;
+}
+
+__global__ void k_copy_total(TreeDev T) { *T.nodes = T.off[T.n]; }
+
+__device__ __forceinline__ double4 ldcg_d4(const double4* p) {
+    double4 v;
+    const double2* q = reinterpret_cast<const double2*>(p);
+    double2 a = __ldcg(q), b = __ldcg(q + 1);
+    v.x = a.x; v.y = a.y; v.z = b.x; v.w = b.y;
+    return v;
+}
+
+__device__ __forceinline__ float rd(double v) { return __double2float_rd(v); }
+__device__ __forceinline__ float ru(double v) { return __double2float_ru(v); }
+
+__global__ void __launch_bounds__(256) k_upward(TreeDev T, const double* __restrict__ sx,
+                                                const double* __restrict__ sy, const double* __restrict__ sz,
+                                                const double* __restrict__ sm, int want_quad,
+                                                const DevStatus* st) {
+    if (st->code) return;
+    const int n = T.n;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
+        const int leaf = T.leaf_node[a];
+        const double px = __ldg(sx + a), py = __ldg(sy + a), pz = __ldg(sz + a), pm = __ldg(sm + a);
+        T.com[leaf] = make_double4(px, py, pz, pm);
+        T.bmin[leaf] = make_float4(rd(px), rd(py), rd(pz), 0.f);
+        T.bmax[leaf] = make_float4(ru(px), ru(py), ru(pz), 0.f);
+        if (want_quad) {
+            T.quad0[leaf] = make_float4(0.f, 0.f, 0.f, 0.f);
+            T.quad1[leaf] = make_float2(0.f, 0.f);
+        }
+        int p = T.parent[leaf];
+        while (p >= 0) {
+            __threadfence();
+            const int old = atomicAdd(&T.arrive[p], 1);
+            if (old != T.nchild[p] - 1) break;
+            __threadfence();
+            const int end = T.link[p].x;
+            double m = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+            float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+            float4 hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+            for (int c = p + 1; c < end; c = __ldcg(&T.link[c].x)) {
+                const double4 cc = ldcg_d4(&T.com[c]);
+                mx = __dadd_rn(mx, __dmul_rn(cc.x, cc.w));
+                my = __dadd_rn(my, __dmul_rn(cc.y, cc.w));
+                mz = __dadd_rn(mz, __dmul_rn(cc.z, cc.w));
+                m = __dadd_rn(m, cc.w);
+                const float4 bl = __ldcg(&T.bmin[c]), bh = __ldcg(&T.bmax[c]);
+                lo.x = fminf(lo.x, bl.x); lo.y = fminf(lo.y, bl.y); lo.z = fminf(lo.z, bl.z);
+                hi.x = fmaxf(hi.x, bh.x); hi.y = fmaxf(hi.y, bh.y); hi.z = fmaxf(hi.z, bh.z);
+            }
+            if (m > 0.0) {
+                mx = __ddiv_rn(mx, m);
+                my = __ddiv_rn(my, m);
+                mz = __ddiv_rn(mz, m);
+            }
+            T.com[p] = make_double4(mx, my, mz, m);
+            T.bmin[p] = lo;
+            T.bmax[p] = hi;
+            if (want_quad) {
+                double q[6] = {0, 0, 0, 0, 0, 0};
+                for (int c = p + 1; c < end; c = __ldcg(&T.link[c].x)) {
+                    const double4 cc = ldcg_d4(&T.com[c]);
+                    const double s0 = cc.x - mx, s1 = cc.y - my, s2 = cc.z - mz;
+                    const double ss = s0 * s0 + s1 * s1 + s2 * s2;
+                    const double w = cc.w;
+                    q[0] += w * (3.0 * s0 * s0 - ss);
+                    q[1] += w * 3.0 * s0 * s1;
+                    q[2] += w * 3.0 * s0 * s2;
+                    q[3] += w * (3.0 * s1 * s1 - ss);
+                    q[4] += w * 3.0 * s1 * s2;
+                    q[5] += w * (3.0 * s2 * s2 - ss);
+                    if (!(__ldcg(&T.link[c].y) & ND_LEAF)) {
+                        const float4 a0 = __ldcg(&T.quad0[c]);
+                        const float2 a1 = __ldcg(&T.quad1[c]);
+                        q[0] += a0.x; q[1] += a0.y; q[2] += a0.z; q[3] += a0.w; q[4] += a1.x; q[5] += a1.y;
+                    }
+                }
+                T.quad0[p] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+                T.quad1[p] = make_float2((float)q[4], (float)q[5]);
+            }
+            p = T.parent[p];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) k_mixed_nodes(TreeDev T, const long long* ord, double inv_theta,
+                                                     const DevStatus* st) {
+    if (st->code) return;
+    const double edge0 = ord_to_dbl(ord[1]) - ord_to_dbl(ord[0]);
+    int total = *T.nodes;
+    if (total > T.cap_nodes) total = T.cap_nodes;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        const double4 c = T.com[i];
+        const int info = T.link[i].y;
+        const float hx = (float)c.x, hy = (float)c.y, hz = (float)c.z;
+        float crit = -1.f;
+        if (!(info & ND_LEAF)) {
+            const double e = ldexp(edge0, -(info & 0xff));
+            crit = (float)(e * e * inv_theta);
+        }
+        T.mpos[i] = make_float4(hx, hy, hz, (float)c.w);
+        T.mlo[i] = make_float4((float)(c.x - (double)hx), (float)(c.y - (double)hy), (float)(c.z - (double)hz), crit);
+    }
+}
+
+}  // namespace
+
+int tree_build(TreeDev& T, const uint64_t* skey, void* scan_scratch, DevStatus* st, cudaStream_t s) {
+    const int n = T.n;
+    if (n <= 0) return MHPC_ERR_ARG;
+    const int g = grid_for(n, 256, 148 * 16);
+    k_lcp<<<g, 256, 0, s>>>(skey, n, T.dl, T.cnt, st);
+    k_count<<<g, 256, 0, s>>>(T.dl, n, T.cnt);
+    CUDA_TRY(cudaGetLastError());
+    int rc = scan_exclusive_i32(T.cnt, T.off, n, scan_scratch, s);
+    if (rc) return rc;
+    k_copy_total<<<1, 1, 0, s>>>(T);
+    k_zero_cells<<<148 * 8, 256, 0, s>>>(T);
+    k_nodes<<<g, 256, 0, s>>>(T, skey, st);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int tree_upward(TreeDev& T, const double* sx, const double* sy, const double* sz, const double* sm,
+                int want_quad, DevStatus* st, cudaStream_t s) {
+    k_upward<<<grid_for(T.n, 256, 148 * 16), 256, 0, s>>>(T, sx, sy, sz, sm, want_quad, st);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int tree_mixed_nodes(TreeDev& T, const long long* ord, double theta, const DevStatus* st, cudaStream_t s) {
+    k_mixed_nodes<<<148 * 8, 256, 0, s>>>(T, ord, 1.0 / theta, st);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}

@@ -1,0 +1,364 @@
+"""Parity of the CUDA path (through the C ABI) with the FP64 oracle.
+
+Bars: SFC keys and sort permutation bit-exact; tree node set equal as a set
+of (key prefix, level); Lebesgue-order centres of mass bit-exact; v2 gravity
+within 1e-9 relative of the oracle's v2 emulation (same accept decisions,
+different rsqrt and summation order); neighbour sets equal; SPH density,
+pressure, sound speed and forces within 1e-10 relative; the mixed FP32 walk
+within 2e-4 (p99) of its FP64 statement and p99 <= 1e-3 against FP64 direct
+summation.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from miluphpc_b200 import _lib, ics
+from miluphpc_b200.miluphpc import Miluphpc, direct_gravity, material
+from oracle import oracle as O
+from tests.helpers import gravity_cfg, nodeset_pairs, rel_err, sph_cfg
+
+pytestmark = pytest.mark.gpu
+
+L = None
+
+
+def lib():
+    global L
+    if L is None:
+        L = _lib.load()
+    return L
+
+
+def dptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def gpu_keys(x, y, z, curve):
+    dev = torch.device("cuda:0")
+    tx, ty, tz = (torch.as_tensor(a, device=dev) for a in (x, y, z))
+    bb = torch.zeros(6, dtype=torch.float64, device=dev)
+    keys = torch.zeros(len(x), dtype=torch.int64, device=dev)
+    s = torch.cuda.current_stream().cuda_stream
+    _lib.check(lib().mhpc_bbox(dptr(tx), dptr(ty), dptr(tz), len(x), dptr(bb), ctypes.c_void_p(s)), "bbox")
+    _lib.check(lib().mhpc_keys(dptr(tx), dptr(ty), dptr(tz), len(x), dptr(bb), curve, dptr(keys),
+                               ctypes.c_void_p(s)), "keys")
+    torch.cuda.synchronize()
+    return bb.cpu().numpy(), keys.cpu().numpy().view(np.uint64)
+
+
+def gpu_sort(keys, vals=None):
+    dev = torch.device("cuda:0")
+    n = len(keys)
+    kin = torch.as_tensor(np.asarray(keys, dtype=np.uint64).view(np.int64), device=dev)
+    vin = torch.as_tensor(np.asarray(vals, dtype=np.int32), device=dev) if vals is not None else None
+    kout = torch.zeros(max(n, 1), dtype=torch.int64, device=dev)
+    vout = torch.zeros(max(n, 1), dtype=torch.int32, device=dev)
+    nb = lib().mhpc_sort_scratch_bytes(n)
+    scratch = torch.zeros(max(nb, 1), dtype=torch.uint8, device=dev)
+    s = torch.cuda.current_stream().cuda_stream
+    rc = lib().mhpc_sort_pairs(dptr(kin), dptr(vin) if vin is not None else None, dptr(kout), dptr(vout), n,
+                               dptr(scratch), nb, ctypes.c_void_p(s))
+    _lib.check(rc, "sort")
+    torch.cuda.synchronize()
+    status = int(scratch[nb - 256:nb - 252].view(torch.int32).item()) if n > 0 else 0
+    assert status == 0
+    return kout.cpu().numpy()[:n].view(np.uint64), vout.cpu().numpy()[:n]
+
+
+@pytest.mark.parametrize("curve", [0, 1])
+@pytest.mark.parametrize("n", [1, 33, 100_000])
+def test_keys_bit_exact(curve, n, cuda):
+    P = ics.plummer(max(n, 2), seed=11)
+    x, y, z = P["x"][:n], P["y"][:n], P["z"][:n]
+    bb, k = gpu_keys(x, y, z, curve)
+    obb = O.bbox(x, y, z)
+    assert np.array_equal(bb, obb)
+    ok = O.keys(x, y, z, obb, curve)
+    assert np.array_equal(k, ok)
+
+
+def test_keys_edge_values(cuda):
+    # points on midpoints, on the box faces, at the origin, negative zero
+    pts = np.array([[0.0, 0.0, 0.0], [1.0, 1.0, 1.0], [-1.0, -1.0, -1.0], [0.5, -0.5, 0.25],
+                    [-0.0, 1e-300, -1e-300], [1.0, -1.0, 0.0], [0.999999999999, -0.999999999999, 0.5]])
+    x, y, z = pts[:, 0].copy(), pts[:, 1].copy(), pts[:, 2].copy()
+    for curve in (0, 1):
+        bb, k = gpu_keys(x, y, z, curve)
+        assert np.array_equal(k, O.keys(x, y, z, O.bbox(x, y, z), curve))
+
+
+@pytest.mark.parametrize("n", [0, 1, 31, 4097, 300_001])
+def test_sort_random(n, cuda):
+    rng = np.random.default_rng(n + 3)
+    keys = rng.integers(0, 2 ** 63 - 1, size=n, dtype=np.int64).astype(np.uint64)
+    ks, perm = gpu_sort(keys)
+    oks, operm = O.sort(keys)
+    assert np.array_equal(ks, oks)
+    assert np.array_equal(perm, operm)
+
+
+def test_sort_duplicates_stable(cuda):
+    rng = np.random.default_rng(9)
+    n = 200_000
+    keys = rng.integers(0, 50, size=n).astype(np.uint64) << np.uint64(40)
+    vals = rng.permutation(n).astype(np.int32)
+    ks, vs = gpu_sort(keys, vals)
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(ks, keys[order])
+    assert np.array_equal(vs, vals[order])
+
+
+def test_sort_all_equal_and_sorted(cuda):
+    n = 70_000
+    ks, perm = gpu_sort(np.full(n, 12345, dtype=np.uint64))
+    assert np.array_equal(perm, np.arange(n))
+    keys = np.arange(n, dtype=np.uint64) * np.uint64(977)
+    ks, perm = gpu_sort(keys[::-1].copy())
+    assert np.array_equal(ks, keys)
+
+
+def _node_map(child, n):
+    """(prefix, level) -> node id for a reference-layout child array."""
+    out = {}
+    stack = [(child[c], c, 1) for c in range(8) if child[c] >= n]
+    while stack:
+        node, pre, lev = stack.pop()
+        out[(pre, lev)] = node
+        for c in range(8):
+            ch = child[8 * node + c]
+            if ch >= n:
+                stack.append((ch, (pre << 3) | c, lev + 1))
+    return out
+
+
+@pytest.mark.parametrize("curve", [0, 1])
+def test_tree_nodeset_and_com(curve, cuda):
+    n = 50_000
+    P = ics.plummer(n, seed=21)
+    cfg = gravity_cfg(sfc=curve)
+    sim = Miluphpc(cfg, P)
+    sim.rhs(0)
+    keys, perm = sim.export_sorted()
+    bb = O.bbox(P["x"], P["y"], P["z"])
+    ok = O.keys(P["x"], P["y"], P["z"], bb, curve)
+    oks, operm = O.sort(ok)
+    assert np.array_equal(keys, oks)
+    assert np.array_equal(perm, operm)
+    T = O.Tree(P["x"], P["y"], P["z"], P["mass"], bb)
+    tr = sim.export_tree(T.num_nodes)
+    assert tr["cells"] == T.nodes - n
+    gmap = _node_map(tr["child"], n)
+    omap = _node_map(T.child, n)
+    assert set(gmap) == set(omap)
+    # leaves attach to the same (prefix, level) cells, in the same octant
+    for key, gid in list(gmap.items())[:20000]:
+        oid = omap[key]
+        gch = tr["child"][8 * gid:8 * gid + 8]
+        och = T.child[8 * oid:8 * oid + 8]
+        assert np.array_equal(gch < n, och < n)
+        assert np.array_equal(np.where(gch < n, gch, -2), np.where(och < n, och, -2))
+    gid = np.array([gmap[k] for k in omap])
+    oid = np.array([omap[k] for k in omap])
+    gm, om = tr["m"][gid], T.m[oid]
+    gx, ox = tr["x"][gid], T.x[oid]
+    if curve == 0:
+        assert np.array_equal(gm, om)
+        assert np.array_equal(gx, ox)
+    else:
+        np.testing.assert_allclose(gm, om, rtol=1e-13)
+        np.testing.assert_allclose(gx, ox, rtol=1e-12, atol=1e-14)
+    lev_g = tr["level"][:n]
+    assert np.array_equal(lev_g, T.level[:n])
+    sim.close()
+
+
+@pytest.mark.parametrize("curve,theta", [(0, 0.5), (1, 0.7), (0, 0.1)])
+def test_gravity_v2_matches_oracle(curve, theta, cuda):
+    n = 65_536
+    P = ics.plummer(n, seed=5)
+    cfg = gravity_cfg(sfc=curve, theta=theta, smoothing=1e-4)
+    sim = Miluphpc(cfg, P)
+    sim.rhs(0)
+    gx, gy, gz = sim.numpy("g_ax"), sim.numpy("g_ay"), sim.numpy("g_az")
+    bb = O.bbox(P["x"], P["y"], P["z"])
+    T = O.Tree(P["x"], P["y"], P["z"], P["mass"], bb)
+    _, operm = O.sort(O.keys(P["x"], P["y"], P["z"], bb, curve))
+    radius = 0.5 * (bb[1] - bb[0])
+    ox, oy, oz = O.gravity_v2(T, operm, radius, theta, 1e-4)
+    e = rel_err(gx, gy, gz, ox, oy, oz)
+    assert e.max() < 1e-9, e.max()
+    st = sim.stats()
+    assert st["gravity_interactions"] > n
+    sim.close()
+
+
+def test_gravity_mixed_accuracy(cuda):
+    n = 131_072
+    P = ics.plummer(n, seed=1)
+    cfg = gravity_cfg(sfc=1, precision=1, theta_mixed=0.3, smoothing=1e-4)
+    sim = Miluphpc(cfg, P)
+    sim.rhs(0)
+    gx, gy, gz = sim.numpy("g_ax"), sim.numpy("g_ay"), sim.numpy("g_az")
+    rng = np.random.default_rng(7)
+    tg = rng.choice(n, 4096, replace=False)
+    dx, dy, dz, _ = O.direct(P["x"], P["y"], P["z"], P["mass"], tg, 1e-4)
+    e = rel_err(gx[tg], gy[tg], gz[tg], dx, dy, dz)
+    assert np.percentile(e, 99) <= 1e-3, np.percentile(e, 99)
+    # same algorithm in FP64 (oracle): FP32 + hi/lo split costs little
+    bb = O.bbox(P["x"], P["y"], P["z"])
+    T = O.Tree(P["x"], P["y"], P["z"], P["mass"], bb)
+    q = O.quad(T)
+    _, operm = O.sort(O.keys(P["x"], P["y"], P["z"], bb, 1))
+    ax, ay, az, _ = O.gravity_group(T, operm, 0.5 * (bb[1] - bb[0]), 0.3, 1e-4, q=q)
+    e2 = rel_err(gx, gy, gz, ax, ay, az)
+    assert np.percentile(e2, 99) < 2e-4, np.percentile(e2, 99)
+    # GPU direct summation agrees with the oracle's
+    t = {k: torch.as_tensor(P[k], device="cuda:0") for k in ("x", "y", "z", "mass")}
+    ggx, ggy, ggz = direct_gravity(t["x"], t["y"], t["z"], t["mass"],
+                                   torch.as_tensor(tg.astype(np.int32), device="cuda:0"), 1e-4)
+    e3 = rel_err(ggx.cpu().numpy(), ggy.cpu().numpy(), ggz.cpu().numpy(), dx, dy, dz)
+    assert e3.max() < 1e-12
+    sim.close()
+
+
+def _sedov_state(nside, seed=5, vel=0.05):
+    S = ics.sedov(nside=nside, seed=seed)
+    rng = np.random.default_rng(seed)
+    n = len(S["x"])
+    for k in ("vx", "vy", "vz"):
+        S[k] = rng.normal(0.0, vel, n)
+    S["p"] = np.zeros(n)
+    S["cs"] = np.zeros(n)
+    return S
+
+
+def test_sph_sedov_matches_oracle(cuda):
+    S = _sedov_state(24)
+    n = len(S["x"])
+    cfg = sph_cfg()
+    mat = material(interactions=60, alpha=1.0, beta=2.0, eos_type=9, gamma=5.0 / 3.0)
+    sim = Miluphpc(cfg, S, materials=[mat], want_nnl=True)
+    # two calls: the first sets p, the second's ideal-gas c_s uses it (reference order)
+    p_prev = np.zeros(n)
+    for call in range(2):
+        sim.rhs(call)
+        off, nbr = O.frnn(S["x"], S["y"], S["z"], S["sml"])
+        noi = sim.numpy("noi")
+        assert np.array_equal(noi, np.diff(off))
+        nnl = sim.t["nnl"].cpu().numpy().reshape(n, cfg.max_num_interactions)
+        for i in range(0, n, 97):
+            got = np.sort(nnl[i, :noi[i]])
+            assert np.array_equal(got, nbr[off[i]:off[i + 1]])
+        rho = O.density(S["x"], S["y"], S["z"], S["mass"], S["sml"], off, nbr)
+        np.testing.assert_allclose(sim.numpy("rho"), rho, rtol=1e-12)
+        par = np.array([0.0, 5.0 / 3.0, 0.0, 0.0, 0.0])
+        p, cs = O.eos(9, par, rho, S["e"], p_prev)
+        np.testing.assert_allclose(sim.numpy("p"), p, rtol=1e-12, atol=1e-300)
+        np.testing.assert_allclose(sim.numpy("cs"), cs, rtol=1e-12, atol=1e-300)
+        ax, ay, az, drho, de, dh = O.forces(S["x"], S["y"], S["z"], S["vx"], S["vy"], S["vz"], S["mass"],
+                                            S["sml"], rho, p, cs, off, nbr, 1.0, 2.0)
+        scale = np.abs(np.stack([ax, ay, az])).max()
+        for got, ref in ((sim.numpy("ax"), ax), (sim.numpy("ay"), ay), (sim.numpy("az"), az)):
+            np.testing.assert_allclose(got, ref, rtol=1e-10, atol=1e-12 * scale)
+        np.testing.assert_allclose(sim.numpy("drhodt"), drho, rtol=1e-10, atol=1e-12 * np.abs(drho).max())
+        np.testing.assert_allclose(sim.numpy("dedt"), de, rtol=1e-10, atol=1e-12 * np.abs(de).max())
+        p_prev = p
+    sim.close()
+
+
+def test_variable_h_matches_oracle(cuda):
+    C = ics.rotating_cloud(20_000, seed=4)
+    n = len(C["x"])
+    C["sml"] = C["sml"] * np.random.default_rng(2).uniform(0.7, 1.4, n)
+    cfg = sph_cfg(variable_sml=1, integrate_energy=0)
+    mat = material(interactions=60, eos_type=0, K=C["cs2"], gamma=1.0)
+    S = dict(C)
+    S["p"] = np.zeros(n)
+    S["cs"] = np.zeros(n)
+    sim = Miluphpc(cfg, S, materials=[mat])
+    sim.rhs(0)
+    h_gpu = sim.numpy("sml")
+    h_orc, cnt, sweeps = O.variable_h(C["x"], C["y"], C["z"], C["sml"], 60, tol=5, max_nb=180, max_iter=5)
+    close = np.abs(h_gpu - h_orc) <= 1e-12 * h_orc
+    assert close.mean() > 0.999, close.mean()
+    sim.close()
+
+
+def test_leapfrog_steps_match_oracle(cuda):
+    n = 16_384
+    P = ics.plummer(n, seed=8)
+    cfg = gravity_cfg(theta=0.5, smoothing=1e-4, integrator=2, time_step=0.025)
+    sim = Miluphpc(cfg, P)
+    for step in range(3):
+        sim.integrate(step)
+    # oracle: initial rhs, then (updateX, rhs, updateV) per step
+    x, y, z = P["x"].copy(), P["y"].copy(), P["z"].copy()
+    vx, vy, vz = P["vx"].copy(), P["vy"].copy(), P["vz"].copy()
+
+    def rhs():
+        bb = O.bbox(x, y, z)
+        T = O.Tree(x, y, z, P["mass"], bb)
+        _, perm = O.sort(O.keys(x, y, z, bb, 0))
+        return O.gravity_v2(T, perm, 0.5 * (bb[1] - bb[0]), 0.5, 1e-4)
+
+    gx, gy, gz = rhs()
+    dt = 0.025
+    for step in range(3):
+        ox, oy, oz = gx.copy(), gy.copy(), gz.copy()
+        x += dt * (vx + 0.5 * dt * gx); y += dt * (vy + 0.5 * dt * gy); z += dt * (vz + 0.5 * dt * gz)
+        gx, gy, gz = rhs()
+        vx += 0.5 * dt * (gx + ox); vy += 0.5 * dt * (gy + oy); vz += 0.5 * dt * (gz + oz)
+    np.testing.assert_allclose(sim.numpy("x"), x, rtol=0, atol=1e-11)
+    np.testing.assert_allclose(sim.numpy("vx"), vx, rtol=0, atol=1e-10)
+    sim.close()
+
+
+def test_errors_are_status_codes(cuda):
+    n = 4096
+    P = ics.plummer(n, seed=3)
+    # non-finite position
+    Q = dict(P)
+    Q["x"] = P["x"].copy()
+    Q["x"][17] = np.nan
+    sim = Miluphpc(gravity_cfg(), Q)
+    with pytest.raises(_lib.MhpcError) as e:
+        sim.rhs(0)
+    assert e.value.code == 7
+    sim.close()
+    # capacity
+    sim = Miluphpc(gravity_cfg(), P, capacity=n)
+    sim._soa.n = n + 1
+    with pytest.raises(_lib.MhpcError) as e:
+        sim.rhs(0)
+    assert e.value.code == 3
+    sim._soa.n = n
+    sim.rhs(0)  # context still usable
+    sim.close()
+    # node pool too small
+    sim = Miluphpc(gravity_cfg(node_pool_factor=1e-9), ics.plummer(65_536, seed=2))
+    with pytest.raises(_lib.MhpcError) as e:
+        sim.rhs(0)
+    assert e.value.code == 4
+    sim.close()
+    # neighbour overflow
+    S = _sedov_state(16)
+    sim = Miluphpc(sph_cfg(max_num_interactions=8), S, materials=[material()])
+    with pytest.raises(_lib.MhpcError) as e:
+        sim.rhs(0)
+    assert e.value.code == 6
+    sim.close()
+
+
+def test_coincident_particles(cuda):
+    n = 10_000
+    P = ics.plummer(n, seed=4)
+    for k in ("x", "y", "z"):
+        P[k][5000:5010] = P[k][4000]
+    sim = Miluphpc(gravity_cfg(), P)
+    sim.rhs(0)
+    st = sim.stats()
+    assert st["key_collisions"] >= 10
+    assert np.isfinite(sim.numpy("g_ax")).all()
+    sim.close()
