@@ -45,7 +45,7 @@ def build(verbose=False, ptxas_info=False):
             continue
         cmd = [NVCC] + ARCH + CUFLAGS + ["-c", src, "-o", obj]
         if src.endswith(".cpp"):
-            cmd = [NVCC] + CUFLAGS + ["-x", "c++", "-c", src, "-o", obj]
+            cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-I" + INCLUDE, "-I" + CSRC, "-c", src, "-o", obj]
         elif ptxas_info:
             cmd += ["-Xptxas", "-v"]
         if verbose:

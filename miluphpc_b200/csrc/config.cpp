@@ -189,7 +189,7 @@ void mhpc_config_default(mhpc_config* c) {
     c->nb_tolerance = 5;
     c->max_sml_iterations = 5;
     c->precision = 0;
-    c->theta_mixed = 0.3;
+    c->theta_mixed = 0.25;
     c->softening_h_factor = 0.0;
     c->node_pool_factor = 1.0;
 }

@@ -92,11 +92,15 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_v2(const double4* __restric
 // lanes hold their position relative to c in FP32, nodes are stored as
 // float hi + float lo of the FP64 centre of mass, so node - c is formed as
 // (hi - c_hi) + (lo - c_lo) without losing the digits that FP32 absolute
-// coordinates would drop.  A cell is accepted for the whole group when
-// edge^2/theta <= dist(node, group box)^2 + eps2_min (the squared-ratio
-// criterion of the reference applied to the group's nearest point); accepted
-// cells add monopole + quadrupole terms.  FP32 partial sums are flushed into
-// FP64 every kFlush accepted nodes (compensated accumulation).
+// coordinates would drop.  A cell is accepted for the warp when every lane
+// has edge^2/theta <= |node - p|^2 + eps2 (the squared-ratio criterion with
+// computeForces_v2's warp vote, applied at every level); accepted cells add
+// monopole + quadrupole terms.  A box test per group would be cheaper per
+// node but opens the whole interior of a group box that straddles a curve
+// jump (Lebesgue order), which leaves single warps with tens of thousands of
+// leaf interactions; the per-lane vote keeps the cost of such a group at the
+// union of its parts.  FP32 partial sums are flushed into FP64 every kFlush
+// accepted nodes (compensated accumulation).
 constexpr int kFlush = 64;
 
 __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restrict__ mpos, const float4* __restrict__ mlo,
@@ -120,8 +124,8 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restr
     const double px = __ldg(sx + sl), py = __ldg(sy + sl), pz = __ldg(sz + sl);
     double e2d = P.eps2;
     if (P.h_factor > 0.0) { double e = P.h_factor * __ldg(sh + sl); e2d += e * e; }
-    // group bounding box
-    double lox = px, loy = py, loz = pz, hix = px, hiy = py, hiz = pz, e2min = e2d;
+    // group bounding box: its centre is the FP64 origin of the warp's FP32 frame
+    double lox = px, loy = py, loz = pz, hix = px, hiy = py, hiz = pz;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         lox = fmin(lox, __shfl_xor_sync(MHPC_FULL, lox, o));
@@ -130,15 +134,12 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restr
         hix = fmax(hix, __shfl_xor_sync(MHPC_FULL, hix, o));
         hiy = fmax(hiy, __shfl_xor_sync(MHPC_FULL, hiy, o));
         hiz = fmax(hiz, __shfl_xor_sync(MHPC_FULL, hiz, o));
-        e2min = fmin(e2min, __shfl_xor_sync(MHPC_FULL, e2min, o));
     }
     const double cx = 0.5 * (lox + hix), cy = 0.5 * (loy + hiy), cz = 0.5 * (loz + hiz);
-    const float hx = __double2float_ru(0.5 * (hix - lox)), hy = __double2float_ru(0.5 * (hiy - loy)),
-                hz = __double2float_ru(0.5 * (hiz - loz));
     const float chx = (float)cx, chy = (float)cy, chz = (float)cz;
     const float clx = (float)(cx - (double)chx), cly = (float)(cy - (double)chy), clz = (float)(cz - (double)chz);
     const float rx = (float)(px - cx), ry = (float)(py - cy), rz = (float)(pz - cz);
-    const float e2 = (float)e2d, e2g = (float)e2min;
+    const float e2 = (float)e2d;
     float fax = 0.f, fay = 0.f, faz = 0.f;
     double ax = 0.0, ay = 0.0, az = 0.0;
     int since = 0;
@@ -153,15 +154,9 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restr
         const float ny = (hp.y - chy) + (lp.y - cly);
         const float nz = (hp.z - chz) + (lp.z - clz);
         const bool leaf = lk.y & ND_LEAF;
-        bool acc = leaf;
-        if (!leaf) {
-            const float ex = fmaxf(fabsf(nx) - hx, 0.f), ey = fmaxf(fabsf(ny) - hy, 0.f),
-                        ez = fmaxf(fabsf(nz) - hz, 0.f);
-            acc = lp.w <= ex * ex + ey * ey + ez * ez + e2g;
-        }
-        if (!acc) { ++nd; continue; }
         const float Rx = rx - nx, Ry = ry - ny, Rz = rz - nz;
         const float r2 = fmaf(Rx, Rx, fmaf(Ry, Ry, fmaf(Rz, Rz, e2)));
+        if (!leaf && !__all_sync(MHPC_FULL, !valid || lp.w <= r2)) { ++nd; continue; }
         const float ri = r2 > 0.f ? rsqrtf(r2) : 0.f;
         const float ri2 = ri * ri;
         const float mri3 = hp.w * ri * ri2;

@@ -52,13 +52,11 @@ static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 static SortScratch carve(void* base, int n) {
     char* p = (char*)base;
     SortScratch s;
-    long ntiles = (n + kTile - 1) / kTile;
     s.keys_tmp = (uint64_t*)p; p += align256(sizeof(uint64_t) * (size_t)n);
     s.vals_tmp = (int*)p; p += align256(sizeof(int) * (size_t)n);
     s.hist = (unsigned*)p; p += align256(sizeof(unsigned) * kPasses * kRadix);
     s.tile_counter = (unsigned*)p; p += align256(sizeof(unsigned) * kPasses);
     s.look = (unsigned long long*)p;
-    (void)ntiles;
     return s;
 }
 
@@ -341,8 +339,9 @@ size_t sort_scratch_bytes(int n) {
 
 int sort_pairs_u64(const uint64_t* keys_in, const int* vals_in, uint64_t* keys_out, int* vals_out, int n,
                    void* scratch, size_t scratch_bytes, DevStatus* st, cudaStream_t s) {
-    if (n < 0 || !keys_in || !keys_out || !vals_out) return MHPC_ERR_ARG;
+    if (n < 0) return MHPC_ERR_ARG;
     if (n == 0) return MHPC_OK;
+    if (!keys_in || !keys_out || !vals_out) return MHPC_ERR_ARG;
     if (!scratch || scratch_bytes < sort_scratch_bytes(n)) return MHPC_ERR_ARG;
     SortScratch S = carve(scratch, n);
     long ntiles = ((long)n + kTile - 1) / kTile;

@@ -394,12 +394,14 @@ void orc_quad(const int* child, const int* level, int n, int nodes, int max_leve
 }
 
 // Group walk of the mixed path in FP64: groups of `gsize` consecutive sorted
-// particles; a cell at level L is accepted when
-//   edge_L^2 / theta <= dist(com, group box)^2 + eps2
-// (edge_L = 2 radius / 2^L), i.e. the reference's squared-ratio criterion
-// applied to the nearest point of the group's bounding box; accepted cells
-// add their monopole and, if q is given, quadrupole term.  Leaves are exact.
-// ninter (per particle) receives the number of accepted nodes.
+// particles; a cell at level L is accepted for the group when, for every
+// particle p of the group,
+//   edge_L^2 / theta <= |com - p|^2 + eps2
+// (edge_L = 2 radius / 2^L): the reference's squared-ratio criterion with
+// computeForces_v2's all-lanes vote, applied to every level (root children
+// included); accepted cells add their monopole and, if q is given,
+// quadrupole term.  Leaves are exact.  ninter (per particle) receives the
+// number of accepted nodes.
 void orc_gravity_group(const double* x, const double* y, const double* z, const double* mass,
                        const double* q, const int* child, const int* level, const int* sorted,
                        int n, int gsize, double radius, double theta, double eps2, double* gax,
@@ -409,23 +411,17 @@ void orc_gravity_group(const double* x, const double* y, const double* z, const 
     for (int g = 0; g < ngroups; ++g) {
         const int base = g * gsize;
         const int lanes = std::min(gsize, n - base);
-        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-        for (int l = 0; l < lanes; ++l) {
-            int s = sorted[base + l];
-            double p[3] = {x[s], y[s], z[s]};
-            for (int d = 0; d < 3; ++d) { lo[d] = std::min(lo[d], p[d]); hi[d] = std::max(hi[d], p[d]); }
-        }
         std::vector<int> stack;
         for (int i = 0; i < 8; ++i) if (child[i] != -1) stack.push_back(child[i]);
         std::vector<int> acc_nodes;
         while (!stack.empty()) {
             int nd = stack.back(); stack.pop_back();
             if (nd < n) { acc_nodes.push_back(nd); continue; }
-            double c[3] = {x[nd], y[nd], z[nd]};
-            double d2 = 0;
-            for (int d = 0; d < 3; ++d) {
-                double e = c[d] < lo[d] ? lo[d] - c[d] : (c[d] > hi[d] ? c[d] - hi[d] : 0.0);
-                d2 += e * e;
+            double d2 = 1e300;
+            for (int l = 0; l < lanes; ++l) {
+                int s = sorted[base + l];
+                double dx = x[nd] - x[s], dy = y[nd] - y[s], dz = z[nd] - z[s];
+                d2 = std::min(d2, dx * dx + dy * dy + dz * dz);
             }
             double edge = 2.0 * radius * std::ldexp(1.0, -level[nd]);
             if (edge * edge / theta <= d2 + eps2) { acc_nodes.push_back(nd); continue; }

@@ -197,7 +197,7 @@ def test_gravity_v2_matches_oracle(curve, theta, cuda):
 def test_gravity_mixed_accuracy(cuda):
     n = 131_072
     P = ics.plummer(n, seed=1)
-    cfg = gravity_cfg(sfc=1, precision=1, theta_mixed=0.3, smoothing=1e-4)
+    cfg = gravity_cfg(sfc=1, precision=1, theta_mixed=0.25, smoothing=1e-4)
     sim = Miluphpc(cfg, P)
     sim.rhs(0)
     gx, gy, gz = sim.numpy("g_ax"), sim.numpy("g_ay"), sim.numpy("g_az")
@@ -211,7 +211,7 @@ def test_gravity_mixed_accuracy(cuda):
     T = O.Tree(P["x"], P["y"], P["z"], P["mass"], bb)
     q = O.quad(T)
     _, operm = O.sort(O.keys(P["x"], P["y"], P["z"], bb, 1))
-    ax, ay, az, _ = O.gravity_group(T, operm, 0.5 * (bb[1] - bb[0]), 0.3, 1e-4, q=q)
+    ax, ay, az, _ = O.gravity_group(T, operm, 0.5 * (bb[1] - bb[0]), 0.25, 1e-4, q=q)
     e2 = rel_err(gx, gy, gz, ax, ay, az)
     assert np.percentile(e2, 99) < 2e-4, np.percentile(e2, 99)
     # GPU direct summation agrees with the oracle's
