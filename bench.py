@@ -31,6 +31,9 @@ WORKLOADS = {
     # Plummer at scale, precision form: N = 2^24, Hilbert keys, leapfrog dt 0.01
     "plummer16m": dict(kind="gravity", n=1 << 24, sfc=1, dt=0.01, eps2=1e-4, theta=0.5, theta_mixed=0.25,
                        theta_plain_matched=0.1, seed=1),
+    # profiling case of the walk: node data (~190 MB) larger than L2
+    "plummer2m": dict(kind="gravity", n=1 << 21, sfc=1, dt=0.01, eps2=1e-4, theta=0.5, theta_mixed=0.25,
+                      theta_plain_matched=0.1, seed=1),
     # the reference's own single-rank case: N = 131072, Lebesgue, leapfrog dt 0.025
     "plummer131k": dict(kind="gravity", n=131072, sfc=0, dt=0.025, eps2=1e-4, theta=0.5, theta_mixed=0.25,
                         theta_plain_matched=0.1, seed=1),
