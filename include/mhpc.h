@@ -146,6 +146,26 @@ size_t mhpc_sort_scratch_bytes(int n);
 int mhpc_sort_pairs(const uint64_t* keys_in, const int* vals_in, uint64_t* keys_out,
                     int* vals_out, int n, void* scratch, size_t scratch_bytes, void* stream);
 
+/* Sort without any device allocation.  No counterpart in the reference (its
+ * sortArray allocates temporary storage on every call).  For callers that
+ * cannot allocate device memory — applications whose own memory pool has
+ * reserved the GPU at start-up, so a cudaMalloc fails or fragments it, and
+ * services that forbid allocation after initialisation — this variant of
+ * mhpc_sort_pairs keeps its scratch in a fixed device array inside the
+ * library, sized for at most mhpc_sort_noalloc_max_n() (= 1048576) keys
+ * (about 16 MB, held on every GPU that loads the library until the process
+ * exits).  Larger n returns MHPC_ERR_CAPACITY.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture.  All calls share
+ * the one array, so calls whose work overlaps on the GPU (other streams, other
+ * host threads) race and must be serialised by the caller.  status_dev
+ * (optional, device int) receives MHPC_OK or MHPC_ERR_TIMEOUT in stream order.
+ * The caller still owns keys/values in and out; nothing is allocated or
+ * freed. */
+int mhpc_sort_noalloc_max_n(void);
+int mhpc_sort_pairs_noalloc(const uint64_t* keys_in, const int* vals_in, uint64_t* keys_out,
+                            int* vals_out, int n, int* status_dev, void* stream);
+
 /* ------------------------------------------------------------ the context */
 typedef struct mhpc_ctx mhpc_ctx;
 

@@ -102,6 +102,8 @@ def load():
     L.mhpc_sort_scratch_bytes.restype = ctypes.c_size_t
     L.mhpc_sort_pairs.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, ctypes.c_size_t,
                                   c_void_p]
+    L.mhpc_sort_noalloc_max_n.restype = c_int
+    L.mhpc_sort_pairs_noalloc.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p]
     L.mhpc_ctx_create.argtypes = [ctypes.POINTER(c_void_p), c_int, ctypes.POINTER(Config),
                                   ctypes.POINTER(Material), c_int]
     L.mhpc_ctx_destroy.argtypes = [c_void_p]
@@ -151,6 +153,7 @@ def default_config(**kw):
 EXPORTS = [
     "mhpc_status_string", "mhpc_version", "mhpc_config_default", "mhpc_config_from_info",
     "mhpc_materials_from_cfg", "mhpc_bbox", "mhpc_keys", "mhpc_sort_scratch_bytes", "mhpc_sort_pairs",
+    "mhpc_sort_noalloc_max_n", "mhpc_sort_pairs_noalloc",
     "mhpc_ctx_create", "mhpc_ctx_destroy", "mhpc_ctx_set_stream", "mhpc_ctx_set_config", "mhpc_rhs",
     "mhpc_rhs_async", "mhpc_ctx_status", "mhpc_integrate", "mhpc_integrate_host", "mhpc_stage_tree",
     "mhpc_stage_gravity", "mhpc_stage_sph", "mhpc_export_sorted", "mhpc_export_tree", "mhpc_get_stats",

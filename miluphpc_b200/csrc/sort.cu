@@ -10,6 +10,8 @@
 // caller-provided; nothing is allocated per call.  Sorting is stable, so equal
 // keys keep ascending input position, which is the contract of the CUB call it
 // replaces.
+#include <mutex>
+
 #include "common.cuh"
 
 namespace {
@@ -327,15 +329,17 @@ __global__ void k_scan_total(const int* __restrict__ in, int* out, int n) {
     else out[0] = 0;
 }
 
+constexpr size_t align256c(size_t b) { return (b + 255) & ~size_t(255); }
+
+constexpr size_t scratch_formula(long n) {
+    return align256c(sizeof(uint64_t) * (size_t)n) + align256c(sizeof(int) * (size_t)n) +
+           align256c(sizeof(unsigned) * kPasses * kRadix) + align256c(sizeof(unsigned) * kPasses) +
+           align256c(sizeof(unsigned long long) * kPasses * (size_t)(((n + kTile - 1) / kTile) < 1 ? 1 : ((n + kTile - 1) / kTile)) * kRadix);
+}
+
 }  // namespace
 
-size_t sort_scratch_bytes(int n) {
-    long ntiles = ((long)n + kTile - 1) / kTile;
-    if (ntiles < 1) ntiles = 1;
-    return align256(sizeof(uint64_t) * (size_t)n) + align256(sizeof(int) * (size_t)n) +
-           align256(sizeof(unsigned) * kPasses * kRadix) + align256(sizeof(unsigned) * kPasses) +
-           align256(sizeof(unsigned long long) * kPasses * ntiles * kRadix);
-}
+size_t sort_scratch_bytes(int n) { return scratch_formula(n); }
 
 int sort_pairs_u64(const uint64_t* keys_in, const int* vals_in, uint64_t* keys_out, int* vals_out, int n,
                    void* scratch, size_t scratch_bytes, DevStatus* st, cudaStream_t s) {
@@ -368,6 +372,70 @@ int sort_pairs_u64(const uint64_t* keys_in, const int* vals_in, uint64_t* keys_o
         CUDA_TRY(cudaGetLastError());
         kin = kout;
         vin = vout;
+    }
+    return MHPC_OK;
+}
+
+// ------------------------------------------------- sort without allocation
+// Some callers cannot allocate device memory: applications whose own pool
+// reserves the device's memory at start-up (a cudaMalloc would fail or
+// fragment it) and services that forbid allocation after initialisation.
+// For them mhpc_sort_pairs_noalloc keeps its scratch in this file-scope
+// device array, sized for kNoAllocMaxN keys.  Every GPU that loads the
+// library holds the array until the process exits.
+constexpr long kNoAllocMaxN = 1L << 20;
+constexpr size_t kNoAllocStatusBytes = 256;
+constexpr size_t kNoAllocBytes = scratch_formula(kNoAllocMaxN) + kNoAllocStatusBytes;
+static __device__ __align__(256) unsigned char g_noalloc_sort_scratch[kNoAllocBytes];
+
+namespace {
+
+__global__ void k_copy_status(const DevStatus* st, int* out) { *out = st->code; }
+
+// Device address of g_noalloc_sort_scratch on the current device.  The host
+// symbol is only a stand-in for the device array, so the address is looked up
+// once per device with that device current and cached.
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[256];
+
+int noalloc_scratch(void** out) {
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return MHPC_ERR_ARG;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_sort_scratch) != cudaSuccess || !p) return MHPC_ERR_CUDA;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return MHPC_OK;
+}
+
+}  // namespace
+
+extern "C" int mhpc_sort_noalloc_max_n(void) { return (int)kNoAllocMaxN; }
+
+extern "C" int mhpc_sort_pairs_noalloc(const uint64_t* keys_in, const int* vals_in, uint64_t* keys_out,
+                                       int* vals_out, int n, int* status_dev, void* stream) {
+    if (n < 0) return MHPC_ERR_ARG;
+    if (n > kNoAllocMaxN) return MHPC_ERR_CAPACITY;
+    cudaStream_t s = (cudaStream_t)stream;
+    void* base = nullptr;
+    int rc = noalloc_scratch(&base);
+    if (rc) return rc;
+    DevStatus* st = reinterpret_cast<DevStatus*>((char*)base + kNoAllocBytes - kNoAllocStatusBytes);
+    CUDA_TRY(cudaMemsetAsync(st, 0, sizeof(DevStatus), s));
+    if (n > 0) {
+        // sort_pairs_u64 clears the histograms, tile counters and look-back
+        // words it needs before its first kernel
+        rc = sort_pairs_u64(keys_in, vals_in, keys_out, vals_out, n, base, kNoAllocBytes - kNoAllocStatusBytes,
+                            st, s);
+        if (rc) return rc;
+    }
+    if (status_dev) {
+        k_copy_status<<<1, 1, 0, s>>>(st, status_dev);
+        CUDA_TRY(cudaGetLastError());
     }
     return MHPC_OK;
 }
