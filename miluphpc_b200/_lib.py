@@ -7,7 +7,7 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libmhpc.so")
+LIB_PATH = os.environ.get("MHPC_LIBRARY") or os.path.join(HERE, "libmhpc.so")
 
 c_int, c_double, c_float, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_float, ctypes.c_void_p
 P_d = ctypes.POINTER(ctypes.c_double)

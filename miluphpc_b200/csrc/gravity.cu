@@ -11,6 +11,9 @@
 namespace {
 
 constexpr int kWalkBlock = 128;
+#ifndef MHPC_MIXED_PPL
+#define MHPC_MIXED_PPL 2
+#endif
 
 // --------------------------------------------------------------- plain v2
 // computeForces_v2 semantics: a child is accepted if it is a leaf or if every
@@ -103,6 +106,11 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_v2(const double4* __restric
 // accepted nodes (compensated accumulation).
 constexpr int kFlush = 64;
 
+// PPL particles per lane: a warp takes 32 * PPL consecutive sorted particles;
+// each visited node is loaded, placed in the warp frame and voted on once for
+// all of them, which amortises the per-node instructions over PPL
+// interactions (the kernel is issue-bound, not memory-bound).
+template <int PPL>
 __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restrict__ mpos, const float4* __restrict__ mlo,
                                                            const float4* __restrict__ q0, const float2* __restrict__ q1,
                                                            const int2* __restrict__ link, const int* __restrict__ nodes_total,
@@ -115,17 +123,25 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restr
     const int M = *nodes_total;
     const int lane = threadIdx.x & 31;
     const long gwarp = ((long)blockIdx.x * kWalkBlock + threadIdx.x) >> 5;
-    const long ngroups = ((long)P.n + 31) >> 5;
+    const long ngroups = ((long)P.n + 32 * PPL - 1) / (32 * PPL);
     if (gwarp >= ngroups) return;
-    const long s0 = gwarp * 32;
-    const long s = s0 + lane;
-    const bool valid = s < P.n;
-    const long sl = valid ? s : (long)P.n - 1;
-    const double px = __ldg(sx + sl), py = __ldg(sy + sl), pz = __ldg(sz + sl);
-    double e2d = P.eps2;
-    if (P.h_factor > 0.0) { double e = P.h_factor * __ldg(sh + sl); e2d += e * e; }
+    const long s0 = gwarp * 32 * PPL;
+    long s[PPL];
+    bool valid[PPL];
+    double px[PPL], py[PPL], pz[PPL], e2d[PPL];
+    double lox = 1e300, loy = 1e300, loz = 1e300, hix = -1e300, hiy = -1e300, hiz = -1e300;
+#pragma unroll
+    for (int k = 0; k < PPL; ++k) {
+        s[k] = s0 + k * 32 + lane;
+        valid[k] = s[k] < P.n;
+        const long sl = valid[k] ? s[k] : (long)P.n - 1;
+        px[k] = __ldg(sx + sl); py[k] = __ldg(sy + sl); pz[k] = __ldg(sz + sl);
+        e2d[k] = P.eps2;
+        if (P.h_factor > 0.0) { const double e = P.h_factor * __ldg(sh + sl); e2d[k] += e * e; }
+        lox = fmin(lox, px[k]); loy = fmin(loy, py[k]); loz = fmin(loz, pz[k]);
+        hix = fmax(hix, px[k]); hiy = fmax(hiy, py[k]); hiz = fmax(hiz, pz[k]);
+    }
     // group bounding box: its centre is the FP64 origin of the warp's FP32 frame
-    double lox = px, loy = py, loz = pz, hix = px, hiy = py, hiz = pz;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         lox = fmin(lox, __shfl_xor_sync(MHPC_FULL, lox, o));
@@ -138,12 +154,17 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restr
     const double cx = 0.5 * (lox + hix), cy = 0.5 * (loy + hiy), cz = 0.5 * (loz + hiz);
     const float chx = (float)cx, chy = (float)cy, chz = (float)cz;
     const float clx = (float)(cx - (double)chx), cly = (float)(cy - (double)chy), clz = (float)(cz - (double)chz);
-    const float rx = (float)(px - cx), ry = (float)(py - cy), rz = (float)(pz - cz);
-    const float e2 = (float)e2d;
-    float fax = 0.f, fay = 0.f, faz = 0.f;
-    double ax = 0.0, ay = 0.0, az = 0.0;
+    float rx[PPL], ry[PPL], rz[PPL], e2[PPL], fax[PPL], fay[PPL], faz[PPL];
+    double ax[PPL], ay[PPL], az[PPL];
+#pragma unroll
+    for (int k = 0; k < PPL; ++k) {
+        rx[k] = (float)(px[k] - cx); ry[k] = (float)(py[k] - cy); rz[k] = (float)(pz[k] - cz);
+        e2[k] = (float)e2d[k];
+        fax[k] = fay[k] = faz[k] = 0.f;
+        ax[k] = ay[k] = az[k] = 0.0;
+    }
     int since = 0;
-    unsigned long long ninter = 0, nvisit = 0, nquad = 0;
+    unsigned ninter = 0, nvisit = 0, nquad = 0;
     int nd = 0;
     while (nd < M) {
         const float4 hp = __ldg(mpos + nd);
@@ -154,47 +175,63 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restr
         const float ny = (hp.y - chy) + (lp.y - cly);
         const float nz = (hp.z - chz) + (lp.z - clz);
         const bool leaf = lk.y & ND_LEAF;
-        const float Rx = rx - nx, Ry = ry - ny, Rz = rz - nz;
-        const float r2 = fmaf(Rx, Rx, fmaf(Ry, Ry, fmaf(Rz, Rz, e2)));
-        if (!leaf && !__all_sync(MHPC_FULL, !valid || lp.w <= r2)) { ++nd; continue; }
-        const float ri = r2 > 0.f ? rsqrtf(r2) : 0.f;
-        const float ri2 = ri * ri;
-        const float mri3 = hp.w * ri * ri2;
-        fax = fmaf(-mri3, Rx, fax);
-        fay = fmaf(-mri3, Ry, fay);
-        faz = fmaf(-mri3, Rz, faz);
-        if (!leaf) {
-            ++nquad;
-            const float4 a0 = __ldg(q0 + nd);
-            const float2 a1 = __ldg(q1 + nd);
-            const float qx = a0.x * Rx + a0.y * Ry + a0.z * Rz;
-            const float qy = a0.y * Rx + a0.w * Ry + a1.x * Rz;
-            const float qz = a0.z * Rx + a1.x * Ry + a1.y * Rz;
-            const float rqr = qx * Rx + qy * Ry + qz * Rz;
-            const float ri5 = ri2 * ri2 * ri;
-            const float t = 2.5f * rqr * ri5 * ri2;
-            fax += qx * ri5 - t * Rx;
-            fay += qy * ri5 - t * Ry;
-            faz += qz * ri5 - t * Rz;
+        float Rx[PPL], Ry[PPL], Rz[PPL], r2[PPL];
+        bool far = true;
+#pragma unroll
+        for (int k = 0; k < PPL; ++k) {
+            Rx[k] = rx[k] - nx; Ry[k] = ry[k] - ny; Rz[k] = rz[k] - nz;
+            r2[k] = fmaf(Rx[k], Rx[k], fmaf(Ry[k], Ry[k], fmaf(Rz[k], Rz[k], e2[k])));
+            far = far && (!valid[k] || lp.w <= r2[k]);
+        }
+        if (!leaf && !__all_sync(MHPC_FULL, far)) { ++nd; continue; }
+        float4 a0;
+        float2 a1;
+        if (!leaf) { a0 = __ldg(q0 + nd); a1 = __ldg(q1 + nd); ++nquad; }
+#pragma unroll
+        for (int k = 0; k < PPL; ++k) {
+            const float ri = r2[k] > 0.f ? rsqrtf(r2[k]) : 0.f;
+            const float ri2 = ri * ri;
+            const float mri3 = hp.w * ri * ri2;
+            fax[k] = fmaf(-mri3, Rx[k], fax[k]);
+            fay[k] = fmaf(-mri3, Ry[k], fay[k]);
+            faz[k] = fmaf(-mri3, Rz[k], faz[k]);
+            if (!leaf) {
+                const float qx = a0.x * Rx[k] + a0.y * Ry[k] + a0.z * Rz[k];
+                const float qy = a0.y * Rx[k] + a0.w * Ry[k] + a1.x * Rz[k];
+                const float qz = a0.z * Rx[k] + a1.x * Ry[k] + a1.y * Rz[k];
+                const float rqr = qx * Rx[k] + qy * Ry[k] + qz * Rz[k];
+                const float ri5 = ri2 * ri2 * ri;
+                const float t = 2.5f * rqr * ri5 * ri2;
+                fax[k] += qx * ri5 - t * Rx[k];
+                fay[k] += qy * ri5 - t * Ry[k];
+                faz[k] += qz * ri5 - t * Rz[k];
+            }
         }
         ++ninter;
         if (++since == kFlush) {
-            ax += fax; ay += fay; az += faz;
-            fax = fay = faz = 0.f;
+#pragma unroll
+            for (int k = 0; k < PPL; ++k) {
+                ax[k] += fax[k]; ay[k] += fay[k]; az[k] += faz[k];
+                fax[k] = fay[k] = faz[k] = 0.f;
+            }
             since = 0;
         }
         nd = lk.x;
     }
-    ax += fax; ay += fay; az += faz;
-    if (valid) {
-        const int o = __ldg(perm + s);
-        gax[o] = P.G * ax; gay[o] = P.G * ay; gaz[o] = P.G * az;
+    unsigned nv = 0;
+#pragma unroll
+    for (int k = 0; k < PPL; ++k) {
+        ax[k] += fax[k]; ay[k] += fay[k]; az[k] += faz[k];
+        if (valid[k]) {
+            const int o = __ldg(perm + s[k]);
+            gax[o] = P.G * ax[k]; gay[o] = P.G * ay[k]; gaz[o] = P.G * az[k];
+        }
+        nv += __popc(__ballot_sync(MHPC_FULL, valid[k]));
     }
-    unsigned nv = __popc(__ballot_sync(MHPC_FULL, valid));
     if (lane == 0) {
-        atomicAdd(&st->interactions, ninter * nv);
-        atomicAdd(&st->nodes_visited, nvisit);
-        atomicAdd(&st->quad_interactions, nquad * nv);
+        atomicAdd(&st->interactions, (unsigned long long)ninter * nv);
+        atomicAdd(&st->nodes_visited, (unsigned long long)nvisit);
+        atomicAdd(&st->quad_interactions, (unsigned long long)nquad * nv);
     }
 }
 
@@ -215,10 +252,11 @@ int gravity_mixed(const TreeDev& T, const GravParams& P, const double* sx, const
                   const double* sh, const int* perm, double* gax, double* gay, double* gaz, DevStatus* st,
                   cudaStream_t s) {
     if (P.n <= 0) return MHPC_OK;
-    long groups = ((long)P.n + 31) / 32;
+    constexpr int PPL = MHPC_MIXED_PPL;
+    long groups = ((long)P.n + 32 * PPL - 1) / (32 * PPL);
     long blocks = (groups * 32 + kWalkBlock - 1) / kWalkBlock;
-    k_grav_mixed<<<(int)blocks, kWalkBlock, 0, s>>>(T.mpos, T.mlo, T.quad0, T.quad1, T.link, T.nodes, P, sx, sy, sz,
-                                                    sh, perm, gax, gay, gaz, st);
+    k_grav_mixed<PPL><<<(int)blocks, kWalkBlock, 0, s>>>(T.mpos, T.mlo, T.quad0, T.quad1, T.link, T.nodes, P, sx,
+                                                         sy, sz, sh, perm, gax, gay, gaz, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

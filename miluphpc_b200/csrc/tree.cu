@@ -73,6 +73,20 @@ __device__ __forceinline__ int cell_node(const int* off, const unsigned char* dl
     return off[a] + (L - dl_at(dl, a - 1) - 1);
 }
 
+// Child slot of `node` (level Lc) in its parent: the key digit at level Lc,
+// unique among siblings, so slots listed by digit are in curve (pre-)order.
+// Leaves below level 21 (particles sharing a full key) have no digit: the
+// parent is flagged and its children are then enumerated by skip pointers.
+__device__ __forceinline__ void add_kid(TreeDev& T, int par, int node, uint64_t key, int Lc) {
+    if (Lc <= MHPC_MAX_LEVEL) {
+        const int d = (int)((key >> (3 * (MHPC_MAX_LEVEL - Lc))) & 7);
+        T.kids[8 * (size_t)par + d] = node;
+        atomicOr(&T.kmask[par], 1 << d);
+    } else {
+        atomicOr(&T.kmask[par], 0x100);
+    }
+}
+
 __global__ void __launch_bounds__(256) k_nodes(TreeDev T, const uint64_t* __restrict__ k, DevStatus* st) {
     const int n = T.n;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
@@ -100,7 +114,7 @@ __global__ void __launch_bounds__(256) k_nodes(TreeDev T, const uint64_t* __rest
             T.parent[node] = par;
             T.arrive[node] = 0;
             if (par >= T.cap_nodes) set_status(st, MHPC_ERR_NODE_POOL, par);
-            else if (par >= 0) atomicAdd(&T.nchild[par], 1);
+            else if (par >= 0) { atomicAdd(&T.nchild[par], 1); add_kid(T, par, node, ka, L); }
             else atomicAdd(T.root_nchild, 1);
         }
         const int node = o + c;
@@ -121,8 +135,8 @@ __global__ void __launch_bounds__(256) k_nodes(TreeDev T, const uint64_t* __rest
         T.nchild[node] = 0;
         T.leaf_node[a] = node;
         if (par >= T.cap_nodes) set_status(st, MHPC_ERR_NODE_POOL, par);
-            else if (par >= 0) atomicAdd(&T.nchild[par], 1);
-            else atomicAdd(T.root_nchild, 1);
+        else if (par >= 0) { atomicAdd(&T.nchild[par], 1); add_kid(T, par, node, ka, P + 1); }
+        else atomicAdd(T.root_nchild, 1);
         if (P + 1 > MHPC_MAX_LEVEL) atomicMax(&st->max_level, P + 1);
     }
 }
@@ -135,6 +149,7 @@ __global__ void k_zero_cells(TreeDev T) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         T.nchild[i] = 0;
         T.arrive[i] = 0;
+        T.kmask[i] = 0;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *T.root_nchild = 0;
 }
@@ -174,11 +189,21 @@ __global__ void __launch_bounds__(256) k_upward(TreeDev T, const double* __restr
             const int old = atomicAdd(&T.arrive[p], 1);
             if (old != T.nchild[p] - 1) break;
             __threadfence();
-            const int end = T.link[p].x;
+            const int mask = T.kmask[p];
+            int kid[8];
+            int nk = 0;
+            if (!(mask & 0x100)) {
+                const int4 k0 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)p));
+                const int4 k1 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)p) + 1);
+                const int all[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+#pragma unroll
+                for (int d = 0; d < 8; ++d)
+                    if ((mask >> d) & 1) kid[nk++] = all[d];
+            }
             double m = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
             float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
             float4 hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
-            for (int c = p + 1; c < end; c = __ldcg(&T.link[c].x)) {
+            auto add_com = [&](int c) {
                 const double4 cc = ldcg_d4(&T.com[c]);
                 mx = __dadd_rn(mx, __dmul_rn(cc.x, cc.w));
                 my = __dadd_rn(my, __dmul_rn(cc.y, cc.w));
@@ -187,6 +212,14 @@ __global__ void __launch_bounds__(256) k_upward(TreeDev T, const double* __restr
                 const float4 bl = __ldcg(&T.bmin[c]), bh = __ldcg(&T.bmax[c]);
                 lo.x = fminf(lo.x, bl.x); lo.y = fminf(lo.y, bl.y); lo.z = fminf(lo.z, bl.z);
                 hi.x = fmaxf(hi.x, bh.x); hi.y = fmaxf(hi.y, bh.y); hi.z = fmaxf(hi.z, bh.z);
+            };
+            const int end = T.link[p].x;
+            if (mask & 0x100) {
+                for (int c = p + 1; c < end; c = __ldcg(&T.link[c].x)) add_com(c);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (q < nk) add_com(kid[q]);
             }
             if (m > 0.0) {
                 mx = __ddiv_rn(mx, m);
@@ -198,7 +231,7 @@ __global__ void __launch_bounds__(256) k_upward(TreeDev T, const double* __restr
             T.bmax[p] = hi;
             if (want_quad) {
                 double q[6] = {0, 0, 0, 0, 0, 0};
-                for (int c = p + 1; c < end; c = __ldcg(&T.link[c].x)) {
+                auto add_quad = [&](int c) {
                     const double4 cc = ldcg_d4(&T.com[c]);
                     const double s0 = cc.x - mx, s1 = cc.y - my, s2 = cc.z - mz;
                     const double ss = s0 * s0 + s1 * s1 + s2 * s2;
@@ -214,6 +247,13 @@ __global__ void __launch_bounds__(256) k_upward(TreeDev T, const double* __restr
                         const float2 a1 = __ldcg(&T.quad1[c]);
                         q[0] += a0.x; q[1] += a0.y; q[2] += a0.z; q[3] += a0.w; q[4] += a1.x; q[5] += a1.y;
                     }
+                };
+                if (mask & 0x100) {
+                    for (int c = p + 1; c < end; c = __ldcg(&T.link[c].x)) add_quad(c);
+                } else {
+#pragma unroll
+                    for (int qq = 0; qq < 8; ++qq)
+                        if (qq < nk) add_quad(kid[qq]);
                 }
                 T.quad0[p] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
                 T.quad1[p] = make_float2((float)q[4], (float)q[5]);

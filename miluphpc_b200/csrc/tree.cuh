@@ -29,6 +29,8 @@ struct TreeDev {
     int* parent;        // [cap] parent node, -1 for root children
     int* nchild;        // [cap] number of children
     int* arrive;        // [cap] bottom-up arrival counters
+    int* kids;          // [cap * 8] children by key digit (valid where kmask has the bit)
+    int* kmask;         // [cap] bit d: slot d used; 0x100: children without a digit (shared keys)
     double4* com;       // [cap] centre of mass (x, y, z, m)
     float4* bmin;       // [cap] particle bounding box min (rounded down)
     float4* bmax;       // [cap] particle bounding box max (rounded up)

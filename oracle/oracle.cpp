@@ -402,10 +402,56 @@ void orc_quad(const int* child, const int* level, int n, int nodes, int max_leve
 // included); accepted cells add their monopole and, if q is given,
 // quadrupole term.  Leaves are exact.  ninter (per particle) receives the
 // number of accepted nodes.
+// With crit != null a cell is accepted when crit[cell] <= min |com - p|^2 + eps2
+// (per-cell thresholds, e.g. from orc_cell_bmax2).
+void orc_gravity_group_crit(const double* x, const double* y, const double* z, const double* mass,
+                            const double* q, const int* child, const int* level, const int* sorted,
+                            int n, int gsize, double radius, double theta, double eps2, double* gax,
+                            double* gay, double* gaz, int* ninter, const double* crit);
+
 void orc_gravity_group(const double* x, const double* y, const double* z, const double* mass,
                        const double* q, const int* child, const int* level, const int* sorted,
                        int n, int gsize, double radius, double theta, double eps2, double* gax,
                        double* gay, double* gaz, int* ninter) {
+    orc_gravity_group_crit(x, y, z, mass, q, child, level, sorted, n, gsize, radius, theta, eps2, gax, gay,
+                           gaz, ninter, nullptr);
+}
+
+// Squared distance from every cell's centre of mass to the farthest corner of
+// the bounding box of its particles (children first, leaves are points).
+void orc_cell_bmax2(const int* child, const int* level, int n, int nodes, int max_level,
+                    const double* x, const double* y, const double* z, double* bmax2) {
+    std::vector<double> lo(3 * (size_t)nodes), hi(3 * (size_t)nodes);
+    for (int i = 0; i < n; ++i) {
+        lo[3 * i] = hi[3 * i] = x[i]; lo[3 * i + 1] = hi[3 * i + 1] = y[i]; lo[3 * i + 2] = hi[3 * i + 2] = z[i];
+    }
+    for (int L = max_level; L > 0; --L) {
+        for (int i = n; i < nodes; ++i) {
+            if (level[i] != L) continue;
+            double l3[3] = {1e300, 1e300, 1e300}, h3[3] = {-1e300, -1e300, -1e300};
+            for (int c = 0; c < 8; ++c) {
+                int ch = child[8 * i + c];
+                if (ch < 0) continue;
+                for (int d = 0; d < 3; ++d) {
+                    l3[d] = std::min(l3[d], lo[3 * (size_t)ch + d]);
+                    h3[d] = std::max(h3[d], hi[3 * (size_t)ch + d]);
+                }
+            }
+            double c3[3] = {x[i], y[i], z[i]}, b = 0;
+            for (int d = 0; d < 3; ++d) {
+                lo[3 * (size_t)i + d] = l3[d]; hi[3 * (size_t)i + d] = h3[d];
+                double e = std::max(c3[d] - l3[d], h3[d] - c3[d]);
+                b += e * e;
+            }
+            bmax2[i] = b;
+        }
+    }
+}
+
+void orc_gravity_group_crit(const double* x, const double* y, const double* z, const double* mass,
+                            const double* q, const int* child, const int* level, const int* sorted,
+                            int n, int gsize, double radius, double theta, double eps2, double* gax,
+                            double* gay, double* gaz, int* ninter, const double* crit) {
     const int ngroups = (n + gsize - 1) / gsize;
 #pragma omp parallel for schedule(dynamic, 4)
     for (int g = 0; g < ngroups; ++g) {
@@ -424,7 +470,8 @@ void orc_gravity_group(const double* x, const double* y, const double* z, const 
                 d2 = std::min(d2, dx * dx + dy * dy + dz * dz);
             }
             double edge = 2.0 * radius * std::ldexp(1.0, -level[nd]);
-            if (edge * edge / theta <= d2 + eps2) { acc_nodes.push_back(nd); continue; }
+            double cr = crit ? crit[nd] : edge * edge / theta;
+            if (cr <= d2 + eps2) { acc_nodes.push_back(nd); continue; }
             for (int i = 0; i < 8; ++i) if (child[8 * nd + i] != -1) stack.push_back(child[8 * nd + i]);
         }
         for (int l = 0; l < lanes; ++l) {

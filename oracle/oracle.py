@@ -68,6 +68,10 @@ def lib():
         L.orc_leapfrog_v.argtypes = [ctypes.c_int, ctypes.c_double] + [_d] * 9
         L.orc_num_threads.restype = ctypes.c_int
         L.orc_quad.argtypes = [_i, _i, ctypes.c_int, ctypes.c_int, ctypes.c_int, _d, _d, _d, _d, _d]
+        L.orc_cell_bmax2.argtypes = [_i, _i, ctypes.c_int, ctypes.c_int, ctypes.c_int, _d, _d, _d, _d]
+        L.orc_gravity_group_crit.argtypes = [_d, _d, _d, _d, _d, _i, _i, _i, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                             _d, _d, _d, _i, _d]
         L.orc_gravity_group.argtypes = [_d, _d, _d, _d, _d, _i, _i, _i, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                         _d, _d, _d, _i]
@@ -250,4 +254,24 @@ def gravity_group(tree, sorted_perm, radius, theta, eps2, q=None, gsize=32):
                             _p(q) if q is not None else None, _p(tree.child, _i),
                             _p(tree.level, _i), _p(sp, _i), n, int(gsize), float(radius),
                             float(theta), float(eps2), _p(ax), _p(ay), _p(az), _p(cnt, _i))
+    return ax, ay, az, cnt
+
+
+def cell_bmax2(tree, max_level=21):
+    b = np.zeros(tree.num_nodes)
+    lib().orc_cell_bmax2(_p(tree.child, _i), _p(tree.level, _i), tree.n, tree.nodes, int(max_level),
+                         _p(tree.x), _p(tree.y), _p(tree.z), _p(b))
+    return b
+
+
+def gravity_group_crit(tree, sorted_perm, crit, eps2, q=None, gsize=32):
+    n = tree.n
+    ax = np.zeros(n); ay = np.zeros(n); az = np.zeros(n)
+    cnt = np.zeros(n, dtype=np.int32)
+    sp = np.ascontiguousarray(sorted_perm, dtype=np.int32)
+    crit = np.ascontiguousarray(crit, dtype=np.float64)
+    lib().orc_gravity_group_crit(_p(tree.x), _p(tree.y), _p(tree.z), _p(tree.m),
+                                 _p(q) if q is not None else None, _p(tree.child, _i),
+                                 _p(tree.level, _i), _p(sp, _i), n, int(gsize), 1.0, 1.0, float(eps2),
+                                 _p(ax), _p(ay), _p(az), _p(cnt, _i), _p(crit))
     return ax, ay, az, cnt
