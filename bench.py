@@ -34,6 +34,9 @@ WORKLOADS = {
     # profiling case of the walk: node data (~190 MB) larger than L2
     "plummer2m": dict(kind="gravity", n=1 << 21, sfc=1, dt=0.01, eps2=1e-4, theta=0.5, theta_mixed=0.25,
                       theta_plain_matched=0.1, seed=1),
+    # Sedov blast, SPH only: 128^3 lattice, fixed h = 2.5 dx, predictor-corrector
+    "sedov2m": dict(kind="sph", nside=128, n=128 ** 3, sfc=0, dt_max=1e-4, seed=2),
+    "sedov262k": dict(kind="sph", nside=64, n=64 ** 3, sfc=0, dt_max=1e-4, seed=2),
     # the reference's own single-rank case: N = 131072, Lebesgue, leapfrog dt 0.025
     "plummer131k": dict(kind="gravity", n=131072, sfc=0, dt=0.025, eps2=1e-4, theta=0.5, theta_mixed=0.25,
                         theta_plain_matched=0.1, seed=1),
@@ -115,12 +118,25 @@ def fp32_peak_tflops(torch):
 
 def plummer_state(wl, rank):
     from miluphpc_b200 import ics
+    if wl["kind"] == "sph":
+        S = ics.sedov(nside=wl["nside"], seed=wl["seed"] + 1000 * rank)
+        S["p"] = np.zeros(len(S["x"]))
+        S["cs"] = np.zeros(len(S["x"]))
+        return S
     return ics.plummer(wl["n"], seed=wl["seed"] + 1000 * rank)
 
 
 def make_sim(wl, state, variant):
     from miluphpc_b200 import _lib
-    from miluphpc_b200.miluphpc import Miluphpc
+    from miluphpc_b200.miluphpc import Miluphpc, material
+    if wl["kind"] == "sph":
+        # testcases/sedov: predictor-corrector, ideal gas, cubic spline,
+        # Monaghan alpha = 1, beta = 2, energy integrated, density summed
+        cfg = _lib.default_config(gravity=0, sph=1, integrator=1, max_time_step=wl["dt_max"], time_end=1e30,
+                                  smoothing_kernel=1, integrate_energy=1, integrate_density=0, sfc=wl["sfc"],
+                                  precision=1 if variant == "mixed" else 0)
+        return Miluphpc(cfg, state, materials=[material(interactions=60, alpha=1.0, beta=2.0, eos_type=9,
+                                                        gamma=5.0 / 3.0)])
     kw = dict(gravity=1, sph=0, integrator=2, time_step=wl["dt"], smoothing=wl["eps2"], sfc=wl["sfc"],
               theta=wl["theta"], theta_mixed=wl["theta_mixed"])
     if variant == "mixed":
@@ -167,13 +183,14 @@ def run_ours(args, wl):
     clocks = ClockSampler(local)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    grav_ms, inter, quad = [], 0.0, 0.0
+    kern_ms, inter, quad = [], 0.0, 0.0
+    sph = wl["kind"] == "sph"
     torch.cuda.synchronize()
     e0.record()
     for _ in range(args.steps):
         sim.integrate(step)
         st = sim.stats()
-        grav_ms.append(st["ms_stage"]["gravity"])
+        kern_ms.append(st["ms_stage"]["forces" if sph else "gravity"])
         inter += st["gravity_interactions"]
         quad += st["gravity_quad_interactions"]
         step += 1
@@ -187,42 +204,60 @@ def run_ours(args, wl):
     ms_max = float(t.item())
     value = n * world * args.steps / (ms_max / 1e3)
     last = sim.stats()
-    ferr = force_error(sim, torch, wl["eps2"])
+    ferr = None if sph else force_error(sim, torch, wl["eps2"])
     # end to end through the public C ABI with host buffers (pinned)
     e2e = run_e2e(args, wl, sim, state, torch, step)
     out = None
     if rank == 0:
-        flops = (inter * FLOP_MONO + quad * FLOP_QUAD) / args.steps
-        gms = float(np.mean(grav_ms))
-        achieved = flops / (gms / 1e3) / 1e12
-        peak = fp32_peak_tflops(torch)
+        kms = float(np.mean(kern_ms))
         traffic = load_traffic(args.workload, args.variant)
-        roof = {"kernel": "k_grav_mixed" if args.variant == "mixed" else "k_grav_v2", "bound": "fp32",
-                "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
-                "frac": round(achieved / peak, 4) if peak > 0 else None, "traffic": traffic,
-                "peak_source": "measured on this GPU by mhpc_fp32_peak (dependent FFMA chains)",
-                "work_unit": "%d flop per accepted monopole interaction + %d per quadrupole term" % (FLOP_MONO, FLOP_QUAD),
-                "kernel_ms_per_launch": round(gms, 3), "interactions_per_launch": inter / args.steps}
+        if sph:
+            # internal forces: 88 B read (x,y,z,v,m,h,rho,p,c_s) + 40 B written per particle
+            nbytes = 128.0 * n
+            achieved = nbytes / (kms / 1e3) / 1e9
+            peak = hbm_peak_gbs()
+            roof = {"kernel": "k_forces", "bound": "hbm", "achieved": round(achieved, 1), "peak": peak["value"],
+                    "unit": "GB/s", "frac": round(achieved / peak["value"], 4), "traffic": traffic,
+                    "peak_source": peak["source"], "work_unit": "128 B per particle (88 read + 40 written)",
+                    "kernel_ms_per_launch": round(kms, 3), "mean_neighbours": last.get("mean_noi")}
+        else:
+            flops = (inter * FLOP_MONO + quad * FLOP_QUAD) / args.steps
+            achieved = flops / (kms / 1e3) / 1e12
+            peak = fp32_peak_tflops(torch)
+            roof = {"kernel": "k_grav_mixed" if args.variant == "mixed" else "k_grav_v2", "bound": "fp32",
+                    "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
+                    "frac": round(achieved / peak, 4) if peak > 0 else None, "traffic": traffic,
+                    "peak_source": "measured on this GPU by mhpc_fp32_peak (dependent FFMA chains)",
+                    "work_unit": "%d flop per accepted monopole interaction + %d per quadrupole term"
+                                 % (FLOP_MONO, FLOP_QUAD),
+                    "kernel_ms_per_launch": round(kms, 3), "interactions_per_launch": inter / args.steps}
         cpu = cpu_baseline(wl, args) if not args.no_cpu_baseline else None
+        if sph:
+            cfg_out = {"workload": args.workload, "n_particles": n, "variant": args.variant,
+                       "integrator": "predictor-corrector", "kernel": "cubic spline", "h": "fixed 2.5 dx",
+                       "dt_max": wl["dt_max"], "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (state %.0f MB)" % (n * 8 * 14 / 1e6)}
+        else:
+            cfg_out = {"workload": args.workload, "n_particles": n, "variant": args.variant,
+                       "theta": wl["theta_mixed"] if args.variant == "mixed" else
+                       (wl["theta_plain_matched"] if args.variant == "plain_matched" else wl["theta"]),
+                       "sfc": "hilbert" if wl["sfc"] else "lebesgue", "integrator": "leapfrog", "dt": wl["dt"],
+                       "eps2": wl["eps2"], "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (positions alone %.0f MB)" % (n * 24 / 1e6)}
         out = {
             "metric": "particle-steps/s on 1 B200: mixed/learned vs plain at rel. force err <=1e-3",
             "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.variant == "mixed" else "f64",
-            "data": "synthetic (seeded Plummer sampler, no dataset)",
-            "config": {"workload": args.workload, "n_particles": n, "variant": args.variant,
-                       "theta": wl["theta_mixed"] if args.variant == "mixed" else
-                       (wl["theta_plain_matched"] if args.variant == "plain_matched" else wl["theta"]),
-                       "sfc": "hilbert" if wl["sfc"] else "lebesgue", "integrator": "leapfrog", "dt": wl["dt"],
-                       "eps2": wl["eps2"], "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "inputs larger than L2 (positions alone %.0f MB)" % (n * 24 / 1e6)},
+            "data": "synthetic (seeded %s generator, no dataset)" % ("Sedov lattice" if sph else "Plummer"),
+            "config": cfg_out,
             "force_error": ferr,
             "stages_ms_last_step": {k: round(v, 3) for k, v in last["ms_stage"].items()},
             "tree_cells": last["cells"],
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": args.steps * launches_per_step(args.variant),
+            "gpu_launches": args.steps * launches_per_step(args.variant, wl["kind"]),
             "clocks": clk,
         }
     sim.close()
@@ -232,10 +267,24 @@ def run_ours(args, wl):
     return out
 
 
-def launches_per_step(variant):
+def hbm_peak_gbs():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return {"value": float(json.load(open(p))["hbm_gbs"]), "source": "MEASURED_PEAKS.json hbm_gbs (measured)"}
+    except Exception:
+        return {"value": 6650.0, "source": "fallback 6.65 TB/s"}
+
+
+def launches_per_step(variant, kind="gravity"):
     # per RHS: bbox, bbox_finish, keys, hist, hist_scan, 8 onesweep, gather,
-    # lcp, count, 4 scan, copy_total, zero_cells, nodes, upward, walk
-    rhs = 2 + 1 + 2 + 8 + 1 + 2 + 4 + 3 + 1 + 1
+    # lcp, count, 4 scan, copy_total, zero_cells, nodes, upward
+    tree = 2 + 1 + 2 + 8 + 1 + 2 + 4 + 3 + 1
+    if kind == "sph":
+        # frnn, density_eos, forces, export noi; predictor-corrector: two RHS,
+        # max_sml + dt_blocks + dt_final, predictor, corrector
+        rhs = tree + 4
+        return 2 * rhs + 3 + 2
+    rhs = tree + 1  # walk
     if variant == "mixed":
         rhs += 1  # mixed node conversion
     return rhs + 2  # leapfrog updateX, updateV
@@ -247,7 +296,13 @@ def run_e2e(args, wl, sim, state, torch, step0):
     import ctypes
     from miluphpc_b200 import _lib
     n = sim.n
-    fields_in = ["x", "y", "z", "mass", "vx", "vy", "vz", "g_ax", "g_ay", "g_az"]
+    if wl["kind"] == "sph":
+        fields_in = ["x", "y", "z", "mass", "vx", "vy", "vz", "sml", "e", "rho", "p", "cs", "ax", "ay", "az",
+                     "g_ax", "g_ay", "g_az"]
+        n_in, n_out = 12, 14
+    else:
+        fields_in = ["x", "y", "z", "mass", "vx", "vy", "vz", "g_ax", "g_ay", "g_az"]
+        n_in, n_out = 10, 9
     host = {}
     for f in fields_in:
         host[f] = torch.empty(n, dtype=torch.float64, pin_memory=True)
@@ -267,8 +322,8 @@ def run_e2e(args, wl, sim, state, torch, step0):
         _lib.check(L.mhpc_integrate_host(sim.ctx, ctypes.byref(hp), step0 + 1 + k, ctypes.byref(dt)),
                    "integrate_host")
     el = time.perf_counter() - t0
-    h2d = 10 * 8 * n
-    d2h = 9 * 8 * n
+    h2d = n_in * 8 * n
+    d2h = n_out * 8 * n
     return {"value": n * steps / el, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d,
             "d2h_bytes_per_step": d2h, "steps": steps}
 
@@ -291,6 +346,21 @@ def cpu_baseline(wl, args, sample_groups=None):
     from oracle import oracle as O
     from miluphpc_b200 import ics
     n = wl["n"]
+    if wl["kind"] == "sph":
+        # neighbours, density, EOS and forces of one RHS on all particles;
+        # a predictor-corrector step runs two of them
+        S = ics.sedov(nside=wl["nside"], seed=wl["seed"])
+        t0 = time.perf_counter()
+        off, nbr = O.frnn(S["x"], S["y"], S["z"], S["sml"])
+        rho = O.density(S["x"], S["y"], S["z"], S["mass"], S["sml"], off, nbr)
+        p, cs = O.eos(9, np.array([0.0, 5.0 / 3.0, 0, 0, 0]), rho, S["e"], np.zeros(n))
+        O.forces(S["x"], S["y"], S["z"], S["vx"], S["vy"], S["vz"], S["mass"], S["sml"], rho, p, cs, off, nbr,
+                 1.0, 2.0)
+        t1 = time.perf_counter()
+        return {"value": n / (2 * (t1 - t0)), "unit": "particle-steps/s", "cores": O.num_threads(), "kind": "port",
+                "sample": "one full SPH RHS (neighbours, density, EOS, forces) on all %d particles (%.1f s), x2 "
+                          "for the two RHS of a predictor-corrector step" % (n, t1 - t0),
+                "seconds": t1 - t0}
     P = ics.plummer(n, seed=wl["seed"])
     theta = wl["theta_plain_matched"]
     t0 = time.perf_counter()

@@ -53,6 +53,11 @@ struct mhpc_ctx {
     bool ev_recorded[EV_COUNT];
     bool first_rhs_done = false;
     int last_n = 0;
+    // predictor-corrector: predicted state (IntegratedParticles), step size on the device
+    mhpc_particles pred;
+    double* dt_dev = nullptr;
+    double* dt_part = nullptr;
+    double time = 0.0;
     // device mirror for mhpc_integrate_host
     mhpc_particles mirror;
     bool mirror_ready = false;
@@ -365,6 +370,17 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
     }
     A(c->diag_part, diagnostics_scratch_doubles());
     A(c->diag_out, 16);
+    A(c->dt_dev, 1);
+    A(c->dt_part, 148 * 2 * 6 + 16);
+    std::memset(&c->pred, 0, sizeof(c->pred));
+    if (cfg->integrator == 1) {
+        mhpc_particles& q = c->pred;
+        A(q.x, n); A(q.y, n); A(q.z, n); A(q.mass, n); A(q.vx, n); A(q.vy, n); A(q.vz, n);
+        if (cfg->sph) {
+            A(q.ax, n); A(q.ay, n); A(q.az, n); A(q.sml, n); A(q.rho, n); A(q.p, n); A(q.cs, n); A(q.e, n);
+            A(q.drhodt, n); A(q.dedt, n); A(q.dsmldt, n);
+        }
+    }
 #undef A
     if (!rc && cudaMallocHost(&c->h_st, sizeof(DevStatus)) != cudaSuccess) rc = MHPC_ERR_CUDA;
     for (int e = 0; e < EV_COUNT && !rc; ++e)
@@ -486,9 +502,38 @@ int mhpc_integrate(mhpc_ctx* c, const mhpc_particles* p, int step, double* dt_ou
             TRY(launch_euler(*p, dt, c->cfg.gravity, c->cfg.sph, c->cfg.integrate_density, c->cfg.integrate_energy,
                              c->cfg.integrate_sml, s));
         } break;
+        case 1: {  // PredictorCorrectorEuler::integrate (src/integrator/predictor_corrector_euler.cpp:47-151)
+            if (!c->pred.x) return MHPC_ERR_ARG;  // context created for another integrator
+            const int sph = c->cfg.sph;
+            TRY(rhs_async(c, p, 1));
+            const double alpha = c->mats[0].alpha, beta = c->mats[0].beta;
+            const double time_left = c->cfg.time_end > c->time ? c->cfg.time_end - c->time : c->cfg.max_time_step;
+            if (c->cfg.time_step > 0 && c->cfg.max_time_step <= 0) return MHPC_ERR_CONFIG;
+            TRY(launch_set_time_step(*p, c->cfg.gravity, sph, alpha, beta, c->cfg.integrate_density, time_left,
+                                     c->cfg.max_time_step, c->dt_part, c->dt_dev, s));
+            mhpc_particles q = c->pred;
+            q.n = p->n;
+            q.num_nodes = p->n;
+            // gravity is not recomputed on the predicted state (rhs(step, false, false));
+            // the walk outputs are not read, the stored g_a is reused by the corrector
+            q.g_ax = p->g_ax; q.g_ay = p->g_ay; q.g_az = p->g_az;
+            q.noi = nullptr; q.nnl = nullptr; q.level = nullptr;
+            q.material_id = p->material_id;
+            TRY(launch_pc_predictor(*p, q, c->dt_dev, sph, c->cfg.integrate_density, c->cfg.integrate_energy, s));
+            TRY(rhs_async(c, &q, 0));
+            TRY(launch_pc_corrector(*p, q, c->dt_dev, sph, c->cfg.integrate_density, c->cfg.integrate_energy,
+                                    c->cfg.integrate_sml, s));
+            double h_dt = 0.0;
+            CUDA_TRY(cudaMemcpyAsync(&h_dt, c->dt_dev, sizeof(double), cudaMemcpyDeviceToHost, s));
+            int code = read_status(c);
+            if (dt_out) *dt_out = h_dt;
+            c->time += h_dt;
+            return code;
+        }
         default:
             return MHPC_ERR_UNSUPPORTED;
     }
+    c->time += dt;
     return read_status(c);
 }
 
@@ -637,6 +682,7 @@ int mhpc_get_stats(mhpc_ctx* c, mhpc_stats* o) {
     o->gravity_nodes_visited = (double)h.nodes_visited;
     o->gravity_quad_interactions = (double)h.quad_interactions;
     o->max_noi = h.max_noi;
+    o->mean_noi = c->last_n > 0 ? (double)h.noi_sum / c->last_n : 0.0;
     o->sml_out_of_band = h.sml_out_of_band;
     o->predictor_used = h.predictor_used;
     o->predictor_fallback = h.predictor_fallback;

@@ -64,6 +64,155 @@ __global__ void __launch_bounds__(256) k_euler(mhpc_particles p, double dt, int 
     }
 }
 
+// PredictorCorrectorEulerNS::Kernel::predictor
+// (src/integrator/device_predictor_corrector_euler.cu:206-270): Euler
+// prediction of the state into `q` with the step on the device.
+__global__ void __launch_bounds__(256) k_pc_predictor(mhpc_particles p, mhpc_particles q, const double* dtp,
+                                                      int sph, int int_rho, int int_e) {
+    const double dt = *dtp;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < p.n; i += (long)gridDim.x * blockDim.x) {
+        double ax = p.g_ax[i], ay = p.g_ay[i], az = p.g_az[i];
+        if (sph) { ax += p.ax[i]; ay += p.ay[i]; az += p.az[i]; }
+        q.x[i] = p.x[i] + dt * p.vx[i];
+        q.vx[i] = p.vx[i] + dt * ax;
+        q.y[i] = p.y[i] + dt * p.vy[i];
+        q.vy[i] = p.vy[i] + dt * ay;
+        q.z[i] = p.z[i] + dt * p.vz[i];
+        q.vz[i] = p.vz[i] + dt * az;
+        q.mass[i] = p.mass[i];
+        if (sph) {
+            if (int_rho) q.rho[i] = p.rho[i] + dt * p.drhodt[i];
+            if (int_e) {
+                q.e[i] = p.e[i] + dt * p.dedt[i];
+                if (q.e[i] < 1e-6) q.e[i] = 1e-6;
+            } else {
+                q.e[i] = p.e[i];
+            }
+            q.sml[i] = p.sml[i];
+            q.cs[i] = p.cs[i];
+            q.p[i] = p.p[i];
+        }
+    }
+}
+
+// PredictorCorrectorEulerNS::Kernel::corrector (device_predictor_corrector_euler.cu:130-205)
+__global__ void __launch_bounds__(256) k_pc_corrector(mhpc_particles p, mhpc_particles q, const double* dtp,
+                                                      int sph, int int_rho, int int_e, int int_sml) {
+    const double h = 0.5 * *dtp;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < p.n; i += (long)gridDim.x * blockDim.x) {
+        const double pax = sph ? q.ax[i] : 0.0, pay = sph ? q.ay[i] : 0.0, paz = sph ? q.az[i] : 0.0;
+        const double cax = sph ? p.ax[i] : 0.0, cay = sph ? p.ay[i] : 0.0, caz = sph ? p.az[i] : 0.0;
+        p.x[i] = p.x[i] + h * (q.vx[i] + p.vx[i]);
+        p.vx[i] = p.vx[i] + h * (pax + cax + 2 * p.g_ax[i]);
+        p.y[i] = p.y[i] + h * (q.vy[i] + p.vy[i]);
+        p.vy[i] = p.vy[i] + h * (pay + cay + 2 * p.g_ay[i]);
+        p.z[i] = p.z[i] + h * (q.vz[i] + p.vz[i]);
+        p.vz[i] = p.vz[i] + h * (paz + caz + 2 * p.g_az[i]);
+        if (sph) {
+            p.ax[i] = 0.5 * (pax + cax) + p.g_ax[i];
+            p.ay[i] = 0.5 * (pay + cay) + p.g_ay[i];
+            p.az[i] = 0.5 * (paz + caz) + p.g_az[i];
+            if (int_rho) {
+                p.rho[i] = p.rho[i] + h * (q.drhodt[i] + p.drhodt[i]);
+                p.drhodt[i] = 0.5 * (q.drhodt[i] + p.drhodt[i]);
+            }
+            if (int_e) {
+                p.e[i] = p.e[i] + h * (q.dedt[i] + p.dedt[i]);
+                if (p.e[i] < 1e-6) p.e[i] = 1e-6;
+                p.dedt[i] = 0.5 * (q.dedt[i] + p.dedt[i]);
+            }
+            if (int_sml) {
+                p.sml[i] = p.sml[i] + h * (q.dsmldt[i] + p.dsmldt[i]);
+                p.dsmldt[i] = 0.5 * (q.dsmldt[i] + p.dsmldt[i]);
+            } else {
+                p.sml[i] = q.sml[i];
+            }
+        }
+    }
+}
+
+// PredictorCorrectorEulerNS::Kernel::setTimeStep
+// (device_predictor_corrector_euler.cu:300-470): per-particle limits
+// sqrt(h/|a|) (x 0.2), h/c_s (x 0.4), the viscous Courant limit
+// 0.4 h / (c_s + 1.2 (alpha c_s + beta mu_max)) (mu_max is never stored by the
+// reference's force kernel, so 0), rho limit for integrated density, and the
+// search-radius limit searchRadius / (2 v_max); the reference's final
+// cross-block v_max combine takes the minimum of the block maxima, which is
+// kept.  Result capped by dt_max and the time left; written to *dt.
+struct DtShared {
+    double forces, courant, rho, visc, vmax;
+};
+
+__global__ void __launch_bounds__(256) k_dt_blocks(mhpc_particles p, int gravity, int sph, double alpha, double beta,
+                                                   int int_rho, double* part) {
+    double forces = 1.7976931348623157e308, courant = forces, dtrho = forces, visc = forces, vmax = 0.0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < p.n; i += (long)gridDim.x * blockDim.x) {
+        double ax = 0, ay = 0, az = 0;
+        if (gravity) { ax += p.g_ax[i]; ay += p.g_ay[i]; az += p.g_az[i]; }
+        if (sph) { ax += p.ax[i]; ay += p.ay[i]; az += p.az[i]; }
+        const double h = p.sml[i];
+        forces = fmin(forces, sqrt(h / sqrt(ax * ax + ay * ay + az * az)));
+        if (sph) {
+            const double cs = p.cs[i];
+            courant = fmin(courant, h / cs);
+            visc = fmin(visc, 0.4 * h / (cs + 1.2 * (alpha * cs + beta * 0.0)));
+            if (int_rho && p.drhodt[i] != 0)
+                dtrho = fmin(dtrho, 0.1 * (fabs(p.rho[i]) + 0.001) / fabs(p.drhodt[i]));
+        }
+        vmax = fmax(vmax, sqrt(p.vx[i] * p.vx[i] + p.vy[i] * p.vy[i] + p.vz[i] * p.vz[i]));
+    }
+    __shared__ double s[5][256];
+    s[0][threadIdx.x] = forces; s[1][threadIdx.x] = courant; s[2][threadIdx.x] = dtrho;
+    s[3][threadIdx.x] = visc; s[4][threadIdx.x] = vmax;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            for (int k = 0; k < 4; ++k) s[k][threadIdx.x] = fmin(s[k][threadIdx.x], s[k][threadIdx.x + o]);
+            s[4][threadIdx.x] = fmax(s[4][threadIdx.x], s[4][threadIdx.x + o]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < 5) part[blockIdx.x * 5 + threadIdx.x] = s[threadIdx.x][0];
+}
+
+__global__ void k_max_sml(int n, const double* h, double* part);
+
+// search radius from the per-block h maxima, then the final combine
+__global__ void k_dt_final_sr(int blocks, const double* hmax_part, const double* part, int int_rho, double time_left,
+                              double dt_max, double* dt_out) {
+    double hmax = 0.0;
+    for (int b = 0; b < blocks; ++b) hmax = fmax(hmax, hmax_part[b]);
+    double forces = 1.7976931348623157e308, courant = forces, dtrho = forces, visc = forces, vmax = 0.0;
+    for (int b = 0; b < blocks; ++b) {
+        forces = fmin(forces, part[5 * b]);
+        courant = fmin(courant, part[5 * b + 1]);
+        dtrho = fmin(dtrho, part[5 * b + 2]);
+        visc = fmin(visc, part[5 * b + 3]);
+        vmax = b == 0 ? part[5 * b + 4] : fmin(vmax, part[5 * b + 4]);
+    }
+    const double search_radius = 2.0 * hmax;
+    double dt = fmin(0.4 * courant, 0.2 * forces);
+    if (vmax > 0. && search_radius > 0.) dt = fmin(dt, search_radius / (2 * vmax));
+    if (int_rho) dt = fmin(dt, dtrho);
+    dt = fmin(dt, visc);
+    dt = fmin(dt, time_left);
+    if (dt > dt_max) dt = dt_max;
+    *dt_out = dt;
+}
+
+__global__ void k_max_sml(int n, const double* h, double* part) {
+    double m = 0.0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) m = fmax(m, h[i]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(MHPC_FULL, m, o));
+    __shared__ double s[8];
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < 8; ++k) m = fmax(m, s[k]);
+        part[blockIdx.x] = m;
+    }
+}
+
 constexpr int kDiag = 11;
 
 __global__ void __launch_bounds__(256) k_diag(mhpc_particles p, int sph, double* part) {
@@ -217,6 +366,31 @@ int launch_leapfrog_v(const mhpc_particles& p, double dt, cudaStream_t s) {
 int launch_euler(const mhpc_particles& p, double dt, int gravity, int sph, int int_rho, int int_e, int int_sml,
                  cudaStream_t s) {
     k_euler<<<grid_for(p.n, 256, 148 * 16), 256, 0, s>>>(p, dt, gravity, sph, int_rho, int_e, int_sml);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int launch_pc_predictor(const mhpc_particles& p, const mhpc_particles& q, const double* dt, int sph, int int_rho,
+                        int int_e, cudaStream_t s) {
+    k_pc_predictor<<<grid_for(p.n, 256, 148 * 16), 256, 0, s>>>(p, q, dt, sph, int_rho, int_e);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int launch_pc_corrector(const mhpc_particles& p, const mhpc_particles& q, const double* dt, int sph, int int_rho,
+                        int int_e, int int_sml, cudaStream_t s) {
+    k_pc_corrector<<<grid_for(p.n, 256, 148 * 16), 256, 0, s>>>(p, q, dt, sph, int_rho, int_e, int_sml);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int launch_set_time_step(const mhpc_particles& p, int gravity, int sph, double alpha, double beta, int int_rho,
+                         double time_left, double dt_max, double* part, double* dt_out, cudaStream_t s) {
+    const int blocks = 148 * 2;
+    // search radius = 2 max(h) (Miluphpc::parallel_sph, src/miluphpc.cpp:2430-2433)
+    k_max_sml<<<blocks, 256, 0, s>>>(p.n, p.sml, part);
+    k_dt_blocks<<<blocks, 256, 0, s>>>(p, gravity, sph, alpha, beta, int_rho, part + blocks);
+    k_dt_final_sr<<<1, 1, 0, s>>>(blocks, part, part + blocks, int_rho, time_left, dt_max, dt_out);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

@@ -18,6 +18,13 @@ int launch_leapfrog_x(const mhpc_particles& p, double dt, cudaStream_t s);
 int launch_leapfrog_v(const mhpc_particles& p, double dt, cudaStream_t s);
 int launch_euler(const mhpc_particles& p, double dt, int gravity, int sph, int int_rho, int int_e, int int_sml,
                  cudaStream_t s);
+int launch_pc_predictor(const mhpc_particles& p, const mhpc_particles& q, const double* dt, int sph, int int_rho,
+                        int int_e, cudaStream_t s);
+int launch_pc_corrector(const mhpc_particles& p, const mhpc_particles& q, const double* dt, int sph, int int_rho,
+                        int int_e, int int_sml, cudaStream_t s);
+// part needs 148 * 2 * 6 doubles
+int launch_set_time_step(const mhpc_particles& p, int gravity, int sph, double alpha, double beta, int int_rho,
+                         double time_left, double dt_max, double* part, double* dt_out, cudaStream_t s);
 int launch_diagnostics(const mhpc_particles& p, int sph, double* part, double* out, cudaStream_t s);
 size_t diagnostics_scratch_doubles();
 int launch_direct(const double* x, const double* y, const double* z, const double* m, int n, const int* tg, int nt,

@@ -158,6 +158,12 @@ __global__ void __launch_bounds__(kBlock) k_frnn(TreeDev T, int n, int maxnb, co
         if (MODE == 0 && k > maxnb) set_status(st, MHPC_ERR_NEIGHBOURS, (int)s);
         if (MODE == 0) atomicMax(&st->max_noi, k);
     }
+    if (MODE == 0) {
+        unsigned long long tot = active ? (unsigned long long)k : 0ULL;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(MHPC_FULL, tot, o);
+        if (lane == 0) atomicAdd(&st->noi_sum, tot);
+    }
 }
 
 // ------------------------------------------------------- variable h update

@@ -316,6 +316,23 @@ def test_leapfrog_steps_match_oracle(cuda):
     sim.close()
 
 
+def test_predictor_corrector_matches_oracle(cuda):
+    from tests.helpers import oracle_pc_step
+    S = _sedov_state(16, vel=0.02)
+    cfg = sph_cfg(integrator=1, max_time_step=1e-3, time_end=1.0)
+    mat = material(interactions=60, alpha=1.0, beta=2.0, eos_type=9, gamma=5.0 / 3.0)
+    sim = Miluphpc(cfg, S, materials=[mat])
+    st = dict(S)
+    for step in range(2):
+        dt = sim.integrate(step)
+        st, odt = oracle_pc_step(O, st, 1e-3)
+        assert abs(dt - odt) <= 1e-12 * odt
+    for k in ("x", "vx", "e"):
+        ref = st[k]
+        np.testing.assert_allclose(sim.numpy(k), ref, rtol=1e-9, atol=1e-12 * np.abs(ref).max())
+    sim.close()
+
+
 def test_errors_are_status_codes(cuda):
     n = 4096
     P = ics.plummer(n, seed=3)
