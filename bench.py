@@ -37,6 +37,11 @@ WORKLOADS = {
     # Sedov blast, SPH only: 128^3 lattice, fixed h = 2.5 dx, predictor-corrector
     "sedov2m": dict(kind="sph", nside=128, n=128 ** 3, sfc=0, dt_max=1e-4, seed=2),
     "sedov262k": dict(kind="sph", nside=64, n=64 ** 3, sfc=0, dt_max=1e-4, seed=2),
+    # self-gravitating isothermal rotating cloud, variable h (60 +- 5), learned h
+    "cloud1m": dict(kind="cloud", n=1 << 20, sfc=1, dt=0.004, theta=0.5, theta_mixed=0.25,
+                    theta_plain_matched=0.1, train_steps=20, train_iters=1500, seed=3),
+    "cloud8m": dict(kind="cloud", n=1 << 23, sfc=1, dt=0.002, theta=0.6, theta_mixed=0.25,
+                    theta_plain_matched=0.1, train_steps=20, train_iters=1500, seed=3),
     # the reference's own single-rank case: N = 131072, Lebesgue, leapfrog dt 0.025
     "plummer131k": dict(kind="gravity", n=131072, sfc=0, dt=0.025, eps2=1e-4, theta=0.5, theta_mixed=0.25,
                         theta_plain_matched=0.1, seed=1),
@@ -123,6 +128,11 @@ def plummer_state(wl, rank):
         S["p"] = np.zeros(len(S["x"]))
         S["cs"] = np.zeros(len(S["x"]))
         return S
+    if wl["kind"] == "cloud":
+        C = ics.rotating_cloud(wl["n"], seed=wl["seed"] + 1000 * rank)
+        C["p"] = np.zeros(wl["n"])
+        C["cs"] = np.zeros(wl["n"])
+        return C
     return ics.plummer(wl["n"], seed=wl["seed"] + 1000 * rank)
 
 
@@ -137,6 +147,19 @@ def make_sim(wl, state, variant):
                                   precision=1 if variant == "mixed" else 0)
         return Miluphpc(cfg, state, materials=[material(interactions=60, alpha=1.0, beta=2.0, eos_type=9,
                                                         gamma=5.0 / 3.0)])
+    if wl["kind"] == "cloud":
+        # gravity (softening tied to h: eps_i = h_i / 2) + SPH (isothermal gas as
+        # polytropic gamma = 1, K = c_s^2), variable h targeting 60 +- 5
+        # neighbours, explicit Euler; mixed = FP32 walk + learned h, plain =
+        # FP64 v2 walk (accuracy-matched theta) + plain variable-h iteration
+        mixed = variant == "mixed"
+        cfg = _lib.default_config(gravity=1, sph=1, integrator=0, time_step=wl["dt"], smoothing=0.0,
+                                  softening_mode=1, softening_h_factor=0.5, sfc=wl["sfc"], variable_sml=1,
+                                  smoothing_kernel=1, integrate_energy=0, precision=1 if mixed else 0,
+                                  theta=wl["theta"] if variant == "plain" else wl["theta_plain_matched"],
+                                  theta_mixed=wl["theta_mixed"], learned_h=1 if mixed else 0)
+        return Miluphpc(cfg, state, materials=[material(interactions=60, alpha=1.0, beta=2.0, eos_type=0,
+                                                        K=state["cs2"], gamma=1.0)])
     kw = dict(gravity=1, sph=0, integrator=2, time_step=wl["dt"], smoothing=wl["eps2"], sfc=wl["sfc"],
               theta=wl["theta"], theta_mixed=wl["theta_mixed"])
     if variant == "mixed":
@@ -174,7 +197,25 @@ def run_ours(args, wl):
     n = wl["n"]
     sim = make_sim(wl, state, args.variant)
     step = 0
-    for _ in range(args.warmup):
+    train_info = None
+    warm = args.warmup
+    if wl["kind"] == "cloud" and args.variant == "mixed":
+        warm = max(warm, wl["train_steps"])
+    for _ in range(warm):
+        sim.integrate(step)
+        step += 1
+    if wl["kind"] == "cloud" and args.variant == "mixed":
+        # train on the (features, converged h) pairs of the plain steps, then one
+        # more step so that the first timed step starts from predictions
+        import ctypes
+        from miluphpc_b200 import _lib
+        L = _lib.load()
+        l0, l1 = ctypes.c_float(), ctypes.c_float()
+        t0 = time.perf_counter()
+        _lib.check(L.mhpc_mlp_train(sim.ctx, 1, 1e-3, ctypes.byref(l0)), "mlp_train")
+        _lib.check(L.mhpc_mlp_train(sim.ctx, wl["train_iters"], 1e-3, ctypes.byref(l1)), "mlp_train")
+        train_info = {"plain_steps": warm, "iters": wl["train_iters"] + 1, "loss_first": l0.value,
+                      "loss_last": l1.value, "seconds": time.perf_counter() - t0}
         sim.integrate(step)
         step += 1
     torch.cuda.synchronize()
@@ -185,6 +226,7 @@ def run_ours(args, wl):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     kern_ms, inter, quad = [], 0.0, 0.0
     sph = wl["kind"] == "sph"
+    fallback, out_band, unconv, stage_sum = [], [], [], {}
     torch.cuda.synchronize()
     e0.record()
     for _ in range(args.steps):
@@ -193,6 +235,10 @@ def run_ours(args, wl):
         kern_ms.append(st["ms_stage"]["forces" if sph else "gravity"])
         inter += st["gravity_interactions"]
         quad += st["gravity_quad_interactions"]
+        fallback.append(st["predictor_fallback"])
+        out_band.append(st["sml_out_of_band"])
+        for k, v in st["ms_stage"].items():
+            stage_sum[k] = stage_sum.get(k, 0.0) + v / args.steps
         step += 1
     e1.record()
     torch.cuda.synchronize()
@@ -204,7 +250,14 @@ def run_ours(args, wl):
     ms_max = float(t.item())
     value = n * world * args.steps / (ms_max / 1e3)
     last = sim.stats()
-    ferr = None if sph else force_error(sim, torch, wl["eps2"])
+    ferr = None if wl["kind"] != "gravity" else force_error(sim, torch, wl["eps2"])
+    learned = None
+    if wl["kind"] == "cloud":
+        learned = {"training": train_info, "target_band": "60 +- 5 (|n - 60| < 5)",
+                   "first_sweep_fallback_per_step": fallback,
+                   "fallback_rate": float(np.mean(fallback)) / n,
+                   "final_out_of_band_per_step": out_band,
+                   "out_of_band_rate": float(np.mean(out_band)) / n}
     # end to end through the public C ABI with host buffers (pinned)
     e2e = run_e2e(args, wl, sim, state, torch, step)
     out = None
@@ -237,6 +290,16 @@ def run_ours(args, wl):
                        "integrator": "predictor-corrector", "kernel": "cubic spline", "h": "fixed 2.5 dx",
                        "dt_max": wl["dt_max"], "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (state %.0f MB)" % (n * 8 * 14 / 1e6)}
+        elif wl["kind"] == "cloud":
+            cfg_out = {"workload": args.workload, "n_particles": n, "variant": args.variant,
+                       "gravity_theta": wl["theta_mixed"] if args.variant == "mixed" else
+                       (wl["theta_plain_matched"] if args.variant == "plain_matched" else wl["theta"]),
+                       "softening": "eps_i = h_i / 2", "sph": "cubic spline, isothermal (polytropic gamma 1)",
+                       "variable_h": "target 60 +- 5, Jacobi sweeps" + (" from learned h" if args.variant == "mixed"
+                                                                         else ""),
+                       "sfc": "hilbert", "integrator": "explicit euler", "dt": wl["dt"],
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (state %.0f MB)" % (n * 8 * 14 / 1e6)}
         else:
             cfg_out = {"workload": args.workload, "n_particles": n, "variant": args.variant,
                        "theta": wl["theta_mixed"] if args.variant == "mixed" else
@@ -249,10 +312,12 @@ def run_ours(args, wl):
             "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.variant == "mixed" else "f64",
-            "data": "synthetic (seeded %s generator, no dataset)" % ("Sedov lattice" if sph else "Plummer"),
+            "data": "synthetic (seeded %s generator, no dataset)" % (
+                {"sph": "Sedov lattice", "cloud": "rotating cloud", "gravity": "Plummer"}[wl["kind"]]),
             "config": cfg_out,
             "force_error": ferr,
-            "stages_ms_last_step": {k: round(v, 3) for k, v in last["ms_stage"].items()},
+            "learned_h": learned,
+            "stages_ms_mean": {k: round(v, 3) for k, v in stage_sum.items()},
             "tree_cells": last["cells"],
             "roofline": roof,
             "cpu_baseline": cpu,
@@ -287,6 +352,15 @@ def launches_per_step(variant, kind="gravity"):
     rhs = tree + 1  # walk
     if variant == "mixed":
         rhs += 1  # mixed node conversion
+    if kind == "cloud":
+        # variable h: 7 sweeps x (copy, flags, 4 scan, compact, count walk,
+        # update) + 1 record, final flags + scan + record, scatter; SPH: frnn,
+        # density, forces, noi export, band stats; learned: apply, collect,
+        # features; explicit Euler update
+        vh = 7 * 9 + 1 + 6 + 1
+        sphk = 5
+        learned = 3 if variant == "mixed" else 0
+        return rhs + vh + sphk + learned + 1
     return rhs + 2  # leapfrog updateX, updateV
 
 
@@ -296,10 +370,10 @@ def run_e2e(args, wl, sim, state, torch, step0):
     import ctypes
     from miluphpc_b200 import _lib
     n = sim.n
-    if wl["kind"] == "sph":
+    if wl["kind"] in ("sph", "cloud"):
         fields_in = ["x", "y", "z", "mass", "vx", "vy", "vz", "sml", "e", "rho", "p", "cs", "ax", "ay", "az",
                      "g_ax", "g_ay", "g_az"]
-        n_in, n_out = 12, 14
+        n_in, n_out = 12, 14 if wl["kind"] == "sph" else 17
     else:
         fields_in = ["x", "y", "z", "mass", "vx", "vy", "vz", "g_ax", "g_ay", "g_az"]
         n_in, n_out = 10, 9
@@ -346,6 +420,8 @@ def cpu_baseline(wl, args, sample_groups=None):
     from oracle import oracle as O
     from miluphpc_b200 import ics
     n = wl["n"]
+    if wl["kind"] == "cloud":
+        return None
     if wl["kind"] == "sph":
         # neighbours, density, EOS and forces of one RHS on all particles;
         # a predictor-corrector step runs two of them

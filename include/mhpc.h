@@ -259,18 +259,28 @@ int mhpc_fp32_peak(double* tflops);
 
 /* ------------------------------------------------ learned smoothing length */
 /* MLP 12 -> 64 -> 64 -> 1 (SiLU), BF16 weights, FP32 accumulation, trained
- * on the GPU by the library's own tensor-core kernels.  Not in the
- * reference. */
+ * on the GPU by the library's own tensor-core kernels; it predicts
+ * log(h_next / h) from 12 per-particle features of the previous RHS.  Needs a
+ * context created with cfg->learned_h (and variable_sml).  While it is
+ * untrained every RHS runs the plain iteration and adds (features, converged
+ * h) pairs to a training buffer; once trained, each RHS starts the iteration
+ * from the predicted h and falls back to the plain iteration for particles
+ * whose prediction misses the band.  Not in the reference. */
 int mhpc_mlp_reset(mhpc_ctx* ctx, uint64_t seed);
-/* Adds the (features, converged h) pairs of the last plain variable-h
- * iteration to the training buffer and runs `iters` Adam steps; *loss_out
- * (optional) receives the last mini-batch loss.  Synchronises. */
+/* `iters` Adam steps (mini-batches of 8192 pairs drawn from the training
+ * buffer; features and target standardised with the buffer's statistics on
+ * the first call); *loss_out (optional) receives the last mini-batch loss.
+ * Returns MHPC_ERR_ARG while fewer than 1024 pairs are available.
+ * Synchronises. */
 int mhpc_mlp_train(mhpc_ctx* ctx, int iters, float lr, float* loss_out);
-/* Forward pass on `rows` feature rows (device, rows x 12 float) into out
- * (device, rows float), and the FP32 gradient of the mean-squared loss
- * against target (device, rows float) w.r.t. all weights into grad (device,
- * mhpc_mlp_num_params() floats) when grad is not NULL. */
+/* Parameter count; layout: W1[64][16] (inputs 12..15 zero), b1[64],
+ * W2[64][64] (out, in), b2[64], w3[64], b3[1]. */
 int mhpc_mlp_num_params(void);
+/* Forward pass on `rows` raw feature rows (device, rows x 12 float) into out
+ * (device, rows float, optional), and the FP32 gradient of the mean-squared
+ * loss against target (device, rows float) w.r.t. all parameters into grad
+ * (device, mhpc_mlp_num_params() floats, optional); *loss_out (host,
+ * optional).  Synchronises. */
 int mhpc_mlp_forward_backward(mhpc_ctx* ctx, const float* feats, int rows, const float* target,
                               float* out, float* grad, float* loss_out);
 /* Copy the FP32 master weights out (host, mhpc_mlp_num_params() floats) or in. */

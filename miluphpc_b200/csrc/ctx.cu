@@ -47,6 +47,9 @@ struct mhpc_ctx {
     int* noi = nullptr;
     double* hold = nullptr;
     int *vh_done = nullptr, *vh_nit = nullptr, *vh_count = nullptr;
+    int *vh_flags = nullptr, *vh_off = nullptr, *vh_list = nullptr;
+    double* h_start = nullptr;  // sorted h the variable-h iteration started from
+    double last_dt = 0.0;
     double* diag_part = nullptr;
     double* diag_out = nullptr;
     cudaEvent_t ev[EV_COUNT];
@@ -196,20 +199,29 @@ int stage_sph(mhpc_ctx* c, const mhpc_particles* p) {
     const int n = p->n;
     cudaStream_t s = c->stream;
     SphParams P = sph_params(c, n);
+    const int target = c->mats[0].interactions > 0 ? c->mats[0].interactions : 50;
+    const bool learned = c->cfg.learned_h && c->mlp;
     if (c->cfg.variable_sml) {
         CUDA_TRY(cudaMemsetAsync(c->vh_done, 0, sizeof(int) * n, s));
         CUDA_TRY(cudaMemsetAsync(c->vh_nit, 0xff, sizeof(int) * n, s));  // nit starts at -1
-        int target = c->mats[0].interactions > 0 ? c->mats[0].interactions : 50;
-        if (c->cfg.learned_h && c->mlp) TRY(mlp_predict_h(c->mlp, c, n));
-        TRY(sph_variable_h(c->T, P, c->sx, c->sy, c->sz, c->sh, c->hold, c->vh_done, c->vh_nit, c->vh_count,
-                           target, c->cfg.nb_tolerance, c->cfg.max_sml_iterations, c->cfg.max_sml_iterations + 2,
-                           c->st, s));
+        CUDA_TRY(cudaMemcpyAsync(c->h_start, c->sh, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+        // learned path: start the iteration from the predicted h; particles whose
+        // prediction lands in the band stop after the first sweep
+        if (learned) TRY(mlp_apply_prediction(c->mlp, c->perm, c->sh, n, s));
+        VhBuffers B;
+        B.hold = c->hold; B.done = c->vh_done; B.nit = c->vh_nit; B.count = c->vh_count;
+        B.flags = c->vh_flags; B.off = c->vh_off; B.list = c->vh_list; B.scan_scratch = c->scan_scratch;
+        TRY(sph_variable_h(c->T, P, c->sx, c->sy, c->sz, c->sh, B, target, c->cfg.nb_tolerance,
+                           c->cfg.max_sml_iterations, c->cfg.max_sml_iterations + 2, c->st, s));
         GatherList L;
         std::memset(&L, 0, sizeof(L));
         L.count = 1;
         L.src[0] = c->sh;
         L.dst[0] = p->sml;
         TRY(launch_scatter(n, c->perm, L, s));
+        if (learned)
+            TRY(mlp_collect(c->mlp, c->perm, c->h_start, c->sh, c->vh_count, c->vh_nit, target, c->cfg.nb_tolerance,
+                            c->cfg.max_sml_iterations, n, s));
     }
     record(c, EV_SML);
     SphSorted S;
@@ -223,8 +235,19 @@ int stage_sph(mhpc_ctx* c, const mhpc_particles* p) {
     record(c, EV_DENS);
     TRY(sph_forces(P, S, c->nbr, c->noi, c->perm, p->ax, p->ay, p->az, p->drhodt, p->dedt, p->dsmldt, c->st, s));
     if (p->nnl || p->noi) TRY(sph_export_nnl(P, c->nbr, c->noi, c->perm, p->nnl, p->noi, s));
-    if (c->cfg.learned_h && c->mlp) TRY(mlp_collect(c->mlp, c, n));
+    if (c->cfg.variable_sml) TRY(sph_band_stats(P, c->noi, target, c->cfg.nb_tolerance, c->st, s));
     record(c, EV_FORCES);
+    if (learned && c->cfg.variable_sml) {
+        MlpFeatureInputs in;
+        in.n = n; in.perm = c->perm; in.h = c->sh; in.h_start = c->h_start; in.rho = c->srho; in.cs = c->scs;
+        in.vx = c->svx; in.vy = c->svy; in.vz = c->svz; in.noi = c->noi; in.nit = c->vh_nit;
+        in.ax = p->ax; in.ay = p->ay; in.az = p->az;
+        in.gx = c->cfg.gravity ? p->g_ax : nullptr; in.gy = p->g_ay; in.gz = p->g_az;
+        in.drhodt = p->drhodt; in.m = c->sm;
+        in.dt = c->last_dt > 0 ? c->last_dt : (c->cfg.time_step > 0 ? c->cfg.time_step : 1.0);
+        in.target = target;
+        TRY(mlp_features_predict(c->mlp, in, s));
+    }
     return MHPC_OK;
 }
 
@@ -355,7 +378,7 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
     A(T.dl, n); A(T.cnt, n); A(T.off, n + 1); A(T.leaf_node, n);
     A(T.link, M); A(T.first, M); A(T.last, M); A(T.parent, M); A(T.nchild, M); A(T.arrive, M);
     A(T.kids, 8 * M); A(T.kmask, M);
-    A(T.com, M); A(T.bmin, M); A(T.bmax, M);
+    A(T.com, M); A(T.bmin, M); A(T.bmax, M); A(T.hmax, M);
     A(T.root_nchild, 1); A(T.nodes, 1);
     if (cfg->gravity) {
         A(T.quad0, M); A(T.quad1, M); A(T.mpos, M); A(T.mlo, M);
@@ -367,6 +390,7 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
         A(c->nbr, groups * 32 * (size_t)c->maxnb);
         A(c->noi, n);
         A(c->hold, n); A(c->vh_done, n); A(c->vh_nit, n); A(c->vh_count, n);
+        A(c->vh_flags, n); A(c->vh_off, n + 1); A(c->vh_list, n); A(c->h_start, n);
     }
     A(c->diag_part, diagnostics_scratch_doubles());
     A(c->diag_out, 16);
@@ -385,7 +409,10 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
     if (!rc && cudaMallocHost(&c->h_st, sizeof(DevStatus)) != cudaSuccess) rc = MHPC_ERR_CUDA;
     for (int e = 0; e < EV_COUNT && !rc; ++e)
         if (cudaEventCreate(&c->ev[e]) != cudaSuccess) rc = MHPC_ERR_CUDA;
-    if (!rc && cfg->learned_h) rc = mlp_create(&c->mlp, capacity);
+    if (!rc && cfg->learned_h) {
+        rc = mlp_create(&c->mlp, capacity);
+        if (!rc) rc = mlp_reset(c->mlp, 0x6d6c70ULL, c->stream);
+    }
     if (rc) {
         mhpc_ctx_destroy(c);
         return rc;
@@ -528,12 +555,14 @@ int mhpc_integrate(mhpc_ctx* c, const mhpc_particles* p, int step, double* dt_ou
             int code = read_status(c);
             if (dt_out) *dt_out = h_dt;
             c->time += h_dt;
+            c->last_dt = h_dt;
             return code;
         }
         default:
             return MHPC_ERR_UNSUPPORTED;
     }
     c->time += dt;
+    c->last_dt = dt;
     return read_status(c);
 }
 
@@ -713,6 +742,35 @@ int mhpc_direct_gravity(const double* x, const double* y, const double* z, const
                         int nt, double eps2, double* gax, double* gay, double* gaz, void* stream) {
     if (n < 0 || nt < 0 || (nt > 0 && (!x || !y || !z || !m || !targets || !gax || !gay || !gaz))) return MHPC_ERR_ARG;
     return launch_direct(x, y, z, m, n, targets, nt, eps2, gax, gay, gaz, (cudaStream_t)stream);
+}
+
+// ------------------------------------------------ learned smoothing length
+int mhpc_mlp_num_params(void) { return MLP_NPARAM; }
+
+int mhpc_mlp_reset(mhpc_ctx* c, uint64_t seed) {
+    if (!c || !c->mlp) return MHPC_ERR_ARG;
+    return mlp_reset(c->mlp, seed, c->stream);
+}
+
+int mhpc_mlp_train(mhpc_ctx* c, int iters, float lr, float* loss_out) {
+    if (!c || !c->mlp || iters < 0 || !(lr > 0.f)) return MHPC_ERR_ARG;
+    return mlp_train(c->mlp, iters, lr, 8192, loss_out, c->stream);
+}
+
+int mhpc_mlp_forward_backward(mhpc_ctx* c, const float* feats, int rows, const float* target, float* out, float* grad,
+                              float* loss_out) {
+    if (!c || !c->mlp || !feats || !target || rows <= 0) return MHPC_ERR_ARG;
+    return mlp_forward_backward(c->mlp, feats, rows, target, out, grad, loss_out, c->stream);
+}
+
+int mhpc_mlp_get_params(mhpc_ctx* c, float* host) {
+    if (!c || !c->mlp || !host) return MHPC_ERR_ARG;
+    return mlp_get_params(c->mlp, host, c->stream);
+}
+
+int mhpc_mlp_set_params(mhpc_ctx* c, const float* host) {
+    if (!c || !c->mlp || !host) return MHPC_ERR_ARG;
+    return mlp_set_params(c->mlp, host, c->stream);
 }
 
 }  // extern "C"

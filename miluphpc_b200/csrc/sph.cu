@@ -79,28 +79,41 @@ __device__ __forceinline__ size_t nb_index(long s, int k, int maxnb) {
 }
 
 // ------------------------------------------------------------ FRNN walk
-// mode 0: write lists (h_i = h[i], h_j = h[j]); mode 1: count only for lanes
-// with done[i] == 0, with h_i = h[i], h_j = h[j] (the variable-h sweep passes
-// the sweep's snapshot as h).
+// mode 0: write lists (h_i = h[i], h_j = h[j]) for all particles; mode 1:
+// count only, with h_i = h[i], h_j = h[j] (the variable-h sweep passes the
+// sweep's snapshot as h), for the particles of `list` (list_count entries, in
+// sorted order, so 32 consecutive entries are still spatially close).
 template <int MODE>
 __global__ void __launch_bounds__(kBlock) k_frnn(TreeDev T, int n, int maxnb, const double* __restrict__ sx,
                                                  const double* __restrict__ sy, const double* __restrict__ sz,
-                                                 const double* __restrict__ sh, const int* __restrict__ done,
-                                                 int* __restrict__ nbr, int* __restrict__ noi, DevStatus* st) {
+                                                 const double* __restrict__ sh, const int* __restrict__ list,
+                                                 const int* __restrict__ list_count,
+                                                 const float* __restrict__ node_hmax, int* __restrict__ nbr,
+                                                 int* __restrict__ noi, DevStatus* st) {
     __shared__ int cand[kWarps][kCap];
     if (st->code) return;
     const int M = *T.nodes;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const long g = ((long)blockIdx.x * kBlock + threadIdx.x) >> 5;
-    const long s = g * 32 + lane;
-    const bool valid = s < n;
-    bool active = valid && (MODE == 0 || done[s] == 0);
+    long s = g * 32 + lane;
+    bool valid = s < n;
+    if (MODE == 1) {
+        const long cnt_list = *list_count;
+        if (g * 32 >= cnt_list) return;  // whole warp beyond the list
+        valid = s < cnt_list;
+        s = valid ? list[s] : 0;
+    }
+    const bool active = valid;
     if (!__any_sync(MHPC_FULL, active)) return;
     double px = 0, py = 0, pz = 0, hi = 0;
     if (valid) { px = sx[s]; py = sy[s]; pz = sz[s]; hi = sh[s]; }
     const double hi2 = hi * hi;
     double lx = active ? px - hi : 1e300, ly = active ? py - hi : 1e300, lz = active ? pz - hi : 1e300;
     double ux = active ? px + hi : -1e300, uy = active ? py + hi : -1e300, uz = active ? pz + hi : -1e300;
+    // group points box (a neighbour j must also satisfy d < h_j, so nodes are
+    // tested against it grown by the node's largest h)
+    double plx = active ? px : 1e300, ply = active ? py : 1e300, plz = active ? pz : 1e300;
+    double pux = active ? px : -1e300, puy = active ? py : -1e300, puz = active ? pz : -1e300;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         lx = fmin(lx, __shfl_xor_sync(MHPC_FULL, lx, o));
@@ -109,9 +122,17 @@ __global__ void __launch_bounds__(kBlock) k_frnn(TreeDev T, int n, int maxnb, co
         ux = fmax(ux, __shfl_xor_sync(MHPC_FULL, ux, o));
         uy = fmax(uy, __shfl_xor_sync(MHPC_FULL, uy, o));
         uz = fmax(uz, __shfl_xor_sync(MHPC_FULL, uz, o));
+        plx = fmin(plx, __shfl_xor_sync(MHPC_FULL, plx, o));
+        ply = fmin(ply, __shfl_xor_sync(MHPC_FULL, ply, o));
+        plz = fmin(plz, __shfl_xor_sync(MHPC_FULL, plz, o));
+        pux = fmax(pux, __shfl_xor_sync(MHPC_FULL, pux, o));
+        puy = fmax(puy, __shfl_xor_sync(MHPC_FULL, puy, o));
+        puz = fmax(puz, __shfl_xor_sync(MHPC_FULL, puz, o));
     }
     const float qlx = __double2float_rd(lx), qly = __double2float_rd(ly), qlz = __double2float_rd(lz);
     const float qux = __double2float_ru(ux), quy = __double2float_ru(uy), quz = __double2float_ru(uz);
+    const float rlx = __double2float_rd(plx), rly = __double2float_rd(ply), rlz = __double2float_rd(plz);
+    const float rux = __double2float_ru(pux), ruy = __double2float_ru(puy), ruz = __double2float_ru(puz);
     int k = 0;       // neighbours found by this lane
     int cnt = 0;     // staged candidates (warp-uniform)
     int* C = cand[w];
@@ -137,7 +158,12 @@ __global__ void __launch_bounds__(kBlock) k_frnn(TreeDev T, int n, int maxnb, co
     while (nd < M) {
         const int2 lk = __ldg(T.link + nd);
         const float4 bl = __ldg(T.bmin + nd), bh = __ldg(T.bmax + nd);
-        const bool overlap = !(bh.x < qlx || bl.x > qux || bh.y < qly || bl.y > quy || bh.z < qlz || bl.z > quz);
+        bool overlap = !(bh.x < qlx || bl.x > qux || bh.y < qly || bl.y > quy || bh.z < qlz || bl.z > quz);
+        if (overlap && node_hmax) {
+            const float hn = __ldg(node_hmax + nd);
+            overlap = !(__fadd_ru(bh.x, hn) < rlx || __fadd_rd(bl.x, -hn) > rux || __fadd_ru(bh.y, hn) < rly ||
+                        __fadd_rd(bl.y, -hn) > ruy || __fadd_ru(bh.z, hn) < rlz || __fadd_rd(bl.z, -hn) > ruz);
+        }
         if (!overlap) { nd = lk.x; continue; }
         const int f = __ldg(T.first + nd);
         int len = 0;
@@ -166,14 +192,62 @@ __global__ void __launch_bounds__(kBlock) k_frnn(TreeDev T, int n, int maxnb, co
     }
 }
 
+// Per-lane count walk for sparse lists (later variable-h sweeps, where the
+// particles still iterating are scattered and a shared group box would be
+// large): every lane walks the tree for its own particle, pruning nodes whose
+// box does not come within h_i of it or whose largest h_j cannot reach it.
+__global__ void __launch_bounds__(kBlock) k_count_lane(TreeDev T, const double* __restrict__ sx,
+                                                       const double* __restrict__ sy, const double* __restrict__ sz,
+                                                       const double* __restrict__ sh, const int* __restrict__ list,
+                                                       const int* __restrict__ list_count,
+                                                       const float* __restrict__ node_hmax, int* __restrict__ count,
+                                                       DevStatus* st) {
+    if (st->code) return;
+    const int M = *T.nodes;
+    const long q = (long)blockIdx.x * kBlock + threadIdx.x;
+    if (q >= *list_count) return;
+    const int s = list[q];
+    const double px = sx[s], py = sy[s], pz = sz[s], hi = sh[s], hi2 = hi * hi;
+    const float lx = __double2float_rd(px - hi), ly = __double2float_rd(py - hi), lz = __double2float_rd(pz - hi);
+    const float ux = __double2float_ru(px + hi), uy = __double2float_ru(py + hi), uz = __double2float_ru(pz + hi);
+    const float fx0 = __double2float_rd(px), fy0 = __double2float_rd(py), fz0 = __double2float_rd(pz);
+    const float fx1 = __double2float_ru(px), fy1 = __double2float_ru(py), fz1 = __double2float_ru(pz);
+    int k = 0;
+    int nd = 0;
+    while (nd < M) {
+        const int2 lk = __ldg(T.link + nd);
+        const float4 bl = __ldg(T.bmin + nd), bh = __ldg(T.bmax + nd);
+        const float hn = __ldg(node_hmax + nd);
+        const bool overlap = !(bh.x < lx || bl.x > ux || bh.y < ly || bl.y > uy || bh.z < lz || bl.z > uz) &&
+                             !(__fadd_ru(bh.x, hn) < fx0 || __fadd_rd(bl.x, -hn) > fx1 || __fadd_ru(bh.y, hn) < fy0 ||
+                               __fadd_rd(bl.y, -hn) > fy1 || __fadd_ru(bh.z, hn) < fz0 || __fadd_rd(bl.z, -hn) > fz1);
+        if (!overlap) { nd = lk.x; continue; }
+        if (lk.y & ND_LEAF) {
+            const int j = __ldg(T.first + nd);
+            if (j != s) {
+                const double dx = px - __ldg(sx + j), dy = py - __ldg(sy + j), dz = pz - __ldg(sz + j);
+                const double d = d2_exact(dx, dy, dz);
+                const double hj = __ldg(sh + j);
+                if (d < hi2 && d < hj * hj) ++k;
+            }
+            nd = lk.x;
+        } else {
+            ++nd;
+        }
+    }
+    count[s] = k;
+}
+
 // ------------------------------------------------------- variable h update
 // Convergence rule and update of fixedRadiusNN_variableSML
 // (src/sph/sph.cu:911-933): stop when nit > max_iter or |n - target| < tol,
 // provided n < maxnb; otherwise h *= 0.5 (1 + (target / max(n,1))^(1/3)).
-__global__ void k_vh_update(int n, const int* __restrict__ count, double* h, int* done, int* nit, int target, int tol,
+__global__ void k_vh_update(const int* __restrict__ list, const int* __restrict__ list_count,
+                            const int* __restrict__ count, double* h, int* done, int* nit, int target, int tol,
                             int max_iter, int maxnb) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        if (done[i]) continue;
+    const int m = *list_count;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x) {
+        const int i = list[q];
         const int it = ++nit[i];
         const int c = count[i];
         if ((it > max_iter || abs(c - target) < tol) && c < maxnb) {
@@ -183,6 +257,26 @@ __global__ void k_vh_update(int n, const int* __restrict__ count, double* h, int
             h[i] *= 0.5 * (1.0 + pow((double)target / (double)cc, 1. / 3.));
         }
     }
+}
+
+__global__ void k_flags(int n, const int* __restrict__ done, int* flags) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) flags[i] = done[i] ? 0 : 1;
+}
+
+__global__ void k_compact(int n, const int* __restrict__ flags, const int* __restrict__ off, int* list) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (flags[i]) list[off[i]] = i;
+}
+
+// number of particles still iterating after the first sweep (the fallback
+// count when the first sweep started from predicted smoothing lengths)
+__global__ void k_record_active(const int* __restrict__ list_count, int n, DevStatus* st) {
+    st->predictor_fallback = *list_count;
+    st->predictor_used = n - *list_count;
+}
+
+__global__ void k_record_unconverged(const int* __restrict__ list_count, DevStatus* st) {
+    st->sml_unconverged = *list_count;
 }
 
 __global__ void k_copy(int n, const double* __restrict__ a, double* b) {
@@ -326,22 +420,51 @@ int sph_frnn(const TreeDev& T, const SphParams& P, const SphSorted& S, int* nbr,
              cudaStream_t s) {
     if (P.n <= 0) return MHPC_OK;
     long blocks = (((long)P.n + 31) / 32 * 32 + kBlock - 1) / kBlock;
-    k_frnn<0><<<(int)blocks, kBlock, 0, s>>>(T, P.n, P.maxnb, S.x, S.y, S.z, S.h, nullptr, nbr, noi, st);
+    const float* hmax = nullptr;
+    if (P.avg_h) {  // smoothing lengths differ: prune nodes by their largest h
+        int rc = tree_node_hmax(T, S.h, st, s);
+        if (rc) return rc;
+        hmax = T.hmax;
+    }
+    k_frnn<0><<<(int)blocks, kBlock, 0, s>>>(T, P.n, P.maxnb, S.x, S.y, S.z, S.h, nullptr, nullptr, hmax, nbr, noi,
+                                              st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }
 
 int sph_variable_h(const TreeDev& T, const SphParams& P, const double* x, const double* y, const double* z,
-                   double* h, double* hold, int* done, int* nit, int* count, int target, int tol, int max_iter,
-                   int sweeps, DevStatus* st, cudaStream_t s) {
+                   double* h, const VhBuffers& B, int target, int tol, int max_iter, int sweeps, DevStatus* st,
+                   cudaStream_t s) {
     if (P.n <= 0) return MHPC_OK;
-    long blocks = (((long)P.n + 31) / 32 * 32 + kBlock - 1) / kBlock;
-    int g = grid_for(P.n, 256, 148 * 16);
+    const long blocks = (((long)P.n + 31) / 32 * 32 + kBlock - 1) / kBlock;
+    const int g = grid_for(P.n, 256, 148 * 16);
+    const int* list_count = B.off + P.n;
     for (int it = 0; it < sweeps; ++it) {
-        k_copy<<<g, 256, 0, s>>>(P.n, h, hold);
-        k_frnn<1><<<(int)blocks, kBlock, 0, s>>>(T, P.n, P.maxnb, x, y, z, hold, done, nullptr, count, st);
-        k_vh_update<<<g, 256, 0, s>>>(P.n, count, h, done, nit, target, tol, max_iter, P.maxnb);
+        // Jacobi snapshot of h, then the list of particles still iterating
+        k_copy<<<g, 256, 0, s>>>(P.n, h, B.hold);
+        k_flags<<<g, 256, 0, s>>>(P.n, B.done, B.flags);
+        int rc = scan_exclusive_i32(B.flags, B.off, P.n, B.scan_scratch, s);
+        if (rc) return rc;
+        k_compact<<<g, 256, 0, s>>>(P.n, B.flags, B.off, B.list);
+        if (it == 1) k_record_active<<<1, 1, 0, s>>>(list_count, P.n, st);
+        rc = tree_node_hmax(T, B.hold, st, s);
+        if (rc) return rc;
+        if (it == 0) {
+            // first sweep: (nearly) every particle, group walks
+            k_frnn<1><<<(int)blocks, kBlock, 0, s>>>(T, P.n, P.maxnb, x, y, z, B.hold, B.list, list_count, T.hmax,
+                                                      nullptr, B.count, st);
+        } else {
+            // later sweeps: the few particles still iterating, one walk per lane
+            k_count_lane<<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(T, x, y, z, B.hold, B.list, list_count,
+                                                                        T.hmax, B.count, st);
+        }
+        k_vh_update<<<g, 256, 0, s>>>(B.list, list_count, B.count, h, B.done, B.nit, target, tol, max_iter,
+                                      P.maxnb);
     }
+    k_flags<<<g, 256, 0, s>>>(P.n, B.done, B.flags);
+    int rc = scan_exclusive_i32(B.flags, B.off, P.n, B.scan_scratch, s);
+    if (rc) return rc;
+    k_record_unconverged<<<1, 1, 0, s>>>(list_count, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }
@@ -359,6 +482,23 @@ int sph_forces(const SphParams& P, const SphSorted& S, const int* nbr, const int
     if (P.n <= 0) return MHPC_OK;
     k_forces<<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(P, S, nbr, noi, perm, ax, ay, az, drhodt, dedt, dsmldt,
                                                            st);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+namespace {
+__global__ void k_band(int n, const int* __restrict__ noi, int target, int tol, DevStatus* st) {
+    int bad = 0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        bad += abs(noi[i] - target) >= tol;
+    for (int o = 16; o > 0; o >>= 1) bad += __shfl_xor_sync(MHPC_FULL, bad, o);
+    if ((threadIdx.x & 31) == 0 && bad) atomicAdd(&st->sml_out_of_band, bad);
+}
+}  // namespace
+
+int sph_band_stats(const SphParams& P, const int* noi, int target, int tol, DevStatus* st, cudaStream_t s) {
+    if (P.n <= 0) return MHPC_OK;
+    k_band<<<grid_for(P.n, 256, 148 * 4), 256, 0, s>>>(P.n, noi, target, tol, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

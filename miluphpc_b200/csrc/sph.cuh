@@ -36,13 +36,23 @@ struct SphSorted {
 // nbr[((s >> 5) * maxnb + k) * 32 + (s & 31)], count noi[s].
 int sph_frnn(const TreeDev& T, const SphParams& P, const SphSorted& S, int* nbr, int* noi, DevStatus* st,
              cudaStream_t s);
+struct VhBuffers {
+    double* hold;        // [n] Jacobi snapshot
+    int* done;           // [n] converged (zeroed by the caller before the first sweep)
+    int* nit;            // [n] iteration counters (-1 before the first sweep)
+    int* count;          // [n] neighbour counts of the last sweep
+    int* flags;          // [n] scratch
+    int* off;            // [n+1] scratch (scan); off[n] = particles still iterating
+    int* list;           // [n] particles still iterating
+    void* scan_scratch;
+};
 // Plain variable-h iteration (Jacobi form of fixedRadiusNN_variableSML):
-// updates h (sorted, in place) for up to `sweeps` sweeps; `done` marks converged
-// particles (caller zeroes it before the first sweep; predictor-accepted
-// particles can be pre-marked), hold/htry are scratch [n].
+// updates h (sorted, in place) for `sweeps` sweeps; every sweep walks only the
+// particles still iterating (compacted list).  Starting h (the caller's h on
+// entry) may be the previous step's or a predicted one.
 int sph_variable_h(const TreeDev& T, const SphParams& P, const double* x, const double* y, const double* z,
-                   double* h, double* hold, int* done, int* nit, int* count, int target, int tol, int max_iter,
-                   int sweeps, DevStatus* st, cudaStream_t s);
+                   double* h, const VhBuffers& B, int target, int tol, int max_iter, int sweeps, DevStatus* st,
+                   cudaStream_t s);
 int sph_density_eos(const SphParams& P, const SphSorted& S, const int* nbr, const int* noi, const int* perm,
                     double* rho_out, double* p_out, double* cs_out, DevStatus* st, cudaStream_t s);
 int sph_forces(const SphParams& P, const SphSorted& S, const int* nbr, const int* noi, const int* perm,
@@ -50,5 +60,7 @@ int sph_forces(const SphParams& P, const SphSorted& S, const int* nbr, const int
                cudaStream_t s);
 // Scatter the sorted neighbour lists into the reference layout
 // nnl[i * maxnb + k] (original indices) and noi[i].
+// particles whose final neighbour count misses |n - target| < tol -> st->sml_out_of_band
+int sph_band_stats(const SphParams& P, const int* noi, int target, int tol, DevStatus* st, cudaStream_t s);
 int sph_export_nnl(const SphParams& P, const int* nbr, const int* noi, const int* perm, int* nnl, int* noi_out,
                    cudaStream_t s);

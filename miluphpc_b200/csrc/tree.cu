@@ -263,6 +263,38 @@ __global__ void __launch_bounds__(256) k_upward(TreeDev T, const double* __restr
     }
 }
 
+// Bottom-up maximum of the smoothing lengths, same last-arriver scheme as
+// k_upward (arrive[] cleared by the caller).
+__global__ void __launch_bounds__(256) k_node_hmax(TreeDev T, const double* __restrict__ h, const DevStatus* st) {
+    if (st->code) return;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < T.n; a += gridDim.x * blockDim.x) {
+        const int leaf = T.leaf_node[a];
+        T.hmax[leaf] = __double2float_ru(h[a]);
+        int p = T.parent[leaf];
+        while (p >= 0) {
+            __threadfence();
+            const int old = atomicAdd(&T.arrive[p], 1);
+            if (old != T.nchild[p] - 1) break;
+            __threadfence();
+            const int mask = T.kmask[p];
+            float m = 0.f;
+            if (mask & 0x100) {
+                const int end = T.link[p].x;
+                for (int c = p + 1; c < end; c = __ldcg(&T.link[c].x)) m = fmaxf(m, __ldcg(&T.hmax[c]));
+            } else {
+                const int4 k0 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)p));
+                const int4 k1 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)p) + 1);
+                const int all[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+#pragma unroll
+                for (int d = 0; d < 8; ++d)
+                    if ((mask >> d) & 1) m = fmaxf(m, __ldcg(&T.hmax[all[d]]));
+            }
+            T.hmax[p] = m;
+            p = T.parent[p];
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) k_mixed_nodes(TreeDev T, const long long* ord, double inv_theta,
                                                      const DevStatus* st) {
     if (st->code) return;
@@ -304,6 +336,13 @@ int tree_build(TreeDev& T, const uint64_t* skey, void* scan_scratch, DevStatus* 
 int tree_upward(TreeDev& T, const double* sx, const double* sy, const double* sz, const double* sm,
                 int want_quad, DevStatus* st, cudaStream_t s) {
     k_upward<<<grid_for(T.n, 256, 148 * 16), 256, 0, s>>>(T, sx, sy, sz, sm, want_quad, st);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int tree_node_hmax(const TreeDev& T, const double* h, const DevStatus* st, cudaStream_t s) {
+    CUDA_TRY(cudaMemsetAsync(T.arrive, 0, sizeof(int) * (size_t)T.cap_nodes, s));
+    k_node_hmax<<<grid_for(T.n, 256, 148 * 16), 256, 0, s>>>(T, h, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

@@ -38,6 +38,7 @@ struct TreeDev {
     float2* quad1;      // [cap] Qyz Qzz
     float4* mpos;       // [cap] mixed path: float(x), float(y), float(z), m
     float4* mlo;        // [cap] mixed path: x - float(x), ..., opening criterion edge^2/theta
+    float* hmax;        // [cap] largest smoothing length below the node (rounded up)
     int* root_nchild;   // [1]
     int* nodes;         // [1] total nodes (= off[n]), device copy
 };
@@ -45,4 +46,6 @@ struct TreeDev {
 int tree_build(TreeDev& T, const uint64_t* skey, void* scan_scratch, DevStatus* st, cudaStream_t s);
 int tree_upward(TreeDev& T, const double* sx, const double* sy, const double* sz, const double* sm,
                 int want_quad, DevStatus* st, cudaStream_t s);
+// T.hmax[node] = max h over the node's particles (h sorted, n entries).
+int tree_node_hmax(const TreeDev& T, const double* h, const DevStatus* st, cudaStream_t s);
 int tree_mixed_nodes(TreeDev& T, const long long* ord, double theta, const DevStatus* st, cudaStream_t s);
