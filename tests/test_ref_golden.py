@@ -1,0 +1,158 @@
+"""Oracle and CUDA path against milupHPC's own outputs.
+
+The fixtures tests/golden/ref_*.npz hold seeded inputs and what the
+reference's kernels returned for them (tests/golden/make_golden.py runs the
+reference harness built from the reference sources):
+
+* gravity (testcases/plummer/parameter.h build): computeBoundingBox, buildTree,
+  calculateCentersOfMass, sortArray of the supplied SFC keys,
+  computeForces_v2 -- src/subdomain_key_tree/tree.cu:302-437, 768-1083,
+  1416-1480; src/helper.cu:150-166; src/gravity/gravity.cu:726-903.
+* SPH (testcases/sedov/parameter.h build: ideal gas, INTEGRATE_ENERGY,
+  INTEGRATE_SML, cubic spline): fixedRadiusNN v0, calculateDensity,
+  calculateSoundSpeed, calculatePressure, internalForces --
+  src/sph/sph.cu:93-281, src/sph/density.cu, src/sph/soundspeed.cu,
+  src/sph/pressure.cu, src/sph/internal_forces.cu.
+
+Bars: bounding box, tree cells (key prefix, level), every particle's path and
+the sorted order exact; centres of mass exact; forces within 1e-12 relative
+(the reference takes CUDA's rsqrt, the oracle 1/sqrt); neighbour sets equal;
+density, pressure, sound speed within 1e-12; SPH rates within 1e-10 of their
+largest magnitude (the neighbour order, hence the summation order, differs).
+"""
+import importlib.util
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import rel_err
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+GRAVITY = ["ref_gravity_lebesgue", "ref_gravity_hilbert"]
+
+
+def fixture(name):
+    path = os.path.join(GOLDEN, name + ".npz")
+    assert os.path.exists(path), "missing reference fixture " + path
+    return dict(np.load(path))
+
+
+def tree_walk(child, n, x, y, z, m):
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLDEN, "make_golden.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.walk_ref_tree(child, n, x, y, z, m)
+
+
+def close_rates(got, ref, tol=1e-10):
+    scale = np.abs(ref).max()
+    assert np.abs(got - ref).max() <= tol * scale, (np.abs(got - ref).max(), scale)
+
+
+# ----------------------------------------------------------------- oracle --
+@pytest.mark.parametrize("name", GRAVITY)
+def test_oracle_tree_and_v2_match_reference(name):
+    F = fixture(name)
+    x, y, z, m = F["x"], F["y"], F["z"], F["m"]
+    n = len(x)
+    bb = O.bbox(x, y, z)
+    assert np.array_equal(bb, F["bbox"])
+    # each particle's path through the reference tree is its Lebesgue key prefix
+    lk = O.keys(x, y, z, bb, 0)
+    shift = (3 * (21 - F["leaf_level"].astype(np.int64))).astype(np.uint64)
+    assert np.array_equal(lk >> shift, F["leaf_prefix"])
+    T = O.Tree(x, y, z, m, bb)
+    assert T.nodes - n == int(F["cells"])
+    cp, cl, com, lp, ll = tree_walk(T.child, n, T.x, T.y, T.z, T.m)
+    assert np.array_equal(cp, F["cell_prefix"]) and np.array_equal(cl, F["cell_level"])
+    assert np.array_equal(lp, F["leaf_prefix"]) and np.array_equal(ll, F["leaf_level"])
+    assert np.array_equal(com, F["cell_com"])
+    keys = O.keys(x, y, z, bb, int(F["curve"]))
+    _, perm = O.sort(keys)
+    assert np.array_equal(perm, F["sorted"])
+    ax, ay, az = O.gravity_v2(T, perm, 0.5 * (bb[1] - bb[0]), float(F["theta"]), float(F["eps2"]))
+    e = rel_err(ax, ay, az, F["ax"], F["ay"], F["az"])
+    assert e.max() < 1e-12, e.max()
+
+
+def test_oracle_sph_matches_reference():
+    F = fixture("ref_sph")
+    x, y, z, m, h = F["x"], F["y"], F["z"], F["m"], F["sml"]
+    assert np.array_equal(O.bbox(x, y, z), F["bbox"])
+    off, nbr = O.frnn(x, y, z, h)
+    noi = np.diff(off)
+    assert np.array_equal(noi, F["noi"])
+    owner = np.repeat(np.arange(len(x)), noi)
+    nb = nbr.astype(np.int64)
+    assert np.array_equal(np.bincount(owner, weights=nb, minlength=len(x)).astype(np.int64), F["nb_sum"])
+    assert np.array_equal(np.bincount(owner, weights=nb * nb, minlength=len(x)).astype(np.int64), F["nb_sq"])
+    # INTEGRATE_SML: kernels of a pair use the mean smoothing length
+    rho = O.density(x, y, z, m, h, off, nbr, avg_h=True)
+    np.testing.assert_allclose(rho, F["rho"], rtol=1e-12)
+    p, cs = O.eos(9, np.array([0.0, float(F["gamma"]), 0.0, 0.0, 0.0]), rho, F["e"], F["p"])
+    np.testing.assert_allclose(p, F["p_out"], rtol=1e-12)
+    np.testing.assert_allclose(cs, F["cs_out"], rtol=1e-12)
+    ax, ay, az, drho, de, dh = O.forces(x, y, z, F["vx"], F["vy"], F["vz"], m, h, rho, p, cs, off, nbr,
+                                        float(F["alpha"]), float(F["beta"]), avg_h=True,
+                                        integrate_sml=True)
+    for got, ref in ((ax, F["ax"]), (ay, F["ay"]), (az, F["az"]), (drho, F["drhodt"]), (de, F["dedt"]),
+                     (dh, F["dsmldt"])):
+        close_rates(got, ref)
+
+
+# -------------------------------------------------------------- CUDA path --
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", GRAVITY)
+def test_cuda_gravity_matches_reference(name, cuda):
+    from miluphpc_b200.miluphpc import Miluphpc
+    from tests.helpers import gravity_cfg
+    F = fixture(name)
+    n = len(F["x"])
+    P = dict(x=F["x"], y=F["y"], z=F["z"], mass=F["m"], vx=np.zeros(n), vy=np.zeros(n), vz=np.zeros(n))
+    cfg = gravity_cfg(sfc=int(F["curve"]), theta=float(F["theta"]), smoothing=float(F["eps2"]))
+    sim = Miluphpc(cfg, P)
+    sim.rhs(0)
+    _, perm = sim.export_sorted()
+    assert np.array_equal(perm, F["sorted"])
+    tr = sim.export_tree(2 * n + 20000)
+    assert tr["cells"] == int(F["cells"])
+    cp, cl, com, lp, ll = tree_walk(tr["child"], n, tr["x"], tr["y"], tr["z"], tr["m"])
+    assert np.array_equal(cp, F["cell_prefix"]) and np.array_equal(cl, F["cell_level"])
+    assert np.array_equal(lp, F["leaf_prefix"]) and np.array_equal(ll, F["leaf_level"])
+    if int(F["curve"]) == 0:
+        assert np.array_equal(com, F["cell_com"])
+    else:
+        np.testing.assert_allclose(com, F["cell_com"], rtol=1e-12, atol=1e-14)
+    e = rel_err(sim.numpy("g_ax"), sim.numpy("g_ay"), sim.numpy("g_az"), F["ax"], F["ay"], F["az"])
+    assert e.max() < 1e-9, e.max()
+    sim.close()
+
+
+@pytest.mark.gpu
+def test_cuda_sph_matches_reference(cuda):
+    from miluphpc_b200.miluphpc import Miluphpc, material
+    from tests.helpers import sph_cfg
+    F = fixture("ref_sph")
+    n = len(F["x"])
+    S = {k: F[k].copy() for k in ("x", "y", "z", "vx", "vy", "vz", "sml", "e", "p", "cs")}
+    S["mass"] = F["m"].copy()
+    cfg = sph_cfg(integrate_sml=1)
+    mat = material(interactions=50, alpha=float(F["alpha"]), beta=float(F["beta"]), eos_type=9,
+                   gamma=float(F["gamma"]))
+    sim = Miluphpc(cfg, S, materials=[mat], want_nnl=True)
+    sim.rhs(0)
+    noi = sim.numpy("noi")
+    assert np.array_equal(noi, F["noi"])
+    nnl = sim.t["nnl"].cpu().numpy().reshape(n, cfg.max_num_interactions).astype(np.int64)
+    mask = np.arange(cfg.max_num_interactions)[None, :] < noi[:, None]
+    assert np.array_equal(np.where(mask, nnl, 0).sum(1), F["nb_sum"])
+    assert np.array_equal(np.where(mask, nnl * nnl, 0).sum(1), F["nb_sq"])
+    np.testing.assert_allclose(sim.numpy("rho"), F["rho"], rtol=1e-12)
+    np.testing.assert_allclose(sim.numpy("p"), F["p_out"], rtol=1e-12)
+    np.testing.assert_allclose(sim.numpy("cs"), F["cs_out"], rtol=1e-12)
+    for k, ref in (("ax", "ax"), ("ay", "ay"), ("az", "az"), ("drhodt", "drhodt"), ("dedt", "dedt"),
+                   ("dsmldt", "dsmldt")):
+        close_rates(sim.numpy(k), F[ref])
+    sim.close()
