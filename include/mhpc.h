@@ -76,7 +76,8 @@ typedef struct mhpc_config {
     int nb_tolerance;          /* TOLERANCE_WANTED_NUMBER_OF_INTERACTIONS (5) */
     int max_sml_iterations;    /* MAX_VARIABLE_SML_ITERATIONS (5) */
     /* additions of this library */
-    int precision;             /* 0 plain FP64 (reference semantics), 1 mixed FP32 split + quadrupoles */
+    int precision;             /* 0 plain FP64 (reference semantics); mixed FP32 split + quadrupoles:
+                                  1 interaction lists (sub-box criterion), 2 per-lane vote */
     double theta_mixed;        /* opening parameter of the mixed walk (same squared-ratio meaning) */
     int learned_h;             /* 1: MLP smoothing-length predictor with plain fallback */
     int softening_mode;        /* 0 global eps^2, 1 eps_i = softening_h_factor * h_i (plus eps^2) */

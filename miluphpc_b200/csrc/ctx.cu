@@ -116,7 +116,7 @@ SphParams sph_params(const mhpc_ctx* c, int n) {
     P.integrate_sml = c->cfg.integrate_sml;
     P.integrate_density = c->cfg.integrate_density;
     P.num_materials = c->nmat;
-    P.mixed = c->cfg.precision == 1;
+    P.mixed = c->cfg.precision >= 1;
     for (int i = 0; i < c->nmat && i < MHPC_MAX_MATERIALS; ++i) P.mat[i] = to_dev(c->mats[i], c->cfg.si_units);
     return P;
 }
@@ -167,7 +167,7 @@ int stage_tree(mhpc_ctx* c, const mhpc_particles* p) {
     c->T.n = n;
     TRY(tree_build(c->T, c->skey, c->scan_scratch, c->st, s));
     record(c, EV_TREE);
-    const int want_quad = c->cfg.gravity && c->cfg.precision == 1;
+    const int want_quad = c->cfg.gravity && c->cfg.precision >= 1;
     TRY(tree_upward(c->T, c->sx, c->sy, c->sz, c->sm, want_quad, c->st, s));
     if (want_quad) TRY(tree_mixed_nodes(c->T, c->ord, c->cfg.theta_mixed, c->st, s));
     record(c, EV_COM);
@@ -183,6 +183,10 @@ int stage_gravity(mhpc_ctx* c, const mhpc_particles* p) {
     G.G = c->cfg.si_units ? 6.67430e-11 : 1.0;
     G.ord = c->ord;
     if (c->cfg.precision == 1) {
+        G.theta = c->cfg.theta_mixed;
+        TRY(gravity_lists(c->T, G, c->sx, c->sy, c->sz, c->sh, c->perm, p->g_ax, p->g_ay, p->g_az, c->st,
+                          c->stream));
+    } else if (c->cfg.precision == 2) {
         G.theta = c->cfg.theta_mixed;
         TRY(gravity_mixed(c->T, G, c->sx, c->sy, c->sz, c->sh, c->perm, p->g_ax, p->g_ay, p->g_az, c->st,
                           c->stream));

@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_v2(const double4* __restric
 // float hi + float lo of the FP64 centre of mass, so node - c is formed as
 // (hi - c_hi) + (lo - c_lo) without losing the digits that FP32 absolute
 // coordinates would drop.  A cell is accepted for the warp when every lane
-// has edge^2/theta <= |node - p|^2 + eps2 (the squared-ratio criterion with
+// has edge^2/theta <= |node - p|^2 (the squared-ratio criterion with
 // computeForces_v2's warp vote, applied at every level); accepted cells add
 // monopole + quadrupole terms.  A box test per group would be cheaper per
 // node but opens the whole interior of a group box that straddles a curve
@@ -114,6 +114,7 @@ template <int PPL>
 __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restrict__ mpos, const float4* __restrict__ mlo,
                                                            const float4* __restrict__ q0, const float2* __restrict__ q1,
                                                            const int2* __restrict__ link, const int* __restrict__ nodes_total,
+                                                           const int* __restrict__ leaf_node,
                                                            GravParams P, const double* __restrict__ sx,
                                                            const double* __restrict__ sy, const double* __restrict__ sz,
                                                            const double* __restrict__ sh, const int* __restrict__ perm,
@@ -158,7 +159,14 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restr
     double ax[PPL], ay[PPL], az[PPL];
 #pragma unroll
     for (int k = 0; k < PPL; ++k) {
-        rx[k] = (float)(px[k] - cx); ry[k] = (float)(py[k] - cy); rz[k] = (float)(pz[k] - cz);
+        // the particle's offset is formed exactly like its own leaf's, so the
+        // self-interaction has R = 0 (a one-ulp mismatch would leave m R / eps^3)
+        const int lf = __ldg(leaf_node + (valid[k] ? s[k] : (long)P.n - 1));
+        const float4 hp = __ldg(mpos + lf);
+        const float4 lp = __ldg(mlo + lf);
+        rx[k] = (hp.x - chx) + (lp.x - clx);
+        ry[k] = (hp.y - chy) + (lp.y - cly);
+        rz[k] = (hp.z - chz) + (lp.z - clz);
         e2[k] = (float)e2d[k];
         fax[k] = fay[k] = faz[k] = 0.f;
         ax[k] = ay[k] = az[k] = 0.0;
@@ -180,8 +188,9 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restr
 #pragma unroll
         for (int k = 0; k < PPL; ++k) {
             Rx[k] = rx[k] - nx; Ry[k] = ry[k] - ny; Rz[k] = rz[k] - nz;
-            r2[k] = fmaf(Rx[k], Rx[k], fmaf(Ry[k], Ry[k], fmaf(Rz[k], Rz[k], e2[k])));
-            far = far && (!valid[k] || lp.w <= r2[k]);
+            const float d2 = fmaf(Rx[k], Rx[k], fmaf(Ry[k], Ry[k], Rz[k] * Rz[k]));
+            far = far && (!valid[k] || lp.w <= d2);
+            r2[k] = d2 + e2[k];
         }
         if (!leaf && !__all_sync(MHPC_FULL, far)) { ++nd; continue; }
         float4 a0;
@@ -235,6 +244,320 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restr
     }
 }
 
+// ------------------------------------------------- mixed, interaction lists
+// One warp per group of kListGroup = 64 consecutive sorted particles (two per
+// lane: members lane and 32 + lane).  The traversal is lane-parallel: each
+// step pops up to 32 nodes from a per-warp stack in shared memory and every
+// lane tests one node against the group's kListSub sub-boxes (bounding boxes
+// of kListGroup / kListSub consecutive members).  A cell is accepted when
+// edge^2/theta <= dist(com, box)^2 for every sub-box, i.e. for every member
+// the cell subtends at most sqrt(theta) (edge over distance); accepted cells
+// go to a cell list (monopole + quadrupole), particles to a leaf list
+// (monopole), opened cells push their children.  Whenever a list holds 32
+// entries or more the whole warp evaluates it: a branch-free loop over
+// shared-memory entries, every lane applying each entry to its two
+// particles, FP32 partial sums added into FP64 accumulators after each list.
+// Positions are FP32 offsets from the group centre formed from the nodes'
+// FP32 hi/lo split, particles taking their own leaf's values so that the
+// self-interaction has R = 0 exactly.
+//
+// Stack bound: a pop of k nodes pushes at most 8k (cells with digit children;
+// shared-key buckets are expanded straight into the leaf list), so k is
+// limited to keep room for a depth-first descent (7 per level, 21 levels)
+// on top of the current stack; the stack never overflows, a check that cannot
+// fire reports MHPC_ERR_DEPTH instead of writing past it.
+constexpr int kListGroup = 64;
+constexpr int kListSub = 8;
+constexpr int kListStack = 1024;
+constexpr int kListReserve = 7 * 22 + 8;
+constexpr int kListCap = 64;
+
+struct ListSmem {
+    int stk[kListStack];
+    float4 cpos[kListCap];  // cell: x, y, z (group frame), m
+    float4 cq0[kListCap];   // cell: Qxx Qxy Qxz Qyy
+    float2 cq1[kListCap];   // cell: Qyz Qzz
+    float4 lpos[kListCap];  // leaf: x, y, z, m
+    float4 blo[kListSub];
+    float4 bhi[kListSub];
+    int defer[32];
+};
+
+__device__ __forceinline__ void eval_cells(const ListSmem& S, int count, const float (&rx)[2], const float (&ry)[2],
+                                           const float (&rz)[2], const float (&e2)[2], double (&ax)[2],
+                                           double (&ay)[2], double (&az)[2]) {
+    float fx[2] = {0.f, 0.f}, fy[2] = {0.f, 0.f}, fz[2] = {0.f, 0.f};
+#pragma unroll 2
+    for (int e = 0; e < count; ++e) {
+        const float4 c = S.cpos[e];
+        const float4 a0 = S.cq0[e];
+        const float2 a1 = S.cq1[e];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const float Rx = rx[k] - c.x, Ry = ry[k] - c.y, Rz = rz[k] - c.z;
+            const float r2 = fmaf(Rx, Rx, fmaf(Ry, Ry, fmaf(Rz, Rz, e2[k])));
+            const float ri = r2 > 0.f ? rsqrtf(r2) : 0.f;
+            const float ri2 = ri * ri;
+            const float ri3 = ri * ri2;
+            const float ri5 = ri3 * ri2;
+            const float qx = fmaf(a0.x, Rx, fmaf(a0.y, Ry, a0.z * Rz));
+            const float qy = fmaf(a0.y, Rx, fmaf(a0.w, Ry, a1.x * Rz));
+            const float qz = fmaf(a0.z, Rx, fmaf(a1.x, Ry, a1.y * Rz));
+            const float rqr = fmaf(qx, Rx, fmaf(qy, Ry, qz * Rz));
+            // -(m/r^3 + 5/2 RQR/r^7) R + Q R / r^5
+            const float cc = -fmaf(c.w, ri3, 2.5f * rqr * ri5 * ri2);
+            fx[k] = fmaf(cc, Rx, fmaf(qx, ri5, fx[k]));
+            fy[k] = fmaf(cc, Ry, fmaf(qy, ri5, fy[k]));
+            fz[k] = fmaf(cc, Rz, fmaf(qz, ri5, fz[k]));
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) { ax[k] += fx[k]; ay[k] += fy[k]; az[k] += fz[k]; }
+}
+
+__device__ __forceinline__ void eval_leaves(const ListSmem& S, int count, const float (&rx)[2], const float (&ry)[2],
+                                            const float (&rz)[2], const float (&e2)[2], double (&ax)[2],
+                                            double (&ay)[2], double (&az)[2]) {
+    float fx[2] = {0.f, 0.f}, fy[2] = {0.f, 0.f}, fz[2] = {0.f, 0.f};
+#pragma unroll 2
+    for (int e = 0; e < count; ++e) {
+        const float4 c = S.lpos[e];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const float Rx = rx[k] - c.x, Ry = ry[k] - c.y, Rz = rz[k] - c.z;
+            const float r2 = fmaf(Rx, Rx, fmaf(Ry, Ry, fmaf(Rz, Rz, e2[k])));
+            const float ri = r2 > 0.f ? rsqrtf(r2) : 0.f;
+            const float mri3 = c.w * (ri * ri * ri);
+            fx[k] = fmaf(-mri3, Rx, fx[k]);
+            fy[k] = fmaf(-mri3, Ry, fy[k]);
+            fz[k] = fmaf(-mri3, Rz, fz[k]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) { ax[k] += fx[k]; ay[k] += fy[k]; az[k] += fz[k]; }
+}
+
+constexpr int kListBlock = 128;
+
+__global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams P, const double* __restrict__ sx,
+                                                           const double* __restrict__ sy,
+                                                           const double* __restrict__ sz,
+                                                           const double* __restrict__ sh,
+                                                           const int* __restrict__ perm, double* __restrict__ gax,
+                                                           double* __restrict__ gay, double* __restrict__ gaz,
+                                                           DevStatus* st) {
+    __shared__ ListSmem smem[kListBlock / 32];
+    if (st->code) return;
+    const int M = *T.nodes;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    ListSmem& S = smem[threadIdx.x >> 5];
+    const long gwarp = ((long)blockIdx.x * kListBlock + threadIdx.x) >> 5;
+    const long ngroups = ((long)P.n + kListGroup - 1) / kListGroup;
+    if (gwarp >= ngroups) return;
+    const long s0 = gwarp * kListGroup;
+    long s[2];
+    bool valid[2];
+    int sl[2];
+    float e2[2];
+    double lox = 1e300, loy = 1e300, loz = 1e300, hix = -1e300, hiy = -1e300, hiz = -1e300;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        s[k] = s0 + k * 32 + lane;
+        valid[k] = s[k] < P.n;
+        sl[k] = (int)(valid[k] ? s[k] : (long)P.n - 1);
+        const double px = __ldg(sx + sl[k]), py = __ldg(sy + sl[k]), pz = __ldg(sz + sl[k]);
+        double e = P.eps2;
+        if (P.h_factor > 0.0) { const double hh = P.h_factor * __ldg(sh + sl[k]); e += hh * hh; }
+        e2[k] = (float)e;
+        lox = fmin(lox, px); loy = fmin(loy, py); loz = fmin(loz, pz);
+        hix = fmax(hix, px); hiy = fmax(hiy, py); hiz = fmax(hiz, pz);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lox = fmin(lox, __shfl_xor_sync(MHPC_FULL, lox, o));
+        loy = fmin(loy, __shfl_xor_sync(MHPC_FULL, loy, o));
+        loz = fmin(loz, __shfl_xor_sync(MHPC_FULL, loz, o));
+        hix = fmax(hix, __shfl_xor_sync(MHPC_FULL, hix, o));
+        hiy = fmax(hiy, __shfl_xor_sync(MHPC_FULL, hiy, o));
+        hiz = fmax(hiz, __shfl_xor_sync(MHPC_FULL, hiz, o));
+    }
+    const double cx = 0.5 * (lox + hix), cy = 0.5 * (loy + hiy), cz = 0.5 * (loz + hiz);
+    const float chx = (float)cx, chy = (float)cy, chz = (float)cz;
+    const float clx = (float)(cx - (double)chx), cly = (float)(cy - (double)chy), clz = (float)(cz - (double)chz);
+    float rx[2], ry[2], rz[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int lf = __ldg(T.leaf_node + sl[k]);
+        const float4 hp = __ldg(T.mpos + lf);
+        const float4 lp = __ldg(T.mlo + lf);
+        rx[k] = (hp.x - chx) + (lp.x - clx);
+        ry[k] = (hp.y - chy) + (lp.y - cly);
+        rz[k] = (hp.z - chz) + (lp.z - clz);
+        // sub-box of members [8b, 8b + 8): 8-lane segments of member row k
+        float bx0 = rx[k], by0 = ry[k], bz0 = rz[k], bx1 = rx[k], by1 = ry[k], bz1 = rz[k];
+#pragma unroll
+        for (int o = 4; o > 0; o >>= 1) {
+            bx0 = fminf(bx0, __shfl_xor_sync(MHPC_FULL, bx0, o));
+            by0 = fminf(by0, __shfl_xor_sync(MHPC_FULL, by0, o));
+            bz0 = fminf(bz0, __shfl_xor_sync(MHPC_FULL, bz0, o));
+            bx1 = fmaxf(bx1, __shfl_xor_sync(MHPC_FULL, bx1, o));
+            by1 = fmaxf(by1, __shfl_xor_sync(MHPC_FULL, by1, o));
+            bz1 = fmaxf(bz1, __shfl_xor_sync(MHPC_FULL, bz1, o));
+        }
+        if ((lane & 7) == 0) {
+            S.blo[4 * k + (lane >> 3)] = make_float4(bx0, by0, bz0, 0.f);
+            S.bhi[4 * k + (lane >> 3)] = make_float4(bx1, by1, bz1, 0.f);
+        }
+    }
+    // the root's children: node 0 and its skip chain
+    int top = 0;
+    if (lane == 0) {
+        int c = 0;
+        while (c < M && top < 8) { S.stk[top++] = c; c = __ldg(&T.link[c].x); }
+        if (c < M) set_status(st, MHPC_ERR_DEPTH, 1);
+    }
+    top = __shfl_sync(MHPC_FULL, top, 0);
+    __syncwarp();
+    double ax[2] = {0.0, 0.0}, ay[2] = {0.0, 0.0}, az[2] = {0.0, 0.0};
+    int ncell = 0, nleaf = 0;
+    unsigned long long tested = 0, ncell_tot = 0, nleaf_tot = 0;
+    while (top > 0) {
+        int room = (kListStack - kListReserve - top) / 7;
+        int k = top < 32 ? top : 32;
+        if (k > room) k = room > 1 ? room : 1;
+        const bool act = lane < k;
+        const int nd = act ? S.stk[top - 1 - lane] : 0;
+        __syncwarp();
+        top -= k;
+        tested += k;
+        bool acc_leaf = false, acc_cell = false, open = false;
+        float nx = 0.f, ny = 0.f, nz = 0.f, m = 0.f;
+        if (act) {
+            const float4 hp = __ldg(T.mpos + nd);
+            const float4 lp = __ldg(T.mlo + nd);
+            const int info = __ldg(&T.link[nd].y);
+            nx = (hp.x - chx) + (lp.x - clx);
+            ny = (hp.y - chy) + (lp.y - cly);
+            nz = (hp.z - chz) + (lp.z - clz);
+            m = hp.w;
+            if (info & ND_LEAF) {
+                acc_leaf = true;
+            } else {
+                bool ok = true;
+#pragma unroll
+                for (int b = 0; b < kListSub; ++b) {
+                    const float4 lo = S.blo[b], hi = S.bhi[b];
+                    const float dx = fmaxf(fmaxf(lo.x - nx, nx - hi.x), 0.f);
+                    const float dy = fmaxf(fmaxf(lo.y - ny, ny - hi.y), 0.f);
+                    const float dz = fmaxf(fmaxf(lo.z - nz, nz - hi.z), 0.f);
+                    ok = ok && lp.w <= fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                }
+                acc_cell = ok;
+                open = !ok;
+            }
+        }
+        const unsigned bl = __ballot_sync(MHPC_FULL, acc_leaf);
+        if (acc_leaf) S.lpos[nleaf + __popc(bl & lt)] = make_float4(nx, ny, nz, m);
+        nleaf += __popc(bl);
+        const unsigned bc = __ballot_sync(MHPC_FULL, acc_cell);
+        if (acc_cell) {
+            const int i = ncell + __popc(bc & lt);
+            S.cpos[i] = make_float4(nx, ny, nz, m);
+            S.cq0[i] = __ldg(T.quad0 + nd);
+            S.cq1[i] = __ldg(T.quad1 + nd);
+        }
+        ncell += __popc(bc);
+        int mask = 0;
+        if (open) mask = __ldg(T.kmask + nd);
+        const bool bucket = open && (mask & 0x100);
+        const unsigned bb = __ballot_sync(MHPC_FULL, bucket);
+        if (bucket) S.defer[__popc(bb & lt)] = nd;
+        const int nkid = (open && !bucket) ? __popc(mask & 0xff) : 0;
+        int incl = nkid;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(MHPC_FULL, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(MHPC_FULL, incl, 31);
+        if (top + total > kListStack) {
+            // unreachable by the bound on k; stop instead of overrunning
+            if (lane == 0) set_status(st, MHPC_ERR_DEPTH, 2);
+            return;
+        }
+        if (nkid) {
+            const int4 k0 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)nd));
+            const int4 k1 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)nd) + 1);
+            const int all[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+            int w = top + incl - nkid;
+#pragma unroll
+            for (int d = 0; d < 8; ++d)
+                if ((mask >> d) & 1) S.stk[w++] = all[d];
+        }
+        top += total;
+        __syncwarp();
+        if (ncell >= 32) {
+            eval_cells(S, ncell, rx, ry, rz, e2, ax, ay, az);
+            ncell_tot += ncell;
+            ncell = 0;
+            __syncwarp();
+        }
+        if (nleaf >= 32) {
+            eval_leaves(S, nleaf, rx, ry, rz, e2, ax, ay, az);
+            nleaf_tot += nleaf;
+            nleaf = 0;
+            __syncwarp();
+        }
+        // shared-key buckets: their children are consecutive leaves (the
+        // leaf list holds fewer than 32 entries here, at most 63 after a round)
+        const int ndefer = __popc(bb);
+        for (int d = 0; d < ndefer; ++d) {
+            const int b = S.defer[d];
+            const int end = __ldg(&T.link[b].x);
+            for (int c0 = b + 1; c0 < end; c0 += 32) {
+                const int c = c0 + lane;
+                const bool a = c < end;
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (a) {
+                    const float4 hp = __ldg(T.mpos + c);
+                    const float4 lp = __ldg(T.mlo + c);
+                    v = make_float4((hp.x - chx) + (lp.x - clx), (hp.y - chy) + (lp.y - cly),
+                                    (hp.z - chz) + (lp.z - clz), hp.w);
+                }
+                const unsigned ba = __ballot_sync(MHPC_FULL, a);
+                if (a) S.lpos[nleaf + __popc(ba & lt)] = v;
+                nleaf += __popc(ba);
+                __syncwarp();
+                if (nleaf >= 32) {
+                    eval_leaves(S, nleaf, rx, ry, rz, e2, ax, ay, az);
+                    nleaf_tot += nleaf;
+                    nleaf = 0;
+                    __syncwarp();
+                }
+            }
+        }
+    }
+    if (ncell) eval_cells(S, ncell, rx, ry, rz, e2, ax, ay, az);
+    if (nleaf) eval_leaves(S, nleaf, rx, ry, rz, e2, ax, ay, az);
+    ncell_tot += ncell;
+    nleaf_tot += nleaf;
+    unsigned nv = 0;
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        if (valid[k]) {
+            const int o = __ldg(perm + s[k]);
+            gax[o] = P.G * ax[k]; gay[o] = P.G * ay[k]; gaz[o] = P.G * az[k];
+        }
+        nv += __popc(__ballot_sync(MHPC_FULL, valid[k]));
+    }
+    if (lane == 0) {
+        atomicAdd(&st->interactions, (ncell_tot + nleaf_tot) * nv);
+        atomicAdd(&st->nodes_visited, tested);
+        atomicAdd(&st->quad_interactions, ncell_tot * nv);
+    }
+}
+
 }  // namespace
 
 int gravity_v2(const TreeDev& T, const GravParams& P, const double* sx, const double* sy, const double* sz,
@@ -255,8 +578,20 @@ int gravity_mixed(const TreeDev& T, const GravParams& P, const double* sx, const
     constexpr int PPL = MHPC_MIXED_PPL;
     long groups = ((long)P.n + 32 * PPL - 1) / (32 * PPL);
     long blocks = (groups * 32 + kWalkBlock - 1) / kWalkBlock;
-    k_grav_mixed<PPL><<<(int)blocks, kWalkBlock, 0, s>>>(T.mpos, T.mlo, T.quad0, T.quad1, T.link, T.nodes, P, sx,
+    k_grav_mixed<PPL><<<(int)blocks, kWalkBlock, 0, s>>>(T.mpos, T.mlo, T.quad0, T.quad1, T.link, T.nodes,
+                                                         T.leaf_node, P, sx,
                                                          sy, sz, sh, perm, gax, gay, gaz, st);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int gravity_lists(const TreeDev& T, const GravParams& P, const double* sx, const double* sy, const double* sz,
+                  const double* sh, const int* perm, double* gax, double* gay, double* gaz, DevStatus* st,
+                  cudaStream_t s) {
+    if (P.n <= 0) return MHPC_OK;
+    const long groups = ((long)P.n + kListGroup - 1) / kListGroup;
+    const long blocks = (groups * 32 + kListBlock - 1) / kListBlock;
+    k_grav_lists<<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

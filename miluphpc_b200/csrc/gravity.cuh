@@ -14,8 +14,15 @@ struct GravParams {
 int gravity_v2(const TreeDev& T, const GravParams& P, const double* sx, const double* sy, const double* sz,
                const double* sh, const int* perm, double* gax, double* gay, double* gaz, DevStatus* st,
                cudaStream_t s);
-// Mixed FP32 walk: hi/lo node positions relative to the group centre, group
-// bounding-box criterion, monopole + quadrupole, FP64 flush of FP32 partial sums.
+// Mixed FP32 walk, per-lane vote: hi/lo node positions relative to the group
+// centre, every particle of the warp votes on each cell, monopole + quadrupole,
+// FP64 flush of FP32 partial sums (precision 2).
 int gravity_mixed(const TreeDev& T, const GravParams& P, const double* sx, const double* sy, const double* sz,
+                  const double* sh, const int* perm, double* gax, double* gay, double* gaz, DevStatus* st,
+                  cudaStream_t s);
+// Mixed FP32 walk with interaction lists: lane-parallel traversal against the
+// sub-boxes of 64-particle groups, accepted cells and leaves evaluated from
+// shared-memory lists (precision 1).
+int gravity_lists(const TreeDev& T, const GravParams& P, const double* sx, const double* sy, const double* sz,
                   const double* sh, const int* perm, double* gax, double* gay, double* gaz, DevStatus* st,
                   cudaStream_t s);

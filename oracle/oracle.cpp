@@ -396,13 +396,14 @@ void orc_quad(const int* child, const int* level, int n, int nodes, int max_leve
 // Group walk of the mixed path in FP64: groups of `gsize` consecutive sorted
 // particles; a cell at level L is accepted for the group when, for every
 // particle p of the group,
-//   edge_L^2 / theta <= |com - p|^2 + eps2
-// (edge_L = 2 radius / 2^L): the reference's squared-ratio criterion with
+//   edge_L^2 / theta <= |com - p|^2
+// (edge_L = 2 radius / 2^L; the softening takes no part in the decision): the
+// reference's squared-ratio criterion with
 // computeForces_v2's all-lanes vote, applied to every level (root children
 // included); accepted cells add their monopole and, if q is given,
 // quadrupole term.  Leaves are exact.  ninter (per particle) receives the
 // number of accepted nodes.
-// With crit != null a cell is accepted when crit[cell] <= min |com - p|^2 + eps2
+// With crit != null a cell is accepted when crit[cell] <= min |com - p|^2
 // (per-cell thresholds, e.g. from orc_cell_bmax2).
 void orc_gravity_group_crit(const double* x, const double* y, const double* z, const double* mass,
                             const double* q, const int* child, const int* level, const int* sorted,
@@ -471,7 +472,7 @@ void orc_gravity_group_crit(const double* x, const double* y, const double* z, c
             }
             double edge = 2.0 * radius * std::ldexp(1.0, -level[nd]);
             double cr = crit ? crit[nd] : edge * edge / theta;
-            if (cr <= d2 + eps2) { acc_nodes.push_back(nd); continue; }
+            if (cr <= d2) { acc_nodes.push_back(nd); continue; }
             for (int i = 0; i < 8; ++i) if (child[8 * nd + i] != -1) stack.push_back(child[8 * nd + i]);
         }
         for (int l = 0; l < lanes; ++l) {
@@ -498,6 +499,93 @@ void orc_gravity_group_crit(const double* x, const double* y, const double* z, c
             }
             gax[s] = ax; gay[s] = ay; gaz[s] = az;
             if (ninter) ninter[s] = (int)acc_nodes.size();
+        }
+    }
+}
+
+// Interaction-list walk of the mixed path in FP64: groups of `gsize`
+// consecutive sorted particles, each split into `nsub` sub-boxes of gsize/nsub
+// consecutive particles (axis-aligned bounding boxes of their positions).  A
+// cell is accepted for the group when, for every sub-box b,
+//   edge_L^2 / theta <= dist(com, box_b)^2
+// (edge_L = 2 radius / 2^L, distance 0 inside the box); otherwise it is
+// opened.  Leaves are always accepted (exact).  Accepted cells add their
+// monopole and quadrupole terms, accepted leaves their monopole; the softened
+// distance |R|^2 + eps2 is used for the interaction, and eps2_i = eps2 +
+// (h_factor h_i)^2 per particle when h is given.  ninter receives the number
+// of accepted nodes, nquad the number of accepted cells (per particle).
+void orc_gravity_boxes(const double* x, const double* y, const double* z, const double* mass,
+                       const double* q, const int* child, const int* level, const int* sorted,
+                       int n, int gsize, int nsub, double radius, double theta, double eps2,
+                       const double* h, double h_factor, double* gax, double* gay, double* gaz,
+                       int* ninter, int* nquad) {
+    const int ngroups = (n + gsize - 1) / gsize;
+    const int w = gsize / nsub;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int g = 0; g < ngroups; ++g) {
+        const int base = g * gsize;
+        const int lanes = std::min(gsize, n - base);
+        // sub-box b covers group members [b*w, (b+1)*w); members past n
+        // repeat the last particle (as the device kernel loads them)
+        std::vector<double> lo(3 * nsub, 1e300), hi(3 * nsub, -1e300);
+        for (int j = 0; j < gsize; ++j) {
+            const int s = sorted[std::min(base + j, n - 1)];
+            const int b = j / w;
+            const double p[3] = {x[s], y[s], z[s]};
+            for (int d = 0; d < 3; ++d) {
+                lo[3 * b + d] = std::min(lo[3 * b + d], p[d]);
+                hi[3 * b + d] = std::max(hi[3 * b + d], p[d]);
+            }
+        }
+        std::vector<int> stack;
+        for (int i = 0; i < 8; ++i) if (child[i] != -1) stack.push_back(child[i]);
+        std::vector<int> acc_nodes;
+        int ncell = 0;
+        while (!stack.empty()) {
+            int nd = stack.back(); stack.pop_back();
+            if (nd < n) { acc_nodes.push_back(nd); continue; }
+            const double edge = 2.0 * radius * std::ldexp(1.0, -level[nd]);
+            const double cr = edge * edge / theta;
+            const double c[3] = {x[nd], y[nd], z[nd]};
+            bool ok = true;
+            for (int b = 0; b < nsub && ok; ++b) {
+                double d2 = 0.0;
+                for (int d = 0; d < 3; ++d) {
+                    const double e = std::max(std::max(lo[3 * b + d] - c[d], c[d] - hi[3 * b + d]), 0.0);
+                    d2 += e * e;
+                }
+                ok = cr <= d2;
+            }
+            if (ok) { acc_nodes.push_back(nd); ++ncell; continue; }
+            for (int i = 0; i < 8; ++i) if (child[8 * nd + i] != -1) stack.push_back(child[8 * nd + i]);
+        }
+        for (int l = 0; l < lanes; ++l) {
+            const int s = sorted[base + l];
+            double e2 = eps2;
+            if (h && h_factor > 0.0) { const double e = h_factor * h[s]; e2 += e * e; }
+            double ax = 0, ay = 0, az = 0;
+            for (int nd : acc_nodes) {
+                if (nd == s) continue;
+                double R[3] = {x[s] - x[nd], y[s] - y[nd], z[s] - z[nd]};
+                double r2 = R[0] * R[0] + R[1] * R[1] + R[2] * R[2] + e2;
+                double ri = 1.0 / std::sqrt(r2), ri2 = ri * ri, ri3 = ri * ri2;
+                double m = mass[nd];
+                ax -= m * ri3 * R[0]; ay -= m * ri3 * R[1]; az -= m * ri3 * R[2];
+                if (q && nd >= n) {
+                    const double* Q = q + 6 * nd;
+                    double QR[3] = {Q[0] * R[0] + Q[1] * R[1] + Q[2] * R[2],
+                                    Q[1] * R[0] + Q[3] * R[1] + Q[4] * R[2],
+                                    Q[2] * R[0] + Q[4] * R[1] + Q[5] * R[2]};
+                    double RQR = R[0] * QR[0] + R[1] * QR[1] + R[2] * QR[2];
+                    double ri5 = ri3 * ri2, ri7 = ri5 * ri2;
+                    ax += QR[0] * ri5 - 2.5 * RQR * R[0] * ri7;
+                    ay += QR[1] * ri5 - 2.5 * RQR * R[1] * ri7;
+                    az += QR[2] * ri5 - 2.5 * RQR * R[2] * ri7;
+                }
+            }
+            gax[s] = ax; gay[s] = ay; gaz[s] = az;
+            if (ninter) ninter[s] = (int)acc_nodes.size();
+            if (nquad) nquad[s] = ncell;
         }
     }
 }

@@ -75,6 +75,9 @@ def lib():
         L.orc_gravity_group.argtypes = [_d, _d, _d, _d, _d, _i, _i, _i, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                         _d, _d, _d, _i]
+        L.orc_gravity_boxes.argtypes = [_d, _d, _d, _d, _d, _i, _i, _i, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_double, ctypes.c_double, ctypes.c_double, _d, ctypes.c_double,
+                                        _d, _d, _d, _i, _i]
         _lib = L
     return _lib
 
@@ -275,3 +278,18 @@ def gravity_group_crit(tree, sorted_perm, crit, eps2, q=None, gsize=32):
                                  _p(tree.level, _i), _p(sp, _i), n, int(gsize), 1.0, 1.0, float(eps2),
                                  _p(ax), _p(ay), _p(az), _p(cnt, _i), _p(crit))
     return ax, ay, az, cnt
+
+
+def gravity_boxes(tree, sorted_perm, radius, theta, eps2, q, gsize=64, nsub=8, h=None, h_factor=0.0):
+    """Interaction-list walk of the mixed path in FP64 (sub-box criterion)."""
+    n = tree.n
+    ax = np.zeros(n); ay = np.zeros(n); az = np.zeros(n)
+    cnt = np.zeros(n, dtype=np.int32)
+    nq = np.zeros(n, dtype=np.int32)
+    sp = np.ascontiguousarray(sorted_perm, dtype=np.int32)
+    hh = _f64(h) if h is not None else None
+    lib().orc_gravity_boxes(_p(tree.x), _p(tree.y), _p(tree.z), _p(tree.m), _p(q), _p(tree.child, _i),
+                            _p(tree.level, _i), _p(sp, _i), n, int(gsize), int(nsub), float(radius),
+                            float(theta), float(eps2), _p(hh) if hh is not None else None, float(h_factor),
+                            _p(ax), _p(ay), _p(az), _p(cnt, _i), _p(nq, _i))
+    return ax, ay, az, cnt, nq
