@@ -385,7 +385,7 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
     A(T.com, M); A(T.bmin, M); A(T.bmax, M); A(T.hmax, M);
     A(T.root_nchild, 1); A(T.nodes, 1);
     if (cfg->gravity) {
-        A(T.quad0, M); A(T.quad1, M); A(T.mpos, M); A(T.mlo, M);
+        A(T.quad0, M); A(T.quad1, M); A(T.wrec, 4 * M);
     }
     if (cfg->sph) {
         A(c->svx, n); A(c->svy, n); A(c->svz, n); A(c->se, n); A(c->srho, n); A(c->sp, n); A(c->scs, n);

@@ -111,8 +111,7 @@ constexpr int kFlush = 64;
 // all of them, which amortises the per-node instructions over PPL
 // interactions (the kernel is issue-bound, not memory-bound).
 template <int PPL>
-__global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restrict__ mpos, const float4* __restrict__ mlo,
-                                                           const float4* __restrict__ q0, const float2* __restrict__ q1,
+__global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restrict__ wrec,
                                                            const int2* __restrict__ link, const int* __restrict__ nodes_total,
                                                            const int* __restrict__ leaf_node,
                                                            GravParams P, const double* __restrict__ sx,
@@ -162,8 +161,8 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restr
         // the particle's offset is formed exactly like its own leaf's, so the
         // self-interaction has R = 0 (a one-ulp mismatch would leave m R / eps^3)
         const int lf = __ldg(leaf_node + (valid[k] ? s[k] : (long)P.n - 1));
-        const float4 hp = __ldg(mpos + lf);
-        const float4 lp = __ldg(mlo + lf);
+        const float4 hp = __ldg(wrec + 4 * (size_t)lf);
+        const float4 lp = __ldg(wrec + 4 * (size_t)lf + 1);
         rx[k] = (hp.x - chx) + (lp.x - clx);
         ry[k] = (hp.y - chy) + (lp.y - cly);
         rz[k] = (hp.z - chz) + (lp.z - clz);
@@ -175,8 +174,8 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restr
     unsigned ninter = 0, nvisit = 0, nquad = 0;
     int nd = 0;
     while (nd < M) {
-        const float4 hp = __ldg(mpos + nd);
-        const float4 lp = __ldg(mlo + nd);
+        const float4 hp = __ldg(wrec + 4 * (size_t)nd);
+        const float4 lp = __ldg(wrec + 4 * (size_t)nd + 1);
         const int2 lk = __ldg(link + nd);
         ++nvisit;
         const float nx = (hp.x - chx) + (lp.x - clx);
@@ -195,7 +194,12 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restr
         if (!leaf && !__all_sync(MHPC_FULL, far)) { ++nd; continue; }
         float4 a0;
         float2 a1;
-        if (!leaf) { a0 = __ldg(q0 + nd); a1 = __ldg(q1 + nd); ++nquad; }
+        if (!leaf) {
+            a0 = __ldg(wrec + 4 * (size_t)nd + 2);
+            const float4 a3 = __ldg(wrec + 4 * (size_t)nd + 3);
+            a1 = make_float2(a3.x, a3.y);
+            ++nquad;
+        }
 #pragma unroll
         for (int k = 0; k < PPL; ++k) {
             const float ri = r2[k] > 0.f ? rsqrtf(r2[k]) : 0.f;
@@ -283,11 +287,15 @@ struct ListSmem {
     int defer[32];
 };
 
+// kGuard: some softened distance may be 0 (eps2 = 0), so 1/r is guarded; with
+// eps2 >= 1e-20 every r^2 >= eps2 keeps 1/r^3 finite and the guard is dropped
+// (it costs 11 % of the walk's instructions).
+template <bool kGuard>
 __device__ __forceinline__ void eval_cells(const ListSmem& S, int count, const float (&rx)[2], const float (&ry)[2],
                                            const float (&rz)[2], const float (&e2)[2], double (&ax)[2],
                                            double (&ay)[2], double (&az)[2]) {
     float fx[2] = {0.f, 0.f}, fy[2] = {0.f, 0.f}, fz[2] = {0.f, 0.f};
-#pragma unroll 2
+#pragma unroll 4
     for (int e = 0; e < count; ++e) {
         const float4 c = S.cpos[e];
         const float4 a0 = S.cq0[e];
@@ -296,7 +304,7 @@ __device__ __forceinline__ void eval_cells(const ListSmem& S, int count, const f
         for (int k = 0; k < 2; ++k) {
             const float Rx = rx[k] - c.x, Ry = ry[k] - c.y, Rz = rz[k] - c.z;
             const float r2 = fmaf(Rx, Rx, fmaf(Ry, Ry, fmaf(Rz, Rz, e2[k])));
-            const float ri = r2 > 0.f ? rsqrtf(r2) : 0.f;
+            const float ri = kGuard ? (r2 > 0.f ? rsqrtf(r2) : 0.f) : rsqrtf(r2);
             const float ri2 = ri * ri;
             const float ri3 = ri * ri2;
             const float ri5 = ri3 * ri2;
@@ -315,18 +323,19 @@ __device__ __forceinline__ void eval_cells(const ListSmem& S, int count, const f
     for (int k = 0; k < 2; ++k) { ax[k] += fx[k]; ay[k] += fy[k]; az[k] += fz[k]; }
 }
 
+template <bool kGuard>
 __device__ __forceinline__ void eval_leaves(const ListSmem& S, int count, const float (&rx)[2], const float (&ry)[2],
                                             const float (&rz)[2], const float (&e2)[2], double (&ax)[2],
                                             double (&ay)[2], double (&az)[2]) {
     float fx[2] = {0.f, 0.f}, fy[2] = {0.f, 0.f}, fz[2] = {0.f, 0.f};
-#pragma unroll 2
+#pragma unroll 4
     for (int e = 0; e < count; ++e) {
         const float4 c = S.lpos[e];
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             const float Rx = rx[k] - c.x, Ry = ry[k] - c.y, Rz = rz[k] - c.z;
             const float r2 = fmaf(Rx, Rx, fmaf(Ry, Ry, fmaf(Rz, Rz, e2[k])));
-            const float ri = r2 > 0.f ? rsqrtf(r2) : 0.f;
+            const float ri = kGuard ? (r2 > 0.f ? rsqrtf(r2) : 0.f) : rsqrtf(r2);
             const float mri3 = c.w * (ri * ri * ri);
             fx[k] = fmaf(-mri3, Rx, fx[k]);
             fy[k] = fmaf(-mri3, Ry, fy[k]);
@@ -339,6 +348,7 @@ __device__ __forceinline__ void eval_leaves(const ListSmem& S, int count, const 
 
 constexpr int kListBlock = 128;
 
+template <bool kGuard>
 __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams P, const double* __restrict__ sx,
                                                            const double* __restrict__ sy,
                                                            const double* __restrict__ sz,
@@ -389,8 +399,8 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
         const int lf = __ldg(T.leaf_node + sl[k]);
-        const float4 hp = __ldg(T.mpos + lf);
-        const float4 lp = __ldg(T.mlo + lf);
+        const float4 hp = __ldg(T.wrec + 4 * (size_t)lf);
+        const float4 lp = __ldg(T.wrec + 4 * (size_t)lf + 1);
         rx[k] = (hp.x - chx) + (lp.x - clx);
         ry[k] = (hp.y - chy) + (lp.y - cly);
         rz[k] = (hp.z - chz) + (lp.z - clz);
@@ -433,10 +443,16 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
         tested += k;
         bool acc_leaf = false, acc_cell = false, open = false;
         float nx = 0.f, ny = 0.f, nz = 0.f, m = 0.f;
+        float4 w2 = make_float4(0.f, 0.f, 0.f, 0.f), w3 = make_float4(0.f, 0.f, 0.f, 0.f);
         if (act) {
-            const float4 hp = __ldg(T.mpos + nd);
-            const float4 lp = __ldg(T.mlo + nd);
-            const int info = __ldg(&T.link[nd].y);
+            // the node's whole record (one 64-byte line): position, criterion,
+            // quadrupole and child mask arrive in one round trip
+            const float4* w = T.wrec + 4 * (size_t)nd;
+            const float4 hp = __ldg(w);
+            const float4 lp = __ldg(w + 1);
+            w2 = __ldg(w + 2);
+            w3 = __ldg(w + 3);
+            const int info = __float_as_int(w3.z);
             nx = (hp.x - chx) + (lp.x - clx);
             ny = (hp.y - chy) + (lp.y - cly);
             nz = (hp.z - chz) + (lp.z - clz);
@@ -464,12 +480,11 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
         if (acc_cell) {
             const int i = ncell + __popc(bc & lt);
             S.cpos[i] = make_float4(nx, ny, nz, m);
-            S.cq0[i] = __ldg(T.quad0 + nd);
-            S.cq1[i] = __ldg(T.quad1 + nd);
+            S.cq0[i] = w2;
+            S.cq1[i] = make_float2(w3.x, w3.y);
         }
         ncell += __popc(bc);
-        int mask = 0;
-        if (open) mask = __ldg(T.kmask + nd);
+        const int mask = open ? __float_as_int(w3.w) : 0;
         const bool bucket = open && (mask & 0x100);
         const unsigned bb = __ballot_sync(MHPC_FULL, bucket);
         if (bucket) S.defer[__popc(bb & lt)] = nd;
@@ -498,13 +513,13 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
         top += total;
         __syncwarp();
         if (ncell >= 32) {
-            eval_cells(S, ncell, rx, ry, rz, e2, ax, ay, az);
+            eval_cells<kGuard>(S, ncell, rx, ry, rz, e2, ax, ay, az);
             ncell_tot += ncell;
             ncell = 0;
             __syncwarp();
         }
         if (nleaf >= 32) {
-            eval_leaves(S, nleaf, rx, ry, rz, e2, ax, ay, az);
+            eval_leaves<kGuard>(S, nleaf, rx, ry, rz, e2, ax, ay, az);
             nleaf_tot += nleaf;
             nleaf = 0;
             __syncwarp();
@@ -520,8 +535,8 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
                 const bool a = c < end;
                 float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (a) {
-                    const float4 hp = __ldg(T.mpos + c);
-                    const float4 lp = __ldg(T.mlo + c);
+                    const float4 hp = __ldg(T.wrec + 4 * (size_t)c);
+                    const float4 lp = __ldg(T.wrec + 4 * (size_t)c + 1);
                     v = make_float4((hp.x - chx) + (lp.x - clx), (hp.y - chy) + (lp.y - cly),
                                     (hp.z - chz) + (lp.z - clz), hp.w);
                 }
@@ -530,7 +545,7 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
                 nleaf += __popc(ba);
                 __syncwarp();
                 if (nleaf >= 32) {
-                    eval_leaves(S, nleaf, rx, ry, rz, e2, ax, ay, az);
+                    eval_leaves<kGuard>(S, nleaf, rx, ry, rz, e2, ax, ay, az);
                     nleaf_tot += nleaf;
                     nleaf = 0;
                     __syncwarp();
@@ -538,8 +553,8 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
             }
         }
     }
-    if (ncell) eval_cells(S, ncell, rx, ry, rz, e2, ax, ay, az);
-    if (nleaf) eval_leaves(S, nleaf, rx, ry, rz, e2, ax, ay, az);
+    if (ncell) eval_cells<kGuard>(S, ncell, rx, ry, rz, e2, ax, ay, az);
+    if (nleaf) eval_leaves<kGuard>(S, nleaf, rx, ry, rz, e2, ax, ay, az);
     ncell_tot += ncell;
     nleaf_tot += nleaf;
     unsigned nv = 0;
@@ -578,8 +593,7 @@ int gravity_mixed(const TreeDev& T, const GravParams& P, const double* sx, const
     constexpr int PPL = MHPC_MIXED_PPL;
     long groups = ((long)P.n + 32 * PPL - 1) / (32 * PPL);
     long blocks = (groups * 32 + kWalkBlock - 1) / kWalkBlock;
-    k_grav_mixed<PPL><<<(int)blocks, kWalkBlock, 0, s>>>(T.mpos, T.mlo, T.quad0, T.quad1, T.link, T.nodes,
-                                                         T.leaf_node, P, sx,
+    k_grav_mixed<PPL><<<(int)blocks, kWalkBlock, 0, s>>>(T.wrec, T.link, T.nodes, T.leaf_node, P, sx,
                                                          sy, sz, sh, perm, gax, gay, gaz, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
@@ -591,7 +605,12 @@ int gravity_lists(const TreeDev& T, const GravParams& P, const double* sx, const
     if (P.n <= 0) return MHPC_OK;
     const long groups = ((long)P.n + kListGroup - 1) / kListGroup;
     const long blocks = (groups * 32 + kListBlock - 1) / kListBlock;
-    k_grav_lists<<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st);
+    // the self-interaction has R = 0 and r^2 = eps2: 1/r^3 stays finite in
+    // FP32 for eps2 >= 1e-20
+    if (P.eps2 >= 1e-20)
+        k_grav_lists<false><<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st);
+    else
+        k_grav_lists<true><<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

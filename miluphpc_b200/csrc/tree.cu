@@ -310,8 +310,15 @@ __global__ void __launch_bounds__(256) k_mixed_nodes(TreeDev T, const long long*
             const double e = ldexp(edge0, -(info & 0xff));
             crit = (float)(e * e * inv_theta);
         }
-        T.mpos[i] = make_float4(hx, hy, hz, (float)c.w);
-        T.mlo[i] = make_float4((float)(c.x - (double)hx), (float)(c.y - (double)hy), (float)(c.z - (double)hz), crit);
+        float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f);
+        float2 q1 = make_float2(0.f, 0.f);
+        int mask = 0;
+        if (!(info & ND_LEAF)) { q0 = T.quad0[i]; q1 = T.quad1[i]; mask = T.kmask[i]; }
+        float4* w = T.wrec + 4 * (size_t)i;
+        w[0] = make_float4(hx, hy, hz, (float)c.w);
+        w[1] = make_float4((float)(c.x - (double)hx), (float)(c.y - (double)hy), (float)(c.z - (double)hz), crit);
+        w[2] = q0;
+        w[3] = make_float4(q1.x, q1.y, __int_as_float(info), __int_as_float(mask));
     }
 }
 

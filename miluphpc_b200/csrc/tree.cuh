@@ -36,8 +36,11 @@ struct TreeDev {
     float4* bmax;       // [cap] particle bounding box max (rounded up)
     float4* quad0;      // [cap] traceless quadrupole Qxx Qxy Qxz Qyy (about com)
     float2* quad1;      // [cap] Qyz Qzz
-    float4* mpos;       // [cap] mixed path: float(x), float(y), float(z), m
-    float4* mlo;        // [cap] mixed path: x - float(x), ..., opening criterion edge^2/theta
+    // [4 * cap] mixed-path walk record, one 64-byte line per node:
+    //   [0] float(x), float(y), float(z), m   (FP32 hi part of the centre of mass)
+    //   [1] x - float(x), ..., opening criterion edge^2/theta (-1 for leaves)
+    //   [2] Qxx Qxy Qxz Qyy   [3] Qyz Qzz, link info bits, kmask bits
+    float4* wrec;
     float* hmax;        // [cap] largest smoothing length below the node (rounded up)
     int* root_nchild;   // [1]
     int* nodes;         // [1] total nodes (= off[n]), device copy
