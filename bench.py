@@ -30,10 +30,10 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     # Plummer at scale, precision form: N = 2^24, Hilbert keys, leapfrog dt 0.01
     "plummer16m": dict(kind="gravity", n=1 << 24, sfc=1, dt=0.01, eps2=1e-4, theta=0.5, theta_mixed=0.28,
-                       theta_plain_matched=0.1, seed=1),
+                       mac_alpha=1.8e-3, theta_plain_matched=0.1, seed=1),
     # profiling case of the walk: node data (~190 MB) larger than L2
     "plummer2m": dict(kind="gravity", n=1 << 21, sfc=1, dt=0.01, eps2=1e-4, theta=0.5, theta_mixed=0.28,
-                      theta_plain_matched=0.1, seed=1),
+                      mac_alpha=1.8e-3, theta_plain_matched=0.1, seed=1),
     # Sedov blast, SPH only: 128^3 lattice, fixed h = 2.5 dx, predictor-corrector
     "sedov2m": dict(kind="sph", nside=128, n=128 ** 3, sfc=0, dt_max=1e-4, seed=2),
     "sedov262k": dict(kind="sph", nside=64, n=64 ** 3, sfc=0, dt_max=1e-4, seed=2),
@@ -44,7 +44,7 @@ WORKLOADS = {
                     theta_plain_matched=0.1, train_steps=20, train_iters=1500, seed=3),
     # the reference's own single-rank case: N = 131072, Lebesgue, leapfrog dt 0.025
     "plummer131k": dict(kind="gravity", n=131072, sfc=0, dt=0.025, eps2=1e-4, theta=0.5, theta_mixed=0.28,
-                        theta_plain_matched=0.1, seed=1),
+                        mac_alpha=1.8e-3, theta_plain_matched=0.1, seed=1),
 }
 
 FLOP_MONO = 19   # flop per accepted particle-node monopole interaction
@@ -165,6 +165,10 @@ def make_sim(wl, state, variant):
               theta=wl["theta"], theta_mixed=wl["theta_mixed"])
     if variant == "mixed":
         kw["precision"] = wl.get("mixed_precision", 1)
+        if wl.get("mac_alpha"):
+            # relative opening rule from the second right-hand side on
+            kw["gravity_mac"] = 1
+            kw["mac_alpha"] = wl["mac_alpha"]
     elif variant == "plain_matched":
         kw["theta"] = wl["theta_plain_matched"]
     cfg = _lib.default_config(**kw)
@@ -309,6 +313,10 @@ def run_ours(args, wl):
                        (wl["theta_plain_matched"] if args.variant == "plain_matched" else wl["theta"]),
                        "sfc": "hilbert" if wl["sfc"] else "lebesgue", "integrator": "leapfrog", "dt": wl["dt"],
                        "eps2": wl["eps2"], "parallelism": "replicas" if world > 1 else "single",
+                       "opening_rule": ("relative: d >= l and M l^3 <= %g |a_prev| d^5 (geometric theta %.2f on "
+                                        "the first RHS)" % (wl["mac_alpha"], wl["theta_mixed"]))
+                       if args.variant == "mixed" and wl.get("mac_alpha") and wl.get("mixed_precision", 1) == 1
+                       else "geometric",
                        "l2": "inputs larger than L2 (positions alone %.0f MB)" % (n * 24 / 1e6)}
         out = {
             "metric": "particle-steps/s on 1 B200: mixed/learned vs plain at rel. force err <=1e-3",
@@ -509,12 +517,16 @@ def main():
     ap.add_argument("--cpu-sample-groups", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--theta-mixed", type=float, default=None, help="override the mixed walk's opening parameter")
+    ap.add_argument("--mac-alpha", type=float, default=None,
+                    help="relative opening rule of the list walk (0: geometric rule only)")
     ap.add_argument("--mixed-walk", default="lists", choices=["lists", "vote"],
                     help="mixed walk: interaction lists (precision 1) or per-lane vote (precision 2)")
     args = ap.parse_args()
     wl = dict(WORKLOADS[args.workload])
     if args.theta_mixed is not None:
         wl["theta_mixed"] = args.theta_mixed
+    if args.mac_alpha is not None:
+        wl["mac_alpha"] = args.mac_alpha
     wl["mixed_precision"] = 1 if args.mixed_walk == "lists" else 2
     if args.impl == "reference":
         out = run_reference(args, wl)

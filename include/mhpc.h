@@ -83,6 +83,13 @@ typedef struct mhpc_config {
     int softening_mode;        /* 0 global eps^2, 1 eps_i = softening_h_factor * h_i (plus eps^2) */
     double softening_h_factor;
     double node_pool_factor;   /* tree cell pool = node_pool_factor * capacity + 20000 */
+    int gravity_mac;           /* mixed walk (precision 1) opening rule: 0 geometric (theta_mixed); 1
+                                  relative: a cell of mass M, edge l is accepted for a group only if
+                                  d >= l and M l^3 <= mac_alpha |a| d^5 (d: distance from the cell's
+                                  centre of mass to the group, |a|: the group's smallest acceleration of
+                                  the previous right-hand side, found in g_ax/g_ay/g_az when the walk
+                                  starts); the first gravity call on a context uses the geometric rule */
+    double mac_alpha;          /* accuracy parameter of the relative rule (0.003: p99 force error ~8e-4) */
 } mhpc_config;
 
 /* Material (include/materials/material.cuh:123-150), one entry of the

@@ -192,6 +192,8 @@ void mhpc_config_default(mhpc_config* c) {
     c->theta_mixed = 0.25;
     c->softening_h_factor = 0.0;
     c->node_pool_factor = 1.0;
+    c->gravity_mac = 0;
+    c->mac_alpha = 0.003;
 }
 
 int mhpc_config_from_info(const char* path, mhpc_config* c) {
@@ -234,6 +236,10 @@ int mhpc_config_from_info(const char* path, mhpc_config* c) {
     b("learnedSml", &c->learned_h);
     i("softeningMode", &c->softening_mode);
     f("softeningHFactor", &c->softening_h_factor);
+    i("gravityMac", &c->gravity_mac);
+    f("macAlpha", &c->mac_alpha);
+    if (c->gravity_mac < 0 || c->gravity_mac > 1 || (c->gravity_mac == 1 && c->mac_alpha <= 0))
+        return MHPC_ERR_CONFIG;
     if (c->integrator < 0 || c->integrator > 2 || c->sfc < 0 || c->sfc > 1 || c->theta <= 0 ||
         c->smoothing_kernel < 0 || c->smoothing_kernel > 4 || c->max_num_interactions <= 0)
         return MHPC_ERR_CONFIG;

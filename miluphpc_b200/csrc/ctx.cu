@@ -55,6 +55,9 @@ struct mhpc_ctx {
     cudaEvent_t ev[EV_COUNT];
     bool ev_recorded[EV_COUNT];
     bool first_rhs_done = false;
+    // particle count of the last gravity walk, -1 before the first: the
+    // relative opening rule reads that walk's accelerations from g_ax/g_ay/g_az
+    int grav_prev_n = -1;
     int last_n = 0;
     // predictor-corrector: predicted state (IntegratedParticles), step size on the device
     mhpc_particles pred;
@@ -168,7 +171,7 @@ int stage_tree(mhpc_ctx* c, const mhpc_particles* p) {
     TRY(tree_build(c->T, c->skey, c->scan_scratch, c->st, s));
     record(c, EV_TREE);
     const int want_quad = c->cfg.gravity && c->cfg.precision >= 1;
-    TRY(tree_upward(c->T, c->sx, c->sy, c->sz, c->sm, want_quad, c->st, s));
+    TRY(tree_upward(c->T, c->sx, c->sy, c->sz, c->sm, want_quad, c->cfg.sph ? 1 : 0, c->st, s));
     if (want_quad) TRY(tree_mixed_nodes(c->T, c->ord, c->cfg.theta_mixed, c->st, s));
     record(c, EV_COM);
     return MHPC_OK;
@@ -184,6 +187,7 @@ int stage_gravity(mhpc_ctx* c, const mhpc_particles* p) {
     G.ord = c->ord;
     if (c->cfg.precision == 1) {
         G.theta = c->cfg.theta_mixed;
+        G.rel_alpha = (c->cfg.gravity_mac == 1 && c->grav_prev_n == p->n) ? c->cfg.mac_alpha : 0.0;
         TRY(gravity_lists(c->T, G, c->sx, c->sy, c->sz, c->sh, c->perm, p->g_ax, p->g_ay, p->g_az, c->st,
                           c->stream));
     } else if (c->cfg.precision == 2) {
@@ -195,6 +199,7 @@ int stage_gravity(mhpc_ctx* c, const mhpc_particles* p) {
         TRY(gravity_v2(c->T, G, c->sx, c->sy, c->sz, c->sh, c->perm, p->g_ax, p->g_ay, p->g_az, c->st,
                        c->stream));
     }
+    c->grav_prev_n = p->n;
     record(c, EV_GRAV);
     return MHPC_OK;
 }
@@ -380,9 +385,10 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
     T.n = 0;
     T.cap_nodes = c->cap_nodes;
     A(T.dl, n); A(T.cnt, n); A(T.off, n + 1); A(T.leaf_node, n);
-    A(T.link, M); A(T.first, M); A(T.last, M); A(T.parent, M); A(T.nchild, M); A(T.arrive, M);
+    A(T.link, M); A(T.first, M); A(T.last, M); A(T.parent, M); A(T.nchild, M);
     A(T.kids, 8 * M); A(T.kmask, M);
     A(T.com, M); A(T.bmin, M); A(T.bmax, M); A(T.hmax, M);
+    A(T.level_cells, M); A(T.level_off, 64);
     A(T.root_nchild, 1); A(T.nodes, 1);
     if (cfg->gravity) {
         A(T.quad0, M); A(T.quad1, M); A(T.wrec, 4 * M);

@@ -348,7 +348,7 @@ __device__ __forceinline__ void eval_leaves(const ListSmem& S, int count, const 
 
 constexpr int kListBlock = 128;
 
-template <bool kGuard>
+template <bool kGuard, bool kRel>
 __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams P, const double* __restrict__ sx,
                                                            const double* __restrict__ sy,
                                                            const double* __restrict__ sz,
@@ -404,7 +404,15 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
         rx[k] = (hp.x - chx) + (lp.x - clx);
         ry[k] = (hp.y - chy) + (lp.y - cly);
         rz[k] = (hp.z - chz) + (lp.z - clz);
-        // sub-box of members [8b, 8b + 8): 8-lane segments of member row k
+        // sub-box of members [8b, 8b + 8): 8-lane segments of member row k;
+        // relative rule: alpha times the smallest previous |a| of the sub-box
+        // (read before this walk overwrites the accelerations)
+        float amin = 0.f;
+        if (kRel) {
+            const int o = __ldg(perm + sl[k]);
+            const double gx = gax[o], gy = gay[o], gz = gaz[o];
+            amin = (float)(P.rel_alpha * sqrt(gx * gx + gy * gy + gz * gz));
+        }
         float bx0 = rx[k], by0 = ry[k], bz0 = rz[k], bx1 = rx[k], by1 = ry[k], bz1 = rz[k];
 #pragma unroll
         for (int o = 4; o > 0; o >>= 1) {
@@ -413,13 +421,16 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
             bz0 = fminf(bz0, __shfl_xor_sync(MHPC_FULL, bz0, o));
             bx1 = fmaxf(bx1, __shfl_xor_sync(MHPC_FULL, bx1, o));
             by1 = fmaxf(by1, __shfl_xor_sync(MHPC_FULL, by1, o));
+            if (kRel) amin = fminf(amin, __shfl_xor_sync(MHPC_FULL, amin, o));
             bz1 = fmaxf(bz1, __shfl_xor_sync(MHPC_FULL, bz1, o));
         }
         if ((lane & 7) == 0) {
-            S.blo[4 * k + (lane >> 3)] = make_float4(bx0, by0, bz0, 0.f);
+            S.blo[4 * k + (lane >> 3)] = make_float4(bx0, by0, bz0, amin);
             S.bhi[4 * k + (lane >> 3)] = make_float4(bx1, by1, bz1, 0.f);
         }
     }
+    const double edge0 = ord_to_dbl(P.ord[1]) - ord_to_dbl(P.ord[0]);
+    const float edge2 = (float)(edge0 * edge0);
     // the root's children: node 0 and its skip chain
     int top = 0;
     if (lane == 0) {
@@ -452,7 +463,8 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
             const float4 lp = __ldg(w + 1);
             w2 = __ldg(w + 2);
             w3 = __ldg(w + 3);
-            const int info = __float_as_int(w3.z);
+            const int bits = __float_as_int(w3.z);
+            const int info = bits & 0x1ff;
             nx = (hp.x - chx) + (lp.x - clx);
             ny = (hp.y - chy) + (lp.y - cly);
             nz = (hp.z - chz) + (lp.z - clz);
@@ -460,6 +472,8 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
             if (info & ND_LEAF) {
                 acc_leaf = true;
             } else {
+                // kRel: squared edge of the cell, edge0^2 / 4^level (exact power of two)
+                const float l2 = kRel ? edge2 * __int_as_float((127 - 2 * (info & 0xff)) << 23) : 0.f;
                 bool ok = true;
 #pragma unroll
                 for (int b = 0; b < kListSub; ++b) {
@@ -467,7 +481,14 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
                     const float dx = fmaxf(fmaxf(lo.x - nx, nx - hi.x), 0.f);
                     const float dy = fmaxf(fmaxf(lo.y - ny, ny - hi.y), 0.f);
                     const float dz = fmaxf(fmaxf(lo.z - nz, nz - hi.z), 0.f);
-                    ok = ok && lp.w <= fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                    if (kRel) {
+                        // safety bound d >= l, then M l^3 <= alpha |a| d^5
+                        // (d2 = 0 gives NaN: not accepted)
+                        ok = ok && l2 <= d2 && w3.w <= lo.w * (d2 * d2) * (d2 * rsqrtf(d2));
+                    } else {
+                        ok = ok && lp.w <= d2;
+                    }
                 }
                 acc_cell = ok;
                 open = !ok;
@@ -484,7 +505,7 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
             S.cq1[i] = make_float2(w3.x, w3.y);
         }
         ncell += __popc(bc);
-        const int mask = open ? __float_as_int(w3.w) : 0;
+        const int mask = open ? (__float_as_int(w3.z) >> 9) : 0;
         const bool bucket = open && (mask & 0x100);
         const unsigned bb = __ballot_sync(MHPC_FULL, bucket);
         if (bucket) S.defer[__popc(bb & lt)] = nd;
@@ -607,10 +628,15 @@ int gravity_lists(const TreeDev& T, const GravParams& P, const double* sx, const
     const long blocks = (groups * 32 + kListBlock - 1) / kListBlock;
     // the self-interaction has R = 0 and r^2 = eps2: 1/r^3 stays finite in
     // FP32 for eps2 >= 1e-20
-    if (P.eps2 >= 1e-20)
-        k_grav_lists<false><<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st);
+    const bool guard = !(P.eps2 >= 1e-20), rel = P.rel_alpha > 0.0;
+    if (!guard && !rel)
+        k_grav_lists<false, false><<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st);
+    else if (!guard && rel)
+        k_grav_lists<false, true><<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st);
+    else if (guard && !rel)
+        k_grav_lists<true, false><<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st);
     else
-        k_grav_lists<true><<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st);
+        k_grav_lists<true, true><<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

@@ -8,6 +8,8 @@ struct GravParams {
     double G;             // gravitational constant (1 unless SI units)
     double theta;         // opening parameter
     const long long* ord; // device bounding box (ordered-int min, max); radius = (max - min) / 2
+    double rel_alpha;     // interaction-list walk: relative opening rule with this alpha (0 = off), reading
+                          // the previous accelerations from the output arrays before overwriting them
 };
 
 // Plain FP64 walk with the reference's computeForces_v2 semantics.

@@ -6,10 +6,11 @@
 // follow calculateCentersOfMass (tree.cu:1416-1497): m = sum of child masses,
 // x = sum(x_c m_c) / m over the children in curve order, computed with
 // explicitly rounded FP64 multiplies and adds (the reference builds with
-// -fmad=false) so that Lebesgue-ordered results match it bit for bit.  The
-// reference runs one launch per level (21 launches, miluphpc.cpp:1205-1210);
-// here one launch climbs from every leaf and the last child to arrive at a
-// cell computes it.
+// -fmad=false) so that Lebesgue-ordered results match it bit for bit.  Like
+// the reference (21 launches, miluphpc.cpp:1205-1210) the pass runs one
+// launch per level, deepest first, each over a dense list of that level's
+// cells built once per tree from the sorted keys' common-digit counts; no
+// atomics or fences are involved.
 #include "tree.cuh"
 
 namespace {
@@ -112,7 +113,6 @@ __global__ void __launch_bounds__(256) k_nodes(TreeDev T, const uint64_t* __rest
             T.first[node] = a;
             T.last[node] = b;
             T.parent[node] = par;
-            T.arrive[node] = 0;
             if (par >= T.cap_nodes) set_status(st, MHPC_ERR_NODE_POOL, par);
             else if (par >= 0) { atomicAdd(&T.nchild[par], 1); add_kid(T, par, node, ka, L); }
             else atomicAdd(T.root_nchild, 1);
@@ -148,7 +148,6 @@ __global__ void k_zero_cells(TreeDev T) {
     if (total > T.cap_nodes) total = T.cap_nodes;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         T.nchild[i] = 0;
-        T.arrive[i] = 0;
         T.kmask[i] = 0;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *T.root_nchild = 0;
@@ -156,142 +155,210 @@ __global__ void k_zero_cells(TreeDev T) {
 
 __global__ void k_copy_total(TreeDev T) { *T.nodes = T.off[T.n]; }
 
-__device__ __forceinline__ double4 ldcg_d4(const double4* p) {
-    double4 v;
-    const double2* q = reinterpret_cast<const double2*>(p);
-    double2 a = __ldcg(q), b = __ldcg(q + 1);
-    v.x = a.x; v.y = a.y; v.z = b.x; v.w = b.y;
-    return v;
-}
-
 __device__ __forceinline__ float rd(double v) { return __double2float_rd(v); }
 __device__ __forceinline__ float ru(double v) { return __double2float_ru(v); }
 
-__global__ void __launch_bounds__(256) k_upward(TreeDev T, const double* __restrict__ sx,
-                                                const double* __restrict__ sy, const double* __restrict__ sz,
-                                                const double* __restrict__ sm, int want_quad,
-                                                const DevStatus* st) {
+// Cell lists per level.  The level-L cell starting at sorted position a
+// exists iff dl[a-1] < L <= dl[a] (its id is off[a] + L - dl[a-1] - 1);
+// k_level_count histograms them per block in shared memory, k_level_offsets
+// scans the 21 counts, k_level_fill reserves one range per (block, level) and
+// scatters the cell ids.  A block takes a fixed chunk of sorted positions, so
+// both passes see the same cells; the order inside a level is irrelevant.
+constexpr int kLevelChunk = 2048;
+
+__global__ void __launch_bounds__(256) k_level_count(TreeDev T, const DevStatus* st) {
     if (st->code) return;
-    const int n = T.n;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
-        const int leaf = T.leaf_node[a];
-        const double px = __ldg(sx + a), py = __ldg(sy + a), pz = __ldg(sz + a), pm = __ldg(sm + a);
-        T.com[leaf] = make_double4(px, py, pz, pm);
-        T.bmin[leaf] = make_float4(rd(px), rd(py), rd(pz), 0.f);
-        T.bmax[leaf] = make_float4(ru(px), ru(py), ru(pz), 0.f);
-        if (want_quad) {
-            T.quad0[leaf] = make_float4(0.f, 0.f, 0.f, 0.f);
-            T.quad1[leaf] = make_float2(0.f, 0.f);
-        }
-        int p = T.parent[leaf];
-        while (p >= 0) {
-            __threadfence();
-            const int old = atomicAdd(&T.arrive[p], 1);
-            if (old != T.nchild[p] - 1) break;
-            __threadfence();
-            const int mask = T.kmask[p];
-            int kid[8];
-            int nk = 0;
-            if (!(mask & 0x100)) {
-                const int4 k0 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)p));
-                const int4 k1 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)p) + 1);
-                const int all[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
-#pragma unroll
-                for (int d = 0; d < 8; ++d)
-                    if ((mask >> d) & 1) kid[nk++] = all[d];
-            }
-            double m = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
-            float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
-            float4 hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
-            auto add_com = [&](int c) {
-                const double4 cc = ldcg_d4(&T.com[c]);
-                mx = __dadd_rn(mx, __dmul_rn(cc.x, cc.w));
-                my = __dadd_rn(my, __dmul_rn(cc.y, cc.w));
-                mz = __dadd_rn(mz, __dmul_rn(cc.z, cc.w));
-                m = __dadd_rn(m, cc.w);
-                const float4 bl = __ldcg(&T.bmin[c]), bh = __ldcg(&T.bmax[c]);
-                lo.x = fminf(lo.x, bl.x); lo.y = fminf(lo.y, bl.y); lo.z = fminf(lo.z, bl.z);
-                hi.x = fmaxf(hi.x, bh.x); hi.y = fmaxf(hi.y, bh.y); hi.z = fmaxf(hi.z, bh.z);
-            };
-            const int end = T.link[p].x;
-            if (mask & 0x100) {
-                for (int c = p + 1; c < end; c = __ldcg(&T.link[c].x)) add_com(c);
-            } else {
-#pragma unroll
-                for (int q = 0; q < 8; ++q)
-                    if (q < nk) add_com(kid[q]);
-            }
-            if (m > 0.0) {
-                mx = __ddiv_rn(mx, m);
-                my = __ddiv_rn(my, m);
-                mz = __ddiv_rn(mz, m);
-            }
-            T.com[p] = make_double4(mx, my, mz, m);
-            T.bmin[p] = lo;
-            T.bmax[p] = hi;
-            if (want_quad) {
-                double q[6] = {0, 0, 0, 0, 0, 0};
-                auto add_quad = [&](int c) {
-                    const double4 cc = ldcg_d4(&T.com[c]);
-                    const double s0 = cc.x - mx, s1 = cc.y - my, s2 = cc.z - mz;
-                    const double ss = s0 * s0 + s1 * s1 + s2 * s2;
-                    const double w = cc.w;
-                    q[0] += w * (3.0 * s0 * s0 - ss);
-                    q[1] += w * 3.0 * s0 * s1;
-                    q[2] += w * 3.0 * s0 * s2;
-                    q[3] += w * (3.0 * s1 * s1 - ss);
-                    q[4] += w * 3.0 * s1 * s2;
-                    q[5] += w * (3.0 * s2 * s2 - ss);
-                    if (!(__ldcg(&T.link[c].y) & ND_LEAF)) {
-                        const float4 a0 = __ldcg(&T.quad0[c]);
-                        const float2 a1 = __ldcg(&T.quad1[c]);
-                        q[0] += a0.x; q[1] += a0.y; q[2] += a0.z; q[3] += a0.w; q[4] += a1.x; q[5] += a1.y;
-                    }
-                };
-                if (mask & 0x100) {
-                    for (int c = p + 1; c < end; c = __ldcg(&T.link[c].x)) add_quad(c);
-                } else {
-#pragma unroll
-                    for (int qq = 0; qq < 8; ++qq)
-                        if (qq < nk) add_quad(kid[qq]);
-                }
-                T.quad0[p] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
-                T.quad1[p] = make_float2((float)q[4], (float)q[5]);
-            }
-            p = T.parent[p];
+    __shared__ int h[32];
+    if (threadIdx.x < 32) h[threadIdx.x] = 0;
+    __syncthreads();
+    const int a0 = blockIdx.x * kLevelChunk;
+    const int a1 = min(a0 + kLevelChunk, T.n);
+    for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+        const int dp = dl_at(T.dl, a - 1), dc = T.dl[a];
+        for (int L = dp + 1; L <= dc; ++L) atomicAdd(&h[L], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x >= 1 && threadIdx.x <= MHPC_MAX_LEVEL && h[threadIdx.x])
+        atomicAdd(&T.level_off[32 + threadIdx.x], h[threadIdx.x]);
+}
+
+__global__ void k_level_offsets(TreeDev T) {
+    int acc = 0;
+    for (int L = 0; L <= MHPC_MAX_LEVEL + 1; ++L) {
+        const int c = (L >= 1 && L <= MHPC_MAX_LEVEL) ? T.level_off[32 + L] : 0;
+        T.level_off[L] = acc;
+        T.level_off[32 + L] = acc;  // fill cursor of level L
+        acc += c;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_level_fill(TreeDev T, const DevStatus* st) {
+    if (st->code) return;
+    __shared__ int h[32], base[32];
+    if (threadIdx.x < 32) h[threadIdx.x] = 0;
+    __syncthreads();
+    const int a0 = blockIdx.x * kLevelChunk;
+    const int a1 = min(a0 + kLevelChunk, T.n);
+    for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+        const int dp = dl_at(T.dl, a - 1), dc = T.dl[a];
+        for (int L = dp + 1; L <= dc; ++L) atomicAdd(&h[L], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const int L = threadIdx.x;
+        base[L] = (L >= 1 && L <= MHPC_MAX_LEVEL && h[L]) ? atomicAdd(&T.level_off[32 + L], h[L]) : 0;
+        h[L] = 0;
+    }
+    __syncthreads();
+    for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
+        const int dp = dl_at(T.dl, a - 1), dc = T.dl[a];
+        const int o = T.off[a];
+        for (int L = dp + 1; L <= dc; ++L) {
+            const int i = base[L] + atomicAdd(&h[L], 1);
+            if (i < T.cap_nodes) T.level_cells[i] = o + (L - dp - 1);
         }
     }
 }
 
-// Bottom-up maximum of the smoothing lengths, same last-arriver scheme as
-// k_upward (arrive[] cleared by the caller).
-__global__ void __launch_bounds__(256) k_node_hmax(TreeDev T, const double* __restrict__ h, const DevStatus* st) {
+// Children of cell p by key digit: slot d holds a child where bit d of the
+// mask is set, so visiting d = 0..7 gives the summation order of the
+// reference's calculateCentersOfMass (child slots 0..7); shared-key buckets
+// (mask bit 0x100) list theirs by skip pointers.
+struct Kids {
+    int id[8];
+    int mask;
+};
+
+__device__ __forceinline__ Kids cell_kids(const TreeDev& T, int p) {
+    Kids K;
+    K.mask = __ldg(T.kmask + p);
+    const int4 k0 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)p));
+    const int4 k1 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)p) + 1);
+    K.id[0] = k0.x; K.id[1] = k0.y; K.id[2] = k0.z; K.id[3] = k0.w;
+    K.id[4] = k1.x; K.id[5] = k1.y; K.id[6] = k1.z; K.id[7] = k1.w;
+    return K;
+}
+
+__global__ void __launch_bounds__(256) k_upward_leaves(TreeDev T, const double* __restrict__ sx,
+                                                       const double* __restrict__ sy, const double* __restrict__ sz,
+                                                       const double* __restrict__ sm, int want_quad,
+                                                       int want_box, const DevStatus* st) {
     if (st->code) return;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < T.n; a += gridDim.x * blockDim.x) {
         const int leaf = T.leaf_node[a];
-        T.hmax[leaf] = __double2float_ru(h[a]);
-        int p = T.parent[leaf];
-        while (p >= 0) {
-            __threadfence();
-            const int old = atomicAdd(&T.arrive[p], 1);
-            if (old != T.nchild[p] - 1) break;
-            __threadfence();
-            const int mask = T.kmask[p];
-            float m = 0.f;
-            if (mask & 0x100) {
-                const int end = T.link[p].x;
-                for (int c = p + 1; c < end; c = __ldcg(&T.link[c].x)) m = fmaxf(m, __ldcg(&T.hmax[c]));
+        const double px = __ldg(sx + a), py = __ldg(sy + a), pz = __ldg(sz + a), pm = __ldg(sm + a);
+        T.com[leaf] = make_double4(px, py, pz, pm);
+        if (want_box) {
+            T.bmin[leaf] = make_float4(rd(px), rd(py), rd(pz), 0.f);
+            T.bmax[leaf] = make_float4(ru(px), ru(py), ru(pz), 0.f);
+        }
+        if (want_quad) {
+            T.quad0[leaf] = make_float4(0.f, 0.f, 0.f, 0.f);
+            T.quad1[leaf] = make_float2(0.f, 0.f);
+        }
+    }
+}
+
+// One level of the upward pass: every cell of level L combines its children,
+// which the previous launches (deeper levels, leaves) completed.  Centres of
+// mass use explicitly rounded products and sums in slot order, so the result
+// is bit-identical to the level-wise sums of the reference.
+__global__ void __launch_bounds__(256) k_upward_level(TreeDev T, int L, int want_quad, int want_box,
+                                                      const DevStatus* st) {
+    if (st->code) return;
+    const int i0 = T.level_off[L], i1 = min(T.level_off[L + 1], T.cap_nodes);
+    for (int i = i0 + blockIdx.x * blockDim.x + threadIdx.x; i < i1; i += gridDim.x * blockDim.x) {
+        const int p = T.level_cells[i];
+        const Kids K = cell_kids(T, p);
+        double m = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+        float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+        float4 hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+        auto add_com = [&](int c) {
+            const double4 cc = ldg_d4(&T.com[c]);
+            mx = __dadd_rn(mx, __dmul_rn(cc.x, cc.w));
+            my = __dadd_rn(my, __dmul_rn(cc.y, cc.w));
+            mz = __dadd_rn(mz, __dmul_rn(cc.z, cc.w));
+            m = __dadd_rn(m, cc.w);
+            if (want_box) {
+                const float4 bl = __ldg(&T.bmin[c]), bh = __ldg(&T.bmax[c]);
+                lo.x = fminf(lo.x, bl.x); lo.y = fminf(lo.y, bl.y); lo.z = fminf(lo.z, bl.z);
+                hi.x = fmaxf(hi.x, bh.x); hi.y = fmaxf(hi.y, bh.y); hi.z = fmaxf(hi.z, bh.z);
+            }
+        };
+        const int end = __ldg(&T.link[p].x);
+        if (K.mask & 0x100) {
+            for (int c = p + 1; c < end; c = __ldg(&T.link[c].x)) add_com(c);
+        } else {
+#pragma unroll
+            for (int d = 0; d < 8; ++d)
+                if ((K.mask >> d) & 1) add_com(K.id[d]);
+        }
+        if (m > 0.0) {
+            mx = __ddiv_rn(mx, m);
+            my = __ddiv_rn(my, m);
+            mz = __ddiv_rn(mz, m);
+        }
+        T.com[p] = make_double4(mx, my, mz, m);
+        if (want_box) {
+            T.bmin[p] = lo;
+            T.bmax[p] = hi;
+        }
+        if (want_quad) {
+            double q[6] = {0, 0, 0, 0, 0, 0};
+            auto add_quad = [&](int c) {
+                const double4 cc = ldg_d4(&T.com[c]);
+                const double s0 = cc.x - mx, s1 = cc.y - my, s2 = cc.z - mz;
+                const double ss = s0 * s0 + s1 * s1 + s2 * s2;
+                const double w = cc.w;
+                q[0] += w * (3.0 * s0 * s0 - ss);
+                q[1] += w * 3.0 * s0 * s1;
+                q[2] += w * 3.0 * s0 * s2;
+                q[3] += w * (3.0 * s1 * s1 - ss);
+                q[4] += w * 3.0 * s1 * s2;
+                q[5] += w * (3.0 * s2 * s2 - ss);
+                if (!(__ldg(&T.link[c].y) & ND_LEAF)) {
+                    const float4 a0 = __ldg(&T.quad0[c]);
+                    const float2 a1 = __ldg(&T.quad1[c]);
+                    q[0] += a0.x; q[1] += a0.y; q[2] += a0.z; q[3] += a0.w; q[4] += a1.x; q[5] += a1.y;
+                }
+            };
+            if (K.mask & 0x100) {
+                for (int c = p + 1; c < end; c = __ldg(&T.link[c].x)) add_quad(c);
             } else {
-                const int4 k0 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)p));
-                const int4 k1 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)p) + 1);
-                const int all[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
 #pragma unroll
                 for (int d = 0; d < 8; ++d)
-                    if ((mask >> d) & 1) m = fmaxf(m, __ldcg(&T.hmax[all[d]]));
+                    if ((K.mask >> d) & 1) add_quad(K.id[d]);
             }
-            T.hmax[p] = m;
-            p = T.parent[p];
+            T.quad0[p] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+            T.quad1[p] = make_float2((float)q[4], (float)q[5]);
         }
+    }
+}
+
+// Bottom-up maximum of the smoothing lengths, level by level like the
+// centres of mass.
+__global__ void __launch_bounds__(256) k_hmax_leaves(TreeDev T, const double* __restrict__ h, const DevStatus* st) {
+    if (st->code) return;
+    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < T.n; a += gridDim.x * blockDim.x)
+        T.hmax[T.leaf_node[a]] = __double2float_ru(h[a]);
+}
+
+__global__ void __launch_bounds__(256) k_hmax_level(TreeDev T, int L, const DevStatus* st) {
+    if (st->code) return;
+    const int i0 = T.level_off[L], i1 = min(T.level_off[L + 1], T.cap_nodes);
+    for (int i = i0 + blockIdx.x * blockDim.x + threadIdx.x; i < i1; i += gridDim.x * blockDim.x) {
+        const int p = T.level_cells[i];
+        const Kids K = cell_kids(T, p);
+        float m = 0.f;
+        if (K.mask & 0x100) {
+            const int end = __ldg(&T.link[p].x);
+            for (int c = p + 1; c < end; c = __ldg(&T.link[c].x)) m = fmaxf(m, __ldg(&T.hmax[c]));
+        } else {
+#pragma unroll
+            for (int d = 0; d < 8; ++d)
+                if ((K.mask >> d) & 1) m = fmaxf(m, __ldg(&T.hmax[K.id[d]]));
+        }
+        T.hmax[p] = m;
     }
 }
 
@@ -313,12 +380,17 @@ __global__ void __launch_bounds__(256) k_mixed_nodes(TreeDev T, const long long*
         float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f);
         float2 q1 = make_float2(0.f, 0.f);
         int mask = 0;
-        if (!(info & ND_LEAF)) { q0 = T.quad0[i]; q1 = T.quad1[i]; mask = T.kmask[i]; }
+        float ml3 = 0.f;
+        if (!(info & ND_LEAF)) {
+            q0 = T.quad0[i]; q1 = T.quad1[i]; mask = T.kmask[i];
+            const double e = ldexp(edge0, -(info & 0xff));
+            ml3 = (float)(c.w * e * e * e);
+        }
         float4* w = T.wrec + 4 * (size_t)i;
         w[0] = make_float4(hx, hy, hz, (float)c.w);
         w[1] = make_float4((float)(c.x - (double)hx), (float)(c.y - (double)hy), (float)(c.z - (double)hz), crit);
         w[2] = q0;
-        w[3] = make_float4(q1.x, q1.y, __int_as_float(info), __int_as_float(mask));
+        w[3] = make_float4(q1.x, q1.y, __int_as_float((info & 0x1ff) | (mask << 9)), ml3);
     }
 }
 
@@ -336,20 +408,28 @@ int tree_build(TreeDev& T, const uint64_t* skey, void* scan_scratch, DevStatus* 
     k_copy_total<<<1, 1, 0, s>>>(T);
     k_zero_cells<<<148 * 8, 256, 0, s>>>(T);
     k_nodes<<<g, 256, 0, s>>>(T, skey, st);
+    CUDA_TRY(cudaMemsetAsync(T.level_off, 0, 64 * sizeof(int), s));
+    const int chunks = (n + kLevelChunk - 1) / kLevelChunk;
+    k_level_count<<<chunks, 256, 0, s>>>(T, st);
+    k_level_offsets<<<1, 1, 0, s>>>(T);
+    k_level_fill<<<chunks, 256, 0, s>>>(T, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }
 
 int tree_upward(TreeDev& T, const double* sx, const double* sy, const double* sz, const double* sm,
-                int want_quad, DevStatus* st, cudaStream_t s) {
-    k_upward<<<grid_for(T.n, 256, 148 * 16), 256, 0, s>>>(T, sx, sy, sz, sm, want_quad, st);
+                int want_quad, int want_box, DevStatus* st, cudaStream_t s) {
+    k_upward_leaves<<<grid_for(T.n, 256, 148 * 16), 256, 0, s>>>(T, sx, sy, sz, sm, want_quad, want_box, st);
+    const int gl = grid_for(T.n / 2 + 1, 256, 148 * 16);
+    for (int L = MHPC_MAX_LEVEL; L >= 1; --L) k_upward_level<<<gl, 256, 0, s>>>(T, L, want_quad, want_box, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }
 
 int tree_node_hmax(const TreeDev& T, const double* h, const DevStatus* st, cudaStream_t s) {
-    CUDA_TRY(cudaMemsetAsync(T.arrive, 0, sizeof(int) * (size_t)T.cap_nodes, s));
-    k_node_hmax<<<grid_for(T.n, 256, 148 * 16), 256, 0, s>>>(T, h, st);
+    k_hmax_leaves<<<grid_for(T.n, 256, 148 * 16), 256, 0, s>>>(T, h, st);
+    const int gl = grid_for(T.n / 2 + 1, 256, 148 * 16);
+    for (int L = MHPC_MAX_LEVEL; L >= 1; --L) k_hmax_level<<<gl, 256, 0, s>>>(T, L, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

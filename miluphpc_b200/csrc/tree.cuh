@@ -28,7 +28,6 @@ struct TreeDev {
     int* last;          // [cap] last sorted particle of the node
     int* parent;        // [cap] parent node, -1 for root children
     int* nchild;        // [cap] number of children
-    int* arrive;        // [cap] bottom-up arrival counters
     int* kids;          // [cap * 8] children by key digit (valid where kmask has the bit)
     int* kmask;         // [cap] bit d: slot d used; 0x100: children without a digit (shared keys)
     double4* com;       // [cap] centre of mass (x, y, z, m)
@@ -39,16 +38,22 @@ struct TreeDev {
     // [4 * cap] mixed-path walk record, one 64-byte line per node:
     //   [0] float(x), float(y), float(z), m   (FP32 hi part of the centre of mass)
     //   [1] x - float(x), ..., opening criterion edge^2/theta (-1 for leaves)
-    //   [2] Qxx Qxy Qxz Qyy   [3] Qyz Qzz, link info bits, kmask bits
+    //   [2] Qxx Qxy Qxz Qyy
+    //   [3] Qyz Qzz, bits (link info & 0x1ff) | kmask << 9, M l^3 (cells; l = edge)
     float4* wrec;
     float* hmax;        // [cap] largest smoothing length below the node (rounded up)
+    int* level_cells;   // [cap] cell ids grouped by level (any order within a level)
+    int* level_off;     // [64] level_off[L] = start of level L's cells (L = 1..21, [22] = end);
+                        // [32 + L] = fill cursors while the lists are built
     int* root_nchild;   // [1]
     int* nodes;         // [1] total nodes (= off[n]), device copy
 };
 
 int tree_build(TreeDev& T, const uint64_t* skey, void* scan_scratch, DevStatus* st, cudaStream_t s);
+// Centres of mass (FP64), quadrupoles (want_quad) and particle bounding boxes
+// (want_box, used by the neighbour search) of every cell, level by level.
 int tree_upward(TreeDev& T, const double* sx, const double* sy, const double* sz, const double* sm,
-                int want_quad, DevStatus* st, cudaStream_t s);
+                int want_quad, int want_box, DevStatus* st, cudaStream_t s);
 // T.hmax[node] = max h over the node's particles (h sorted, n entries).
 int tree_node_hmax(const TreeDev& T, const double* h, const DevStatus* st, cudaStream_t s);
 int tree_mixed_nodes(TreeDev& T, const long long* ord, double theta, const DevStatus* st, cudaStream_t s);

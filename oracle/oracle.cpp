@@ -514,11 +514,18 @@ void orc_gravity_group_crit(const double* x, const double* y, const double* z, c
 // distance |R|^2 + eps2 is used for the interaction, and eps2_i = eps2 +
 // (h_factor h_i)^2 per particle when h is given.  ninter receives the number
 // of accepted nodes, nquad the number of accepted cells (per particle).
-void orc_gravity_boxes(const double* x, const double* y, const double* z, const double* mass,
-                       const double* q, const int* child, const int* level, const int* sorted,
-                       int n, int gsize, int nsub, double radius, double theta, double eps2,
-                       const double* h, double h_factor, double* gax, double* gay, double* gaz,
-                       int* ninter, int* nquad) {
+// With amag != null the relative criterion is added (Springel 2005, the
+// GADGET-2 opening rule, for a group): a cell of mass M and edge l is
+// accepted only if, for every sub-box b with smallest previous |a| a_b,
+//   M l^lpow <= alpha a_b dist(com, box_b)^(lpow + 2),
+// i.e. the first neglected multipole term stays below alpha times the
+// particle's own acceleration; the geometric condition with theta stays as a
+// safety bound.  amag is indexed like x (original order).
+static void gravity_boxes_impl(const double* x, const double* y, const double* z, const double* mass,
+                               const double* q, const int* child, const int* level, const int* sorted,
+                               int n, int gsize, int nsub, double radius, double theta, double eps2,
+                               const double* h, double h_factor, const double* amag, double alpha, int lpow,
+                               double* gax, double* gay, double* gaz, int* ninter, int* nquad) {
     const int ngroups = (n + gsize - 1) / gsize;
     const int w = gsize / nsub;
 #pragma omp parallel for schedule(dynamic, 4)
@@ -527,10 +534,11 @@ void orc_gravity_boxes(const double* x, const double* y, const double* z, const 
         const int lanes = std::min(gsize, n - base);
         // sub-box b covers group members [b*w, (b+1)*w); members past n
         // repeat the last particle (as the device kernel loads them)
-        std::vector<double> lo(3 * nsub, 1e300), hi(3 * nsub, -1e300);
+        std::vector<double> lo(3 * nsub, 1e300), hi(3 * nsub, -1e300), amin(nsub, 1e300);
         for (int j = 0; j < gsize; ++j) {
             const int s = sorted[std::min(base + j, n - 1)];
             const int b = j / w;
+            if (amag) amin[b] = std::min(amin[b], amag[s]);
             const double p[3] = {x[s], y[s], z[s]};
             for (int d = 0; d < 3; ++d) {
                 lo[3 * b + d] = std::min(lo[3 * b + d], p[d]);
@@ -555,6 +563,11 @@ void orc_gravity_boxes(const double* x, const double* y, const double* z, const 
                     d2 += e * e;
                 }
                 ok = cr <= d2;
+                if (ok && amag) {
+                    const double lp = lpow == 3 ? edge * edge * edge : edge * edge;
+                    const double dp = lpow == 3 ? d2 * d2 * std::sqrt(d2) : d2 * d2;
+                    ok = mass[nd] * lp <= alpha * amin[b] * dp;
+                }
             }
             if (ok) { acc_nodes.push_back(nd); ++ncell; continue; }
             for (int i = 0; i < 8; ++i) if (child[8 * nd + i] != -1) stack.push_back(child[8 * nd + i]);
@@ -588,6 +601,24 @@ void orc_gravity_boxes(const double* x, const double* y, const double* z, const 
             if (nquad) nquad[s] = ncell;
         }
     }
+}
+
+void orc_gravity_boxes(const double* x, const double* y, const double* z, const double* mass,
+                       const double* q, const int* child, const int* level, const int* sorted,
+                       int n, int gsize, int nsub, double radius, double theta, double eps2,
+                       const double* h, double h_factor, double* gax, double* gay, double* gaz,
+                       int* ninter, int* nquad) {
+    gravity_boxes_impl(x, y, z, mass, q, child, level, sorted, n, gsize, nsub, radius, theta, eps2, h, h_factor,
+                       nullptr, 0.0, 2, gax, gay, gaz, ninter, nquad);
+}
+
+void orc_gravity_boxes_rel(const double* x, const double* y, const double* z, const double* mass,
+                           const double* q, const int* child, const int* level, const int* sorted,
+                           int n, int gsize, int nsub, double radius, double theta, double eps2,
+                           const double* h, double h_factor, const double* amag, double alpha, int lpow,
+                           double* gax, double* gay, double* gaz, int* ninter, int* nquad) {
+    gravity_boxes_impl(x, y, z, mass, q, child, level, sorted, n, gsize, nsub, radius, theta, eps2, h, h_factor,
+                       amag, alpha, lpow, gax, gay, gaz, ninter, nquad);
 }
 
 // ----------------------------------------------------------------- SPH ----

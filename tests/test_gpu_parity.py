@@ -237,6 +237,38 @@ def test_gravity_mixed_accuracy(precision, theta, cuda):
     sim.close()
 
 
+def test_gravity_relative_mac(cuda):
+    """Relative opening rule of the interaction-list walk: the first call has
+    no previous accelerations and uses the geometric rule; the second reads
+    them from g_ax/g_ay/g_az and needs far fewer interactions at p99 <= 1e-3,
+    close to the FP64 statement of the same rule fed the same |a|."""
+    n = 131_072
+    P = ics.plummer(n, seed=1)
+    cfg = gravity_cfg(sfc=1, precision=1, theta_mixed=0.28, smoothing=1e-4, gravity_mac=1, mac_alpha=3e-3)
+    sim = Miluphpc(cfg, P)
+    sim.rhs(0)
+    g0 = np.stack([sim.numpy("g_ax"), sim.numpy("g_ay"), sim.numpy("g_az")])
+    i0 = sim.stats()["gravity_interactions"]
+    sim.rhs(1)
+    g1 = np.stack([sim.numpy("g_ax"), sim.numpy("g_ay"), sim.numpy("g_az")])
+    i1 = sim.stats()["gravity_interactions"]
+    assert i1 < 0.7 * i0, (i0, i1)
+    tg = np.random.default_rng(7).choice(n, 4096, replace=False)
+    dx, dy, dz, _ = O.direct(P["x"], P["y"], P["z"], P["mass"], tg, 1e-4)
+    e = rel_err(g1[0][tg], g1[1][tg], g1[2][tg], dx, dy, dz)
+    assert np.percentile(e, 99) <= 1e-3, np.percentile(e, 99)
+    bb = O.bbox(P["x"], P["y"], P["z"])
+    T = O.Tree(P["x"], P["y"], P["z"], P["mass"], bb)
+    q = O.quad(T)
+    _, operm = O.sort(O.keys(P["x"], P["y"], P["z"], bb, 1))
+    amag = np.sqrt((g0 ** 2).sum(0))
+    ax, ay, az, cnt, nq = O.gravity_boxes_rel(T, operm, 0.5 * (bb[1] - bb[0]), 1.0, 1e-4, q, amag, 3e-3, 3)
+    e2 = rel_err(g1[0], g1[1], g1[2], ax, ay, az)
+    assert np.percentile(e2, 99) < 2e-4, np.percentile(e2, 99)
+    assert abs(i1 / cnt.sum() - 1.0) < 3e-3, (i1, cnt.sum())
+    sim.close()
+
+
 @pytest.mark.parametrize("precision", [1, 2])
 def test_gravity_mixed_small_and_coincident(precision, cuda):
     """Ragged last group (n not a multiple of 64), tiny n, and particles
