@@ -414,13 +414,17 @@ def run_e2e(args, wl, sim, state, torch, step0):
 
 
 def load_traffic(workload, variant):
-    """DRAM bytes per launch of the walk from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    try:
-        d = json.load(open(p))
-        return d.get("%s/%s" % (workload, variant))
-    except Exception:
-        return None
+    """DRAM bytes (read + write) per launch of the dominant kernel, from the
+    `traffic <workload>/<variant> <bytes>` lines of the committed ncu
+    summaries under profiles/ (None when no capture covers the workload)."""
+    import glob
+    key = "%s/%s" % (workload, variant)
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        for line in open(path):
+            f = line.split()
+            if len(f) == 3 and f[0] == "traffic" and f[1] == key:
+                return float(f[2])
+    return None
 
 
 def cpu_baseline(wl, args, sample_groups=None):
