@@ -90,6 +90,8 @@ typedef struct mhpc_config {
                                   the previous right-hand side, found in g_ax/g_ay/g_az when the walk
                                   starts); the first gravity call on a context uses the geometric rule */
     double mac_alpha;          /* accuracy parameter of the relative rule (0.003: p99 force error ~8e-4) */
+    int balsara;               /* BALSARA_SWITCH: viscous mu_ij scaled by (f_i + f_j)/2,
+                                  f = |div v| / (|div v| + |curl v| + 1e-4 c_s / h) */
 } mhpc_config;
 
 /* Material (include/materials/material.cuh:123-150), one entry of the
@@ -252,6 +254,20 @@ int mhpc_get_stats(mhpc_ctx* ctx, mhpc_stats* out);
  * out[1] internal energy sum m e, out[2..4] linear momentum, out[5..7]
  * angular momentum, out[8..10] centre of mass.  Synchronises. */
 int mhpc_diagnostics(mhpc_ctx* ctx, const mhpc_particles* p, double* out11);
+
+/* Miluphpc::removeParticles (src/miluphpc.cpp:3216-3348) with
+ * ParticlesNS::Kernel::mark2remove (src/subdomain_key_tree/subdomain.cu:2161-2240):
+ * removes the particles outside the region of config remove_particles_criterion
+ * (0: sqrt(x^2+y^2+z^2) < d kept, 1: |x|, |y|, |z| < d kept; d =
+ * remove_particles_dimension) from every non-null array of *p (all FP64 fields,
+ * noi and material_id; nnl and level are per-RHS outputs and are left alone),
+ * keeping the order of the survivors and zeroing the vacated tail; p->n is
+ * lowered accordingly.  The reference's integrators call it at the start of
+ * each step when removeParticles is set; so should the caller of
+ * mhpc_integrate.  Unlike the reference, the gravitational and leapfrog-old
+ * accelerations and the rates are compacted too, so they stay with their
+ * particles.  Synchronises the context's stream once. */
+int mhpc_remove_particles(mhpc_ctx* ctx, mhpc_particles* p, int* n_removed);
 
 /* FP64 direct summation for verification: accelerations of `nt` target
  * particles (original indices, device) from all n particles with softening

@@ -41,7 +41,7 @@ class Config(ctypes.Structure):
         ("nb_tolerance", c_int), ("max_sml_iterations", c_int),
         ("precision", c_int), ("theta_mixed", c_double), ("learned_h", c_int), ("softening_mode", c_int),
         ("softening_h_factor", c_double), ("node_pool_factor", c_double),
-        ("gravity_mac", c_int), ("mac_alpha", c_double),
+        ("gravity_mac", c_int), ("mac_alpha", c_double), ("balsara", c_int),
     ]
 
 
@@ -122,6 +122,7 @@ def load():
     L.mhpc_export_tree.argtypes = [c_void_p, c_int, P_i, P_i, P_d, P_d, P_d, P_d, P_i]
     L.mhpc_get_stats.argtypes = [c_void_p, ctypes.POINTER(Stats)]
     L.mhpc_diagnostics.argtypes = [c_void_p, ctypes.POINTER(Particles), P_d]
+    L.mhpc_remove_particles.argtypes = [c_void_p, ctypes.POINTER(Particles), P_i]
     L.mhpc_direct_gravity.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_double,
                                       c_void_p, c_void_p, c_void_p, c_void_p]
     L.mhpc_fp32_peak.argtypes = [P_d]
@@ -160,4 +161,5 @@ EXPORTS = [
     "mhpc_stage_gravity", "mhpc_stage_sph", "mhpc_export_sorted", "mhpc_export_tree", "mhpc_get_stats",
     "mhpc_diagnostics", "mhpc_direct_gravity", "mhpc_fp32_peak", "mhpc_mlp_reset", "mhpc_mlp_train", "mhpc_mlp_num_params",
     "mhpc_mlp_forward_backward", "mhpc_mlp_get_params", "mhpc_mlp_set_params",
+    "mhpc_remove_particles",
 ]

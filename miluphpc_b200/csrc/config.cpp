@@ -194,6 +194,7 @@ void mhpc_config_default(mhpc_config* c) {
     c->node_pool_factor = 1.0;
     c->gravity_mac = 0;
     c->mac_alpha = 0.003;
+    c->balsara = 0;
 }
 
 int mhpc_config_from_info(const char* path, mhpc_config* c) {
@@ -238,6 +239,7 @@ int mhpc_config_from_info(const char* path, mhpc_config* c) {
     f("softeningHFactor", &c->softening_h_factor);
     i("gravityMac", &c->gravity_mac);
     f("macAlpha", &c->mac_alpha);
+    b("balsaraSwitch", &c->balsara);
     if (c->gravity_mac < 0 || c->gravity_mac > 1 || (c->gravity_mac == 1 && c->mac_alpha <= 0))
         return MHPC_ERR_CONFIG;
     if (c->integrator < 0 || c->integrator > 2 || c->sfc < 0 || c->sfc > 1 || c->theta <= 0 ||

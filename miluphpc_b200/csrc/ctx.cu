@@ -40,7 +40,7 @@ struct mhpc_ctx {
     void* scan_scratch = nullptr;
     double *sx = nullptr, *sy = nullptr, *sz = nullptr, *sm = nullptr, *sh = nullptr;
     double *svx = nullptr, *svy = nullptr, *svz = nullptr, *se = nullptr, *srho = nullptr, *sp = nullptr,
-           *scs = nullptr;
+           *scs = nullptr, *sbal = nullptr;
     int* smat = nullptr;
     TreeDev T;
     int* nbr = nullptr;
@@ -120,6 +120,8 @@ SphParams sph_params(const mhpc_ctx* c, int n) {
     P.integrate_density = c->cfg.integrate_density;
     P.num_materials = c->nmat;
     P.mixed = c->cfg.precision >= 1;
+    P.balsara = c->cfg.balsara ? 1 : 0;
+    P.variable_sml = c->cfg.variable_sml ? 1 : 0;
     for (int i = 0; i < c->nmat && i < MHPC_MAX_MATERIALS; ++i) P.mat[i] = to_dev(c->mats[i], c->cfg.si_units);
     return P;
 }
@@ -237,10 +239,11 @@ int stage_sph(mhpc_ctx* c, const mhpc_particles* p) {
     S.x = c->sx; S.y = c->sy; S.z = c->sz; S.m = c->sm; S.h = c->sh;
     S.vx = c->svx; S.vy = c->svy; S.vz = c->svz; S.e = c->se;
     S.mat = p->material_id ? c->smat : nullptr;
-    S.rho = c->srho; S.p = c->sp; S.cs = c->scs;
+    S.rho = c->srho; S.p = c->sp; S.cs = c->scs; S.bal = c->sbal;
     TRY(sph_frnn(c->T, P, S, c->nbr, c->noi, c->st, s));
     record(c, EV_FRNN);
     TRY(sph_density_eos(P, S, c->nbr, c->noi, c->perm, p->rho, p->p, p->cs, c->st, s));
+    if (c->cfg.balsara) TRY(sph_balsara(P, S, c->nbr, c->noi, c->st, s));
     record(c, EV_DENS);
     TRY(sph_forces(P, S, c->nbr, c->noi, c->perm, p->ax, p->ay, p->az, p->drhodt, p->dedt, p->dsmldt, c->st, s));
     if (p->nnl || p->noi) TRY(sph_export_nnl(P, c->nbr, c->noi, c->perm, p->nnl, p->noi, s));
@@ -395,6 +398,7 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
     }
     if (cfg->sph) {
         A(c->svx, n); A(c->svy, n); A(c->svz, n); A(c->se, n); A(c->srho, n); A(c->sp, n); A(c->scs, n);
+        A(c->sbal, n);
         A(c->smat, n);
         size_t groups = (n + 31) / 32;
         A(c->nbr, groups * 32 * (size_t)c->maxnb);
@@ -737,6 +741,49 @@ int mhpc_get_stats(mhpc_ctx* c, mhpc_stats* o) {
         cudaEventElapsedTime(&o->ms_stage[6], c->ev[EV_GRAV], c->ev[EV_SML]);
     }
     return code;
+}
+
+int mhpc_remove_particles(mhpc_ctx* c, mhpc_particles* p, int* n_removed) {
+    if (!c || !p) return MHPC_ERR_ARG;
+    TRY(check_particles(c, p));
+    if (n_removed) *n_removed = 0;
+    const int n = p->n;
+    if (n == 0) return MHPC_OK;
+    const int crit = c->cfg.remove_particles_criterion;
+    if (crit != 0 && crit != 1) return MHPC_ERR_CONFIG;
+    cudaStream_t s = c->stream;
+    // the tree's per-position scratch (free between right-hand sides) holds
+    // the flags and their exclusive scan; the sorted-copy buffers hold the
+    // compacted arrays before they are copied back
+    int* keep = c->T.cnt;
+    int* rank = c->T.off;
+    TRY(launch_remove_mark(n, p->x, p->y, p->z, crit, c->cfg.remove_particles_dimension, keep, s));
+    TRY(scan_exclusive_i32(keep, rank, n, c->scan_scratch, s));
+    int kept = 0;
+    CUDA_TRY(cudaMemcpyAsync(&kept, rank + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (kept == n) return MHPC_OK;
+    double* dfields[] = {p->x, p->y, p->z, p->mass, p->vx, p->vy, p->vz, p->ax, p->ay, p->az,
+                         p->g_ax, p->g_ay, p->g_az, p->g_ax_old, p->g_ay_old, p->g_az_old,
+                         p->sml, p->rho, p->p, p->cs, p->e, p->drhodt, p->dedt, p->dsmldt};
+    for (double* f : dfields) {
+        if (!f) continue;
+        TRY(launch_compact_d(n, keep, rank, f, c->sx, s));
+        CUDA_TRY(cudaMemcpyAsync(f, c->sx, sizeof(double) * (size_t)kept, cudaMemcpyDeviceToDevice, s));
+        CUDA_TRY(cudaMemsetAsync(f + kept, 0, sizeof(double) * (size_t)(n - kept), s));
+    }
+    int* ifields[] = {p->noi, p->material_id};
+    for (int* f : ifields) {
+        if (!f) continue;
+        TRY(launch_compact_i(n, keep, rank, f, c->T.leaf_node, s));
+        CUDA_TRY(cudaMemcpyAsync(f, c->T.leaf_node, sizeof(int) * (size_t)kept, cudaMemcpyDeviceToDevice, s));
+        CUDA_TRY(cudaMemsetAsync(f + kept, 0, sizeof(int) * (size_t)(n - kept), s));
+    }
+    CUDA_TRY(cudaStreamSynchronize(s));
+    p->n = kept;
+    c->grav_prev_n = -1;  // the previous accelerations no longer match the particle count
+    if (n_removed) *n_removed = n - kept;
+    return MHPC_OK;
 }
 
 int mhpc_diagnostics(mhpc_ctx* c, const mhpc_particles* p, double* out) {

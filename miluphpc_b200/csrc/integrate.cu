@@ -308,6 +308,36 @@ __global__ void __launch_bounds__(256) k_fma_peak(float* out, float b, float c) 
     if (s == 1234.5f) out[blockIdx.x] = s;
 }
 
+// ------------------------------------------------------ particle removal
+// ParticlesNS::Kernel::mark2remove with applySphericalCriterion /
+// applyCubicCriterion (src/subdomain_key_tree/subdomain.cu:2161-2240): a
+// particle is kept when sqrt(x^2 + y^2 + z^2) < d (criterion 0) or when
+// |x|, |y|, |z| < d (criterion 1); products and sums explicitly rounded like
+// the reference's -fmad=false build.
+__global__ void __launch_bounds__(256) k_remove_mark(int n, const double* __restrict__ x,
+                                                     const double* __restrict__ y, const double* __restrict__ z,
+                                                     int criterion, double d, int* keep) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double xi = x[i], yi = y[i], zi = z[i];
+        bool k;
+        if (criterion == 0)
+            k = sqrt(__dadd_rn(__dadd_rn(__dmul_rn(xi, xi), __dmul_rn(yi, yi)), __dmul_rn(zi, zi))) < d;
+        else
+            k = fabs(xi) < d && fabs(yi) < d && fabs(zi) < d;
+        keep[i] = k ? 1 : 0;
+    }
+}
+
+// Stable compaction of one array: kept entries move to their rank among the
+// kept ones (the reference's stable sort by the removal flag).
+template <typename T>
+__global__ void __launch_bounds__(256) k_compact_field(int n, const int* __restrict__ keep,
+                                                       const int* __restrict__ rank, const T* __restrict__ src,
+                                                       T* __restrict__ dst) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        if (keep[i]) dst[rank[i]] = src[i];
+}
+
 }  // namespace
 
 extern "C" int mhpc_fp32_peak(double* tflops) {
@@ -418,6 +448,25 @@ int launch_direct(const double* x, const double* y, const double* z, const doubl
     if (by > maxby) by = (int)maxby;
     dim3 grid(bx, by);
     k_direct<<<grid, 256, 0, s>>>(x, y, z, m, n, tg, nt, eps2, gax, gay, gaz);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int launch_remove_mark(int n, const double* x, const double* y, const double* z, int criterion, double d, int* keep,
+                       cudaStream_t s) {
+    k_remove_mark<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(n, x, y, z, criterion, d, keep);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int launch_compact_d(int n, const int* keep, const int* rank, const double* src, double* dst, cudaStream_t s) {
+    k_compact_field<double><<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(n, keep, rank, src, dst);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int launch_compact_i(int n, const int* keep, const int* rank, const int* src, int* dst, cudaStream_t s) {
+    k_compact_field<int><<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(n, keep, rank, src, dst);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

@@ -25,6 +25,12 @@ int launch_pc_corrector(const mhpc_particles& p, const mhpc_particles& q, const 
 // part needs 148 * 2 * 6 doubles
 int launch_set_time_step(const mhpc_particles& p, int gravity, int sph, double alpha, double beta, int int_rho,
                          double time_left, double dt_max, double* part, double* dt_out, cudaStream_t s);
+// Particle removal: keep[i] = 1 for particles inside the criterion's region;
+// stable compaction of one array by the exclusive scan (rank) of keep.
+int launch_remove_mark(int n, const double* x, const double* y, const double* z, int criterion, double d, int* keep,
+                       cudaStream_t s);
+int launch_compact_d(int n, const int* keep, const int* rank, const double* src, double* dst, cudaStream_t s);
+int launch_compact_i(int n, const int* keep, const int* rank, const int* src, int* dst, cudaStream_t s);
 int launch_diagnostics(const mhpc_particles& p, int sph, double* part, double* out, cudaStream_t s);
 size_t diagnostics_scratch_doubles();
 int launch_direct(const double* x, const double* y, const double* z, const double* m, int n, const int* tg, int nt,

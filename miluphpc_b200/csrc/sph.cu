@@ -340,6 +340,43 @@ __global__ void __launch_bounds__(kBlock) k_density_eos(SphParams P, SphSorted S
     cs_out[o] = cs;
 }
 
+// ------------------------------------------------------------- Balsara
+// SPH::Kernel::CalcDivvandCurlv (src/sph/kernel.cu:223-342) and the factor of
+// internalForces (src/sph/internal_forces.cu:210-217):
+//   div v_i = sum_j m_j / rho_j (v_j - v_i) . grad W,
+//   curl v_i = sum_j m_j / rho_i (v_i - v_j) x grad W,
+//   f_i = |div v_i| / (|div v_i| + |curl v_i| + 1e-4 c_s,i / h_i),
+// grad W at h_i (h_bar only under VARIABLE_SML, as in the reference).
+__global__ void __launch_bounds__(kBlock) k_balsara(SphParams P, SphSorted S, const int* __restrict__ nbr,
+                                                    const int* __restrict__ noi, DevStatus* st) {
+    if (st->code) return;
+    const long s = (long)blockIdx.x * kBlock + threadIdx.x;
+    if (s >= P.n) return;
+    const double xi = S.x[s], yi = S.y[s], zi = S.z[s], hi = S.h[s];
+    const double vxi = S.vx[s], vyi = S.vy[s], vzi = S.vz[s], rhoi = S.rho[s];
+    double divv = 0.0, c0 = 0.0, c1 = 0.0, c2 = 0.0;
+    const int k = min(noi[s], P.maxnb);
+    for (int q = 0; q < k; ++q) {
+        const int j = nbr[nb_index(s, q, P.maxnb)];
+        const double hb = P.variable_sml ? 0.5 * (hi + __ldg(S.h + j)) : hi;
+        const double dx = xi - __ldg(S.x + j), dy = yi - __ldg(S.y + j), dz = zi - __ldg(S.z + j);
+        const double r = sqrt(dx * dx + dy * dy + dz * dz);
+        double W, dWdr;
+        skernel(P.kernel, r, hb, W, dWdr);
+        const double g = dWdr / r;
+        const double gx = g * dx, gy = g * dy, gz = g * dz;
+        const double dvx = vxi - __ldg(S.vx + j), dvy = vyi - __ldg(S.vy + j), dvz = vzi - __ldg(S.vz + j);
+        const double mj = __ldg(S.m + j);
+        divv += mj / __ldg(S.rho + j) * (-dvx * gx - dvy * gy - dvz * gz);
+        const double w = mj / rhoi;
+        c0 += w * (dvy * gz - dvz * gy);
+        c1 += w * (dvz * gx - dvx * gz);
+        c2 += w * (dvx * gy - dvy * gx);
+    }
+    const double curl = sqrt(c0 * c0 + c1 * c1 + c2 * c2);
+    S.bal[s] = fabs(divv) / (fabs(divv) + curl + 1e-4 * S.cs[s] / hi);
+}
+
 // ------------------------------------------------------------- forces
 // SPH::Kernel::internalForces, hydro part, SPH_EQU_VERSION 1
 // (src/sph/internal_forces.cu:372-552).
@@ -377,8 +414,9 @@ __global__ void __launch_bounds__(kBlock) k_forces(SphParams P, SphSorted S, con
         if (vr < 0) {
             const double csbar = 0.5 * (csi + __ldg(S.cs + j));
             const double smooth = 0.5 * (hi + hj);
-            const double mu = smooth * vr / (rr + smooth * smooth * 1e-2);
+            double mu = smooth * vr / (rr + smooth * smooth * 1e-2);
             const double rhobar = 0.5 * (rhoi + rhoj);
+            if (P.balsara) mu *= (S.bal[s] + __ldg(S.bal + j)) / 2.;
             pij = (beta * mu - alpha * csbar) * mu / rhobar;
         }
         const double pf = -mj * (pri + __ldg(S.p + j) / (rhoj * rhoj));
@@ -473,6 +511,14 @@ int sph_density_eos(const SphParams& P, const SphSorted& S, const int* nbr, cons
                     double* rho_out, double* p_out, double* cs_out, DevStatus* st, cudaStream_t s) {
     if (P.n <= 0) return MHPC_OK;
     k_density_eos<<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(P, S, nbr, noi, perm, rho_out, p_out, cs_out, st);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int sph_balsara(const SphParams& P, const SphSorted& S, const int* nbr, const int* noi, DevStatus* st,
+                cudaStream_t s) {
+    if (P.n <= 0) return MHPC_OK;
+    k_balsara<<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(P, S, nbr, noi, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

@@ -21,6 +21,8 @@ struct SphParams {
     int integrate_density; // density from state (no kernel sum)
     int num_materials;
     int mixed;             // FP32 pair sums on group-relative coordinates
+    int balsara;           // Balsara switch on the viscosity (S.bal holds the factors)
+    int variable_sml;      // the Balsara gradients use h_bar only under VARIABLE_SML
     MatDev mat[MHPC_MAX_MATERIALS];
 };
 
@@ -30,6 +32,7 @@ struct SphSorted {
     const double *vx, *vy, *vz, *e;
     const int* mat;        // may be null
     double *rho, *p, *cs;  // sorted outputs of the density/EOS pass (p, cs hold previous values on entry)
+    double* bal;           // sorted Balsara factors (written by sph_balsara, read by sph_forces)
 };
 
 // Neighbour lists in sorted index space, group-transposed:
@@ -55,6 +58,11 @@ int sph_variable_h(const TreeDev& T, const SphParams& P, const double* x, const 
                    cudaStream_t s);
 int sph_density_eos(const SphParams& P, const SphSorted& S, const int* nbr, const int* noi, const int* perm,
                     double* rho_out, double* p_out, double* cs_out, DevStatus* st, cudaStream_t s);
+// Balsara switch (SPH::Kernel::CalcDivvandCurlv, src/sph/kernel.cu:223-342, and
+// the factor of internalForces, src/sph/internal_forces.cu:210-217): div v and
+// curl v from the neighbour lists, f_i into S.bal; after sph_density_eos.
+int sph_balsara(const SphParams& P, const SphSorted& S, const int* nbr, const int* noi, DevStatus* st,
+                cudaStream_t s);
 int sph_forces(const SphParams& P, const SphSorted& S, const int* nbr, const int* noi, const int* perm,
                double* ax, double* ay, double* az, double* drhodt, double* dedt, double* dsmldt, DevStatus* st,
                cudaStream_t s);

@@ -114,7 +114,18 @@ class Miluphpc:
     def status(self):
         return self.L.mhpc_ctx_status(self.ctx)
 
+    def remove_particles(self):
+        """Miluphpc::removeParticles: drop the particles outside the configured
+        region (compacting every array, lowering n); returns how many left."""
+        k = ctypes.c_int(0)
+        check(self.L.mhpc_remove_particles(self.ctx, ctypes.byref(self._soa), ctypes.byref(k)), "remove_particles")
+        self.n = self._soa.n
+        return k.value
+
     def integrate(self, step):
+        # the reference's integrators remove particles at the start of a step
+        if self.cfg.remove_particles:
+            self.remove_particles()
         dt = ctypes.c_double(0)
         check(self.L.mhpc_integrate(self.ctx, ctypes.byref(self._soa), int(step), ctypes.byref(dt)), "integrate")
         return dt.value

@@ -761,12 +761,48 @@ void orc_eos(int n, int eos, const double* par, const double* rho, const double*
 // -m_j (p_i/rho_i^2 + p_j/rho_j^2) gradW, Pi_ij = (beta mu - alpha cbar) mu /
 // rhobar for v.r < 0 with mu = hbar v.r/(r^2 + 0.01 hbar^2); drho/dt, de/dt
 // (integrate_energy), dh/dt (integrate_sml).
+// Balsara switch, SPH::Kernel::CalcDivvandCurlv (kernel.cu:223-342) and the
+// factor of internalForces (internal_forces.cu:210-217):
+//   div v_i  = sum_j m_j / rho_j (v_j - v_i) . grad W_ij
+//   curl v_i = sum_j m_j / rho_i (v_i - v_j) x grad W_ij
+//   f_i = |div v_i| / (|div v_i| + |curl v_i| + 1e-4 c_s,i / h_i)
+// with grad W at h_i, or at (h_i + h_j)/2 under VARIABLE_SML (avg_h; the
+// reference does not average here for INTEGRATE_SML alone).  divv, curlv
+// (3 per particle) and f may be null.
+void orc_balsara(const double* x, const double* y, const double* z, const double* vx, const double* vy,
+                 const double* vz, const double* mass, const double* h, const double* rho, const double* cs,
+                 int n, const long* off, const int* nbr, int avg_h, double* divv_out, double* curlv_out,
+                 double* f) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        double divv = 0, curl[3] = {0, 0, 0};
+        for (long k = off[i]; k < off[i + 1]; ++k) {
+            const int j = nbr[k];
+            const double sml = avg_h ? 0.5 * (h[i] + h[j]) : h[i];
+            const double dr[3] = {x[i] - x[j], y[i] - y[j], z[i] - z[j]};
+            double W, dW[3], dWdr;
+            cubic(&W, dW, &dWdr, dr, sml);
+            const double vi[3] = {vx[i], vy[i], vz[i]}, vj[3] = {vx[j], vy[j], vz[j]};
+            for (int d = 0; d < 3; ++d) divv += mass[j] / rho[j] * (vj[d] - vi[d]) * dW[d];
+            curl[0] += mass[j] / rho[i] * ((vi[1] - vj[1]) * dW[2] - (vi[2] - vj[2]) * dW[1]);
+            curl[1] += mass[j] / rho[i] * ((vi[2] - vj[2]) * dW[0] - (vi[0] - vj[0]) * dW[2]);
+            curl[2] += mass[j] / rho[i] * ((vi[0] - vj[0]) * dW[1] - (vi[1] - vj[1]) * dW[0]);
+        }
+        if (divv_out) divv_out[i] = divv;
+        if (curlv_out) for (int d = 0; d < 3; ++d) curlv_out[3 * (size_t)i + d] = curl[d];
+        const double c = std::sqrt(curl[0] * curl[0] + curl[1] * curl[1] + curl[2] * curl[2]);
+        if (f) f[i] = std::fabs(divv) / (std::fabs(divv) + c + 1e-4 * cs[i] / h[i]);
+    }
+}
+
+// bal (may be null): Balsara factors f; the viscous mu_ij is scaled by
+// (f_i + f_j)/2 (internal_forces.cu:387-395).
 void orc_forces(const double* x, const double* y, const double* z, const double* vx,
                 const double* vy, const double* vz, const double* mass, const double* h,
                 const double* rho, const double* p, const double* cs, int n, const long* off,
                 const int* nbr, double alpha, double beta, int avg_h, int integrate_energy,
                 int integrate_sml, double* ax, double* ay, double* az, double* drhodt,
-                double* dedt, double* dsmldt) {
+                double* dedt, double* dsmldt, const double* bal) {
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i) {
         double acc[3] = {0, 0, 0}, drho = 0, de = 0, dh = 0;
@@ -786,6 +822,7 @@ void orc_forces(const double* x, const double* y, const double* z, const double*
                 double smooth = 0.5 * (h[i] + h[j]);
                 double mu = smooth * vr / (rr + smooth * smooth * 1e-2);
                 double rhobar = 0.5 * (rho[i] + rho[j]);
+                if (bal) mu *= (bal[i] + bal[j]) / 2.;
                 pij = (beta * mu - alpha * csbar) * mu / rhobar;
             }
             double accj[3];

@@ -60,7 +60,8 @@ def lib():
         L.orc_density.argtypes = [_d, _d, _d, _d, _d, ctypes.c_int, _l, _i, ctypes.c_int, _d]
         L.orc_eos.argtypes = [ctypes.c_int, ctypes.c_int, _d, _d, _d, _d, _d]
         L.orc_forces.argtypes = [_d] * 11 + [ctypes.c_int, _l, _i, ctypes.c_double, ctypes.c_double,
-                                             ctypes.c_int, ctypes.c_int, ctypes.c_int] + [_d] * 6
+                                             ctypes.c_int, ctypes.c_int, ctypes.c_int] + [_d] * 7
+        L.orc_balsara.argtypes = [_d] * 10 + [ctypes.c_int, _l, _i, ctypes.c_int, _d, _d, _d]
         L.orc_variable_h.argtypes = [_d, _d, _d, _d, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int, ctypes.c_int, _i]
         L.orc_variable_h.restype = ctypes.c_int
@@ -225,14 +226,25 @@ def eos(eos_type, par, rho, e, p_prev):
 
 
 def forces(x, y, z, vx, vy, vz, m, h, rho, p, cs, off, nbr, alpha, beta, avg_h=False,
-           integrate_energy=True, integrate_sml=False):
+           integrate_energy=True, integrate_sml=False, bal=None):
     arrs = [_f64(a) for a in (x, y, z, vx, vy, vz, m, h, rho, p, cs)]
     n = len(x)
     outs = [np.zeros(n) for _ in range(6)]
+    b = _f64(bal) if bal is not None else None
     lib().orc_forces(*[_p(a) for a in arrs], n, _p(off, _l), _p(nbr, _i), float(alpha),
                      float(beta), int(avg_h), int(integrate_energy), int(integrate_sml),
-                     *[_p(o) for o in outs])
+                     *[_p(o) for o in outs], _p(b) if b is not None else None)
     return outs
+
+
+def balsara(x, y, z, vx, vy, vz, m, h, rho, cs, off, nbr, avg_h=False):
+    """Balsara switch: (div v, curl v [n x 3], f)."""
+    arrs = [_f64(a) for a in (x, y, z, vx, vy, vz, m, h, rho, cs)]
+    n = len(x)
+    divv, curl, f = np.zeros(n), np.zeros((n, 3)), np.zeros(n)
+    lib().orc_balsara(*[_p(a) for a in arrs], n, _p(off, _l), _p(nbr, _i), int(avg_h), _p(divv), _p(curl),
+                      _p(f))
+    return divv, curl, f
 
 
 def variable_h(x, y, z, h, target, tol=5, max_nb=180, max_iter=5):

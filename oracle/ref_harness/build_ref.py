@@ -7,7 +7,8 @@ parameter.h per test case (testcases/*/parameter.h, copied over
 include/parameter.h before a build); here the test case's header is
 pre-included (-include), so its include guard shadows include/parameter.h.
 Boost.MPI, MPI and libconfig are replaced by the single-rank shims in
-oracle/ref_harness/shim.  Flags follow the reference Makefile (-dc -fmad=false
+oracle/ref_harness/shim.  ref_sph_bal is the Sedov build with the Balsara
+switch on (balsara_on.h pre-included after the test case's parameter.h).  Flags follow the reference Makefile (-dc -fmad=false
 -O3), for sm_100a.  Outputs go only to oracle/_ref/ (git-ignored).
 """
 import os
@@ -23,26 +24,30 @@ COMMON = ["src/particles.cu", "src/particle_handler.cpp", "src/subdomain_key_tre
           "src/helper_handler.cpp", "src/device_rhs.cu", "src/cuda_utils/cuda_utilities.cu",
           "src/cuda_utils/cuda_launcher.cu", "src/cuda_utils/cuda_runtime.cpp", "src/cuda_utils/linalg.cu",
           "src/utils/logger.cpp", "src/materials/material.cu"]
+SPH_SRCS = COMMON + ["src/materials/material_handler.cpp", "src/sph/sph.cu", "src/sph/density.cu",
+                     "src/sph/soundspeed.cu", "src/sph/pressure.cu", "src/sph/internal_forces.cu",
+                     "src/sph/kernel.cu", "src/sph/kernel_handler.cu", "src/sph/stress.cu",
+                     "src/sph/artificial_stress.cu", "src/sph/viscosity.cu"]
+# name: (test-case parameter.h, extra pre-included header of this directory or None, sources)
 BUILDS = {
-    "gravity": ("testcases/plummer/parameter.h", COMMON + ["src/gravity/gravity.cu"]),
-    "sph": ("testcases/sedov/parameter.h",
-            COMMON + ["src/materials/material_handler.cpp", "src/sph/sph.cu", "src/sph/density.cu",
-                      "src/sph/soundspeed.cu", "src/sph/pressure.cu", "src/sph/internal_forces.cu",
-                      "src/sph/kernel.cu", "src/sph/kernel_handler.cu", "src/sph/stress.cu",
-                      "src/sph/artificial_stress.cu", "src/sph/viscosity.cu"]),
+    "gravity": ("testcases/plummer/parameter.h", None, COMMON + ["src/gravity/gravity.cu"]),
+    "sph": ("testcases/sedov/parameter.h", None, SPH_SRCS),
+    "sph_bal": ("testcases/sedov/parameter.h", "balsara_on.h", SPH_SRCS),
 }
 
 
 def build(verbose=False):
     if not os.path.isdir(REF):
         return False
-    for name, (param, srcs) in BUILDS.items():
+    for name, (param, extra, srcs) in BUILDS.items():
         objdir = os.path.join(OUT, "obj_" + name)
         os.makedirs(objdir, exist_ok=True)
         exe = os.path.join(OUT, "ref_" + name)
         flags = ["nvcc", "-std=c++14", "-x", "cu", "-dc", "-w", "-fmad=false", "-O3",
-                 "-gencode", "arch=compute_100a,code=sm_100a", "-include", os.path.join(REF, param),
-                 "-I" + os.path.join(HERE, "shim"), "-I" + os.path.join(REF, "include")]
+                 "-gencode", "arch=compute_100a,code=sm_100a", "-include", os.path.join(REF, param)]
+        if extra:
+            flags += ["-include", os.path.join(HERE, extra)]
+        flags += ["-I" + os.path.join(HERE, "shim"), "-I" + os.path.join(REF, "include")]
         objs = []
         for s in srcs + [os.path.join(HERE, "ref_driver.cu")]:
             src = s if os.path.isabs(s) else os.path.join(REF, s)

@@ -21,7 +21,8 @@
 // last cell), int32 MAX_NUM_INTERACTIONS, then (gravity) sorted[n],
 // child[8*numNodes], level, x, y, z, mass [numNodes each], g_ax, g_ay, g_az
 // [n each]; (SPH) noi[n], nnl[MAX_NUM_INTERACTIONS*n], rho, cs, p, ax, ay, az,
-// drhodt, dedt, dsmldt [n each], double diam.
+// drhodt, dedt, dsmldt [n each], double diam, and with BALSARA_SWITCH divv[n],
+// curlv[3n] (x, y, z per particle).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -182,6 +183,10 @@ int main(int argc, char** argv) {
     SPH::Kernel::Launch::fixedRadiusNN(th.d_tree, ph.d_particles, ph.d_nnl, diam, n, n, numNodes);
     SPH::Kernel::Launch::calculateDensity(kh.kernel, th.d_tree, ph.d_particles, ph.d_nnl, n);
     SPH::Kernel::Launch::calculateSoundSpeed(ph.d_particles, mh.d_materials, n);
+#if BALSARA_SWITCH
+    // src/miluphpc.cpp:2944-2947: divergence and curl of v after the sound speed
+    SPH::Kernel::Launch::CalcDivvandCurlv(kh.kernel, ph.d_particles, ph.d_nnl, n);
+#endif
     SPH::Kernel::Launch::calculatePressure(mh.d_materials, ph.d_particles, n);
     SPH::Kernel::Launch::internalForces(kh.kernel, mh.d_materials, th.d_tree, ph.d_particles, ph.d_nnl, n);
     CK(cudaDeviceSynchronize());
@@ -197,6 +202,10 @@ int main(int argc, char** argv) {
     wr(fo, dl(ph.d_dedt, n).data(), n);
     wr(fo, dl(ph.d_dsmldt, n).data(), n);
     wr(fo, &diam, 1);
+#if BALSARA_SWITCH
+    wr(fo, dl(ph.d_divv, n).data(), n);
+    wr(fo, dl(ph.d_curlv, (size_t)3 * n).data(), (size_t)3 * n);
+#endif
 #endif
     std::fclose(fo);
     std::fclose(fi);

@@ -160,7 +160,10 @@ def sph_input(seed=21):
     return dict(x=x, y=y, z=z, m=m, vx=vx, vy=vy, vz=vz, sml=h, e=e, p=p, cs=cs)
 
 
-def sph_case(out, run):
+def sph_case(out, run, balsara=False):
+    """ref_sph: the Sedov build; ref_sph_balsara: the same with the Balsara
+    switch on (harness build ref_sph_bal), which adds div v and curl v."""
+    name = "ref_sph_balsara" if balsara else "ref_sph"
     S = sph_input()
     n = len(S["x"])
     bb = O.bbox(S["x"], S["y"], S["z"])
@@ -169,17 +172,17 @@ def sph_case(out, run):
     noi = np.diff(off)
     if noi.max() > MAXNB_MARGIN or (S["m"] <= 0).any() or (S["p"] < 0).any() or (S["e"] < 0).any():
         raise RuntimeError("sph input outside the checked range")
-    print("ref_sph: n=%d depth=%d noi %d..%d" % (n, depth, noi.min(), noi.max()), flush=True)
+    print("%s: n=%d depth=%d noi %d..%d" % (name, n, depth, noi.min(), noi.max()), flush=True)
     if not run:
         return
     P = SPH_PARAMS
-    fin = os.path.join(out, "ref_sph.in")
-    fout = os.path.join(out, "ref_sph.out")
+    fin = os.path.join(out, name + ".in")
+    fout = os.path.join(out, name + ".out")
     with open(fin, "wb") as f:
         f.write(header(n, 0.0, 0.0, [P["interactions"], P["alpha"], P["beta"], P["eos"], P["K"], P["gamma"]]))
         for k in ("x", "y", "z", "m", "vx", "vy", "vz", "sml", "e", "p", "cs"):
             f.write(np.ascontiguousarray(S[k], dtype="<f8").tobytes())
-    subprocess.check_call([os.path.join(REF, "ref_sph"), fin, fout])
+    subprocess.check_call([os.path.join(REF, "ref_sph_bal" if balsara else "ref_sph"), fin, fout])
     buf = open(fout, "rb").read()
     pos = 0
 
@@ -195,6 +198,10 @@ def sph_case(out, run):
     nnl = take("<i4", int(maxnb) * n).reshape(n, int(maxnb))
     rho, cs, p, ax, ay, az, drhodt, dedt, dsmldt = (take("<f8", n) for _ in range(9))
     diam = take("<f8", 1)[0]
+    extra = {}
+    if balsara:
+        extra["divv"] = take("<f8", n)
+        extra["curlv"] = take("<f8", 3 * n).reshape(n, 3)
     nb_sum = np.zeros(n, dtype=np.int64)
     nb_sq = np.zeros(n, dtype=np.int64)
     for i in range(n):
@@ -203,10 +210,10 @@ def sph_case(out, run):
             raise RuntimeError("reference neighbour list of %d malformed" % i)
         nb_sum[i] = row.sum()
         nb_sq[i] = (row * row).sum()
-    np.savez_compressed(os.path.join(out, "ref_sph.npz"), **S, alpha=P["alpha"], beta=P["beta"],
+    np.savez_compressed(os.path.join(out, name + ".npz"), **S, alpha=P["alpha"], beta=P["beta"],
                         gamma=P["gamma"], bbox=bbox, diam=diam, noi=rnoi, nb_sum=nb_sum, nb_sq=nb_sq,
                         rho=rho, cs_out=cs, p_out=p, ax=ax, ay=ay, az=az, drhodt=drhodt, dedt=dedt,
-                        dsmldt=dsmldt)
+                        dsmldt=dsmldt, **extra)
     os.remove(fin)
     os.remove(fout)
 
@@ -215,12 +222,18 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--check-only", action="store_true", help="run the CPU input checks only")
+    ap.add_argument("--only", default=None, help="comma-separated fixture names to make")
     a = ap.parse_args()
+    only = a.only.split(",") if a.only else None
     os.makedirs(a.out, exist_ok=True)
     O.build()
     for case in GRAVITY_CASES:
-        gravity_case(*case, out=a.out, run=not a.check_only)
-    sph_case(a.out, run=not a.check_only)
+        if only is None or case[0] in only:
+            gravity_case(*case, out=a.out, run=not a.check_only)
+    if only is None or "ref_sph" in only:
+        sph_case(a.out, run=not a.check_only)
+    if only is None or "ref_sph_balsara" in only:
+        sph_case(a.out, run=not a.check_only, balsara=True)
 
 
 if __name__ == "__main__":

@@ -457,3 +457,27 @@ def test_coincident_particles(cuda):
     assert st["key_collisions"] >= 10
     assert np.isfinite(sim.numpy("g_ax")).all()
     sim.close()
+
+
+@pytest.mark.parametrize("criterion,d", [(0, 2.0), (1, 1.5)])
+def test_remove_particles(criterion, d, cuda):
+    """Miluphpc::removeParticles: the survivors keep their order in every
+    array, the tail is zeroed, n drops; a later step runs on the rest."""
+    n = 50_000
+    P = ics.plummer(n, seed=6)
+    r = np.sqrt(P["x"] ** 2 + P["y"] ** 2 + P["z"] ** 2)
+    keep = r < d if criterion == 0 else (np.abs(P["x"]) < d) & (np.abs(P["y"]) < d) & (np.abs(P["z"]) < d)
+    cfg = gravity_cfg(remove_particles=1, remove_particles_criterion=criterion, remove_particles_dimension=d,
+                      precision=1, theta_mixed=0.3)
+    sim = Miluphpc(cfg, P)
+    sim.t["g_ax"][:n] = torch.arange(n, dtype=torch.float64, device="cuda:0")
+    removed = sim.remove_particles()
+    assert removed == n - keep.sum() and sim.n == keep.sum() and removed > 0
+    for k in ("x", "y", "z", "mass", "vx"):
+        np.testing.assert_array_equal(sim.numpy(k), P[k][keep])
+        assert (sim.t[k][sim.n:n].cpu().numpy() == 0).all()
+    np.testing.assert_array_equal(sim.numpy("g_ax"), np.arange(n)[keep].astype(np.float64))
+    assert sim.remove_particles() == 0
+    sim.integrate(0)
+    assert np.isfinite(sim.numpy("g_ax")).all()
+    sim.close()

@@ -102,6 +102,32 @@ def test_oracle_sph_matches_reference():
         close_rates(got, ref)
 
 
+def test_oracle_balsara_matches_reference():
+    """Balsara switch (harness build with BALSARA_SWITCH on): div v, curl v of
+    CalcDivvandCurlv and the switched viscosity of internalForces."""
+    F = fixture("ref_sph_balsara")
+    x, y, z, m, h = F["x"], F["y"], F["z"], F["m"], F["sml"]
+    off, nbr = O.frnn(x, y, z, h)
+    assert np.array_equal(np.diff(off), F["noi"])
+    rho = O.density(x, y, z, m, h, off, nbr, avg_h=True)
+    np.testing.assert_allclose(rho, F["rho"], rtol=1e-12)
+    p, cs = O.eos(9, np.array([0.0, float(F["gamma"]), 0.0, 0.0, 0.0]), rho, F["e"], F["p"])
+    # INTEGRATE_SML without VARIABLE_SML: the gradients use h_i
+    divv, curl, f = O.balsara(x, y, z, F["vx"], F["vy"], F["vz"], m, h, rho, cs, off, nbr, avg_h=False)
+    close_rates(divv, F["divv"])
+    close_rates(curl, F["curlv"])
+    ax, ay, az, drho, de, dh = O.forces(x, y, z, F["vx"], F["vy"], F["vz"], m, h, rho, p, cs, off, nbr,
+                                        float(F["alpha"]), float(F["beta"]), avg_h=True, integrate_sml=True,
+                                        bal=f)
+    for got, ref in ((ax, F["ax"]), (ay, F["ay"]), (az, F["az"]), (drho, F["drhodt"]), (de, F["dedt"]),
+                     (dh, F["dsmldt"])):
+        close_rates(got, ref)
+    # the switch changes the answer: without it the viscous terms differ
+    ax0 = O.forces(x, y, z, F["vx"], F["vy"], F["vz"], m, h, rho, p, cs, off, nbr, float(F["alpha"]),
+                   float(F["beta"]), avg_h=True, integrate_sml=True)[0]
+    assert np.abs(ax0 - F["ax"]).max() > 1e-6 * np.abs(F["ax"]).max()
+
+
 # -------------------------------------------------------------- CUDA path --
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", GRAVITY)
@@ -155,4 +181,23 @@ def test_cuda_sph_matches_reference(cuda):
     for k, ref in (("ax", "ax"), ("ay", "ay"), ("az", "az"), ("drhodt", "drhodt"), ("dedt", "dedt"),
                    ("dsmldt", "dsmldt")):
         close_rates(sim.numpy(k), F[ref])
+    sim.close()
+
+
+@pytest.mark.gpu
+def test_cuda_balsara_matches_reference(cuda):
+    from miluphpc_b200.miluphpc import Miluphpc, material
+    from tests.helpers import sph_cfg
+    F = fixture("ref_sph_balsara")
+    S = {k: F[k].copy() for k in ("x", "y", "z", "vx", "vy", "vz", "sml", "e", "p", "cs")}
+    S["mass"] = F["m"].copy()
+    cfg = sph_cfg(integrate_sml=1, balsara=1)
+    mat = material(interactions=50, alpha=float(F["alpha"]), beta=float(F["beta"]), eos_type=9,
+                   gamma=float(F["gamma"]))
+    sim = Miluphpc(cfg, S, materials=[mat])
+    sim.rhs(0)
+    assert np.array_equal(sim.numpy("noi"), F["noi"])
+    np.testing.assert_allclose(sim.numpy("rho"), F["rho"], rtol=1e-12)
+    for k in ("ax", "ay", "az", "drhodt", "dedt", "dsmldt"):
+        close_rates(sim.numpy(k), F[k])
     sim.close()
