@@ -275,6 +275,12 @@ int mhpc_remove_particles(mhpc_ctx* ctx, mhpc_particles* p, int* n_removed);
 int mhpc_direct_gravity(const double* x, const double* y, const double* z, const double* m, int n,
                         const int* targets, int nt, double eps2, double* gax, double* gay,
                         double* gaz, void* stream);
+/* The same with a per-target softening added: target t uses eps2 +
+ * eps2_targets[t] (device, nt doubles), e.g. (softening_h_factor h_i)^2 to
+ * check the walks' h-tied softening rule. */
+int mhpc_direct_gravity_soft(const double* x, const double* y, const double* z, const double* m, int n,
+                             const int* targets, int nt, double eps2, const double* eps2_targets, double* gax,
+                             double* gay, double* gaz, void* stream);
 
 /* Measured FP32 FMA throughput of the current device in TFLOP/s (dependent
  * FFMA chains on every SM; the roofline denominator of the FP32 walk).

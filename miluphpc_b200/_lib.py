@@ -125,6 +125,8 @@ def load():
     L.mhpc_remove_particles.argtypes = [c_void_p, ctypes.POINTER(Particles), P_i]
     L.mhpc_direct_gravity.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_double,
                                       c_void_p, c_void_p, c_void_p, c_void_p]
+    L.mhpc_direct_gravity_soft.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int,
+                                           c_double, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
     L.mhpc_fp32_peak.argtypes = [P_d]
     L.mhpc_mlp_reset.argtypes = [c_void_p, ctypes.c_uint64]
     L.mhpc_mlp_train.argtypes = [c_void_p, c_int, c_float, P_f]
@@ -161,5 +163,5 @@ EXPORTS = [
     "mhpc_stage_gravity", "mhpc_stage_sph", "mhpc_export_sorted", "mhpc_export_tree", "mhpc_get_stats",
     "mhpc_diagnostics", "mhpc_direct_gravity", "mhpc_fp32_peak", "mhpc_mlp_reset", "mhpc_mlp_train", "mhpc_mlp_num_params",
     "mhpc_mlp_forward_backward", "mhpc_mlp_get_params", "mhpc_mlp_set_params",
-    "mhpc_remove_particles",
+    "mhpc_remove_particles", "mhpc_direct_gravity_soft",
 ]

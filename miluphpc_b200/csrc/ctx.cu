@@ -798,7 +798,15 @@ int mhpc_diagnostics(mhpc_ctx* c, const mhpc_particles* p, double* out) {
 int mhpc_direct_gravity(const double* x, const double* y, const double* z, const double* m, int n, const int* targets,
                         int nt, double eps2, double* gax, double* gay, double* gaz, void* stream) {
     if (n < 0 || nt < 0 || (nt > 0 && (!x || !y || !z || !m || !targets || !gax || !gay || !gaz))) return MHPC_ERR_ARG;
-    return launch_direct(x, y, z, m, n, targets, nt, eps2, gax, gay, gaz, (cudaStream_t)stream);
+    return launch_direct(x, y, z, m, n, targets, nt, eps2, nullptr, gax, gay, gaz, (cudaStream_t)stream);
+}
+
+int mhpc_direct_gravity_soft(const double* x, const double* y, const double* z, const double* m, int n,
+                             const int* targets, int nt, double eps2, const double* eps2_targets, double* gax,
+                             double* gay, double* gaz, void* stream) {
+    if (n < 0 || nt < 0 || (nt > 0 && (!x || !y || !z || !m || !targets || !eps2_targets || !gax || !gay || !gaz)))
+        return MHPC_ERR_ARG;
+    return launch_direct(x, y, z, m, n, targets, nt, eps2, eps2_targets, gax, gay, gaz, (cudaStream_t)stream);
 }
 
 // ------------------------------------------------ learned smoothing length

@@ -258,13 +258,15 @@ __global__ void k_diag_final(int blocks, const double* part, double* out, const 
 // a slice of the sources, staged 256 at a time in shared memory.
 __global__ void __launch_bounds__(256) k_direct(const double* __restrict__ x, const double* __restrict__ y,
                                                 const double* __restrict__ z, const double* __restrict__ m, int n,
-                                                const int* __restrict__ tg, int nt, double eps2, double* gax,
-                                                double* gay, double* gaz) {
+                                                const int* __restrict__ tg, int nt, double eps2,
+                                                const double* __restrict__ eps2_t, double* gax, double* gay,
+                                                double* gaz) {
     __shared__ double4 src[256];
     const int t = blockIdx.x * 256 + threadIdx.x;
     const bool valid = t < nt;
     const int ti = valid ? tg[t] : 0;
     const double px = x[ti], py = y[ti], pz = z[ti];
+    if (eps2_t && valid) eps2 += eps2_t[t];  // softening of the target (h-tied rule)
     const long per = ((long)n + gridDim.y - 1) / gridDim.y;
     const long j0 = (long)blockIdx.y * per;
     const long j1 = min((long)n, j0 + per);
@@ -436,7 +438,7 @@ int launch_diagnostics(const mhpc_particles& p, int sph, double* part, double* o
 size_t diagnostics_scratch_doubles() { return 148 * 4 * kDiag + 16; }
 
 int launch_direct(const double* x, const double* y, const double* z, const double* m, int n, const int* tg, int nt,
-                  double eps2, double* gax, double* gay, double* gaz, cudaStream_t s) {
+                  double eps2, const double* eps2_t, double* gax, double* gay, double* gaz, cudaStream_t s) {
     if (nt <= 0) return MHPC_OK;
     CUDA_TRY(cudaMemsetAsync(gax, 0, sizeof(double) * nt, s));
     CUDA_TRY(cudaMemsetAsync(gay, 0, sizeof(double) * nt, s));
@@ -447,7 +449,7 @@ int launch_direct(const double* x, const double* y, const double* z, const doubl
     long maxby = ((long)n + 255) / 256;
     if (by > maxby) by = (int)maxby;
     dim3 grid(bx, by);
-    k_direct<<<grid, 256, 0, s>>>(x, y, z, m, n, tg, nt, eps2, gax, gay, gaz);
+    k_direct<<<grid, 256, 0, s>>>(x, y, z, m, n, tg, nt, eps2, eps2_t, gax, gay, gaz);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

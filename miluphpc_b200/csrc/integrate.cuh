@@ -34,4 +34,4 @@ int launch_compact_i(int n, const int* keep, const int* rank, const int* src, in
 int launch_diagnostics(const mhpc_particles& p, int sph, double* part, double* out, cudaStream_t s);
 size_t diagnostics_scratch_doubles();
 int launch_direct(const double* x, const double* y, const double* z, const double* m, int n, const int* tg, int nt,
-                  double eps2, double* gax, double* gay, double* gaz, cudaStream_t s);
+                  double eps2, const double* eps2_t, double* gax, double* gay, double* gaz, cudaStream_t s);

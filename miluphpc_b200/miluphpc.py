@@ -177,14 +177,21 @@ class Miluphpc:
             pass
 
 
-def direct_gravity(x, y, z, m, targets, eps2):
-    """FP64 direct summation on the GPU (verification): torch tensors in, (gx, gy, gz) out."""
+def direct_gravity(x, y, z, m, targets, eps2, eps2_targets=None):
+    """FP64 direct summation on the GPU (verification): torch tensors in, (gx, gy, gz) out.
+    eps2_targets (optional, per target) is added to eps2 (h-tied softening)."""
     L = _lib.load()
     nt = int(targets.numel())
     out = [torch.zeros(nt, dtype=torch.float64, device=x.device) for _ in range(3)]
     st = torch.cuda.current_stream(x.device).cuda_stream
-    check(L.mhpc_direct_gravity(*(ctypes.c_void_p(t.data_ptr()) for t in (x, y, z, m)), int(x.numel()),
-                                ctypes.c_void_p(targets.data_ptr()), nt, float(eps2),
-                                *(ctypes.c_void_p(o.data_ptr()) for o in out), ctypes.c_void_p(st)),
-          "direct_gravity")
+    ptrs = [ctypes.c_void_p(t.data_ptr()) for t in (x, y, z, m)]
+    if eps2_targets is None:
+        check(L.mhpc_direct_gravity(*ptrs, int(x.numel()), ctypes.c_void_p(targets.data_ptr()), nt, float(eps2),
+                                    *(ctypes.c_void_p(o.data_ptr()) for o in out), ctypes.c_void_p(st)),
+              "direct_gravity")
+    else:
+        check(L.mhpc_direct_gravity_soft(*ptrs, int(x.numel()), ctypes.c_void_p(targets.data_ptr()), nt,
+                                         float(eps2), ctypes.c_void_p(eps2_targets.data_ptr()),
+                                         *(ctypes.c_void_p(o.data_ptr()) for o in out), ctypes.c_void_p(st)),
+              "direct_gravity_soft")
     return out
