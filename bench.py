@@ -30,10 +30,10 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     # Plummer at scale, precision form: N = 2^24, Hilbert keys, leapfrog dt 0.01
     "plummer16m": dict(kind="gravity", n=1 << 24, sfc=1, dt=0.01, eps2=1e-4, theta=0.5, theta_mixed=0.28,
-                       mac_alpha=1.8e-3, theta_plain_matched=0.1, seed=1),
+                       mac_alpha=1.8e-3, mac_quad_alpha=3e-4, theta_plain_matched=0.1, seed=1),
     # profiling case of the walk: node data (~190 MB) larger than L2
     "plummer2m": dict(kind="gravity", n=1 << 21, sfc=1, dt=0.01, eps2=1e-4, theta=0.5, theta_mixed=0.28,
-                      mac_alpha=1.8e-3, theta_plain_matched=0.1, seed=1),
+                      mac_alpha=1.8e-3, mac_quad_alpha=3e-4, theta_plain_matched=0.1, seed=1),
     # Sedov blast, SPH only: 128^3 lattice, fixed h = 2.5 dx, predictor-corrector
     "sedov2m": dict(kind="sph", nside=128, n=128 ** 3, sfc=0, dt_max=1e-4, seed=2),
     "sedov262k": dict(kind="sph", nside=64, n=64 ** 3, sfc=0, dt_max=1e-4, seed=2),
@@ -46,7 +46,7 @@ WORKLOADS = {
                     theta_plain_matched=0.05, train_steps=20, train_iters=1500, seed=3),
     # the reference's own single-rank case: N = 131072, Lebesgue, leapfrog dt 0.025
     "plummer131k": dict(kind="gravity", n=131072, sfc=0, dt=0.025, eps2=1e-4, theta=0.5, theta_mixed=0.28,
-                        mac_alpha=1.8e-3, theta_plain_matched=0.1, seed=1),
+                        mac_alpha=1.8e-3, mac_quad_alpha=3e-4, theta_plain_matched=0.1, seed=1),
 }
 
 FLOP_MONO = 19   # flop per accepted particle-node monopole interaction
@@ -173,6 +173,7 @@ def make_sim(wl, state, variant):
             # relative opening rule from the second right-hand side on
             kw["gravity_mac"] = 1
             kw["mac_alpha"] = wl["mac_alpha"]
+            kw["mac_quad_alpha"] = wl.get("mac_quad_alpha", 0.0)
     elif variant == "plain_matched":
         kw["theta"] = wl["theta_plain_matched"]
     cfg = _lib.default_config(**kw)
@@ -543,6 +544,8 @@ def main():
                     help="override the accuracy-matched opening parameter of the plain FP64 walk")
     ap.add_argument("--mac-alpha", type=float, default=None,
                     help="relative opening rule of the list walk (0: geometric rule only)")
+    ap.add_argument("--mac-quad-alpha", type=float, default=None,
+                    help="relative rule: cells with a small quadrupole term enter as monopoles (0: never)")
     ap.add_argument("--mixed-walk", default="lists", choices=["lists", "vote"],
                     help="mixed walk: interaction lists (precision 1) or per-lane vote (precision 2)")
     args = ap.parse_args()
@@ -551,6 +554,8 @@ def main():
         wl["theta_mixed"] = args.theta_mixed
     if args.mac_alpha is not None:
         wl["mac_alpha"] = args.mac_alpha
+    if args.mac_quad_alpha is not None:
+        wl["mac_quad_alpha"] = args.mac_quad_alpha
     if args.theta_plain is not None:
         wl["theta_plain_matched"] = args.theta_plain
     wl["mixed_precision"] = 1 if args.mixed_walk == "lists" else 2

@@ -92,6 +92,9 @@ typedef struct mhpc_config {
     double mac_alpha;          /* accuracy parameter of the relative rule (0.003: p99 force error ~8e-4) */
     int balsara;               /* BALSARA_SWITCH: viscous mu_ij scaled by (f_i + f_j)/2,
                                   f = |div v| / (|div v| + |curl v| + 1e-4 c_s / h) */
+    double mac_quad_alpha;     /* relative rule only: an accepted cell whose quadrupole term is small,
+                                  M l^2 <= mac_quad_alpha |a| d^4 for every sub-box, enters as a monopole
+                                  (0: every accepted cell with its quadrupole) */
 } mhpc_config;
 
 /* Material (include/materials/material.cuh:123-150), one entry of the

@@ -41,7 +41,7 @@ class Config(ctypes.Structure):
         ("nb_tolerance", c_int), ("max_sml_iterations", c_int),
         ("precision", c_int), ("theta_mixed", c_double), ("learned_h", c_int), ("softening_mode", c_int),
         ("softening_h_factor", c_double), ("node_pool_factor", c_double),
-        ("gravity_mac", c_int), ("mac_alpha", c_double), ("balsara", c_int),
+        ("gravity_mac", c_int), ("mac_alpha", c_double), ("balsara", c_int), ("mac_quad_alpha", c_double),
     ]
 
 

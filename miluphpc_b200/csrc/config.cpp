@@ -195,6 +195,7 @@ void mhpc_config_default(mhpc_config* c) {
     c->gravity_mac = 0;
     c->mac_alpha = 0.003;
     c->balsara = 0;
+    c->mac_quad_alpha = 0.0;
 }
 
 int mhpc_config_from_info(const char* path, mhpc_config* c) {
@@ -240,6 +241,7 @@ int mhpc_config_from_info(const char* path, mhpc_config* c) {
     i("gravityMac", &c->gravity_mac);
     f("macAlpha", &c->mac_alpha);
     b("balsaraSwitch", &c->balsara);
+    f("macQuadAlpha", &c->mac_quad_alpha);
     if (c->gravity_mac < 0 || c->gravity_mac > 1 || (c->gravity_mac == 1 && c->mac_alpha <= 0))
         return MHPC_ERR_CONFIG;
     if (c->integrator < 0 || c->integrator > 2 || c->sfc < 0 || c->sfc > 1 || c->theta <= 0 ||

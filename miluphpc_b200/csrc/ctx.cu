@@ -190,6 +190,7 @@ int stage_gravity(mhpc_ctx* c, const mhpc_particles* p) {
     if (c->cfg.precision == 1) {
         G.theta = c->cfg.theta_mixed;
         G.rel_alpha = (c->cfg.gravity_mac == 1 && c->grav_prev_n == p->n) ? c->cfg.mac_alpha : 0.0;
+        G.quad_alpha = G.rel_alpha > 0.0 ? c->cfg.mac_quad_alpha : 0.0;
         TRY(gravity_lists(c->T, G, c->sx, c->sy, c->sz, c->sh, c->perm, p->g_ax, p->g_ay, p->g_az, c->st,
                           c->stream));
     } else if (c->cfg.precision == 2) {

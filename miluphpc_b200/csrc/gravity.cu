@@ -408,6 +408,7 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
         // relative rule: alpha times the smallest previous |a| of the sub-box
         // (read before this walk overwrites the accelerations)
         float amin = 0.f;
+        const float qratio = kRel ? (float)(P.quad_alpha / P.rel_alpha) : 0.f;
         if (kRel) {
             const int o = __ldg(perm + sl[k]);
             const double gx = gax[o], gy = gay[o], gz = gaz[o];
@@ -426,7 +427,8 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
         }
         if ((lane & 7) == 0) {
             S.blo[4 * k + (lane >> 3)] = make_float4(bx0, by0, bz0, amin);
-            S.bhi[4 * k + (lane >> 3)] = make_float4(bx1, by1, bz1, 0.f);
+            // bhi.w: quad_alpha |a|_min of the sub-box (monopole threshold)
+            S.bhi[4 * k + (lane >> 3)] = make_float4(bx1, by1, bz1, kRel ? amin * qratio : 0.f);
         }
     }
     const double edge0 = ord_to_dbl(P.ord[1]) - ord_to_dbl(P.ord[0]);
@@ -475,6 +477,10 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
                 // kRel: squared edge of the cell, edge0^2 / 4^level (exact power of two)
                 const float l2 = kRel ? edge2 * __int_as_float((127 - 2 * (info & 0xff)) << 23) : 0.f;
                 bool ok = true;
+                // relative rule: the quadrupole term M l^2 / d^4 below
+                // quad_alpha |a| for every sub-box makes the cell a monopole
+                bool mono = kRel;
+                const float ml2 = m * l2;
 #pragma unroll
                 for (int b = 0; b < kListSub; ++b) {
                     const float4 lo = S.blo[b], hi = S.bhi[b];
@@ -486,11 +492,14 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
                         // safety bound d >= l, then M l^3 <= alpha |a| d^5
                         // (d2 = 0 gives NaN: not accepted)
                         ok = ok && l2 <= d2 && w3.w <= lo.w * (d2 * d2) * (d2 * rsqrtf(d2));
+                        mono = mono && ml2 <= hi.w * (d2 * d2);
                     } else {
                         ok = ok && lp.w <= d2;
                     }
                 }
-                acc_cell = ok;
+                // accepted monopoles go to the leaf list (monopole evaluation)
+                acc_leaf = ok && mono;
+                acc_cell = ok && !mono;
                 open = !ok;
             }
         }

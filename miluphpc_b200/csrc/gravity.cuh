@@ -10,6 +10,7 @@ struct GravParams {
     const long long* ord; // device bounding box (ordered-int min, max); radius = (max - min) / 2
     double rel_alpha;     // interaction-list walk: relative opening rule with this alpha (0 = off), reading
                           // the previous accelerations from the output arrays before overwriting them
+    double quad_alpha;    // relative rule: accepted cells with M l^2 <= quad_alpha |a| d^4 enter as monopoles
 };
 
 // Plain FP64 walk with the reference's computeForces_v2 semantics.

@@ -525,7 +525,8 @@ static void gravity_boxes_impl(const double* x, const double* y, const double* z
                                const double* q, const int* child, const int* level, const int* sorted,
                                int n, int gsize, int nsub, double radius, double theta, double eps2,
                                const double* h, double h_factor, const double* amag, double alpha, int lpow,
-                               double* gax, double* gay, double* gaz, int* ninter, int* nquad) {
+                               double* gax, double* gay, double* gaz, int* ninter, int* nquad,
+                               double mono_alpha = 0.0) {
     const int ngroups = (n + gsize - 1) / gsize;
     const int w = gsize / nsub;
 #pragma omp parallel for schedule(dynamic, 4)
@@ -548,10 +549,11 @@ static void gravity_boxes_impl(const double* x, const double* y, const double* z
         std::vector<int> stack;
         for (int i = 0; i < 8; ++i) if (child[i] != -1) stack.push_back(child[i]);
         std::vector<int> acc_nodes;
-        int ncell = 0;
+        std::vector<char> use_quad;
+        int ncell = 0, nquad_g = 0;
         while (!stack.empty()) {
             int nd = stack.back(); stack.pop_back();
-            if (nd < n) { acc_nodes.push_back(nd); continue; }
+            if (nd < n) { acc_nodes.push_back(nd); use_quad.push_back(0); continue; }
             const double edge = 2.0 * radius * std::ldexp(1.0, -level[nd]);
             const double cr = edge * edge / theta;
             const double c[3] = {x[nd], y[nd], z[nd]};
@@ -569,7 +571,24 @@ static void gravity_boxes_impl(const double* x, const double* y, const double* z
                     ok = mass[nd] * lp <= alpha * amin[b] * dp;
                 }
             }
-            if (ok) { acc_nodes.push_back(nd); ++ncell; continue; }
+            if (ok) {
+                // monopole only when the quadrupole term M l^2 / d^4 stays below
+                // mono_alpha |a| for every sub-box (mono_alpha = 0: always quadrupole)
+                bool quad = true;
+                if (mono_alpha > 0.0 && amag) {
+                    quad = false;
+                    for (int b = 0; b < nsub && !quad; ++b) {
+                        double d2 = 0.0;
+                        for (int d = 0; d < 3; ++d) {
+                            const double e = std::max(std::max(lo[3 * b + d] - c[d], c[d] - hi[3 * b + d]), 0.0);
+                            d2 += e * e;
+                        }
+                        quad = !(mass[nd] * edge * edge <= mono_alpha * amin[b] * d2 * d2);
+                    }
+                }
+                acc_nodes.push_back(nd); use_quad.push_back(quad ? 1 : 0); ++ncell; nquad_g += quad;
+                continue;
+            }
             for (int i = 0; i < 8; ++i) if (child[8 * nd + i] != -1) stack.push_back(child[8 * nd + i]);
         }
         for (int l = 0; l < lanes; ++l) {
@@ -577,14 +596,15 @@ static void gravity_boxes_impl(const double* x, const double* y, const double* z
             double e2 = eps2;
             if (h && h_factor > 0.0) { const double e = h_factor * h[s]; e2 += e * e; }
             double ax = 0, ay = 0, az = 0;
-            for (int nd : acc_nodes) {
+            for (size_t t = 0; t < acc_nodes.size(); ++t) {
+                const int nd = acc_nodes[t];
                 if (nd == s) continue;
                 double R[3] = {x[s] - x[nd], y[s] - y[nd], z[s] - z[nd]};
                 double r2 = R[0] * R[0] + R[1] * R[1] + R[2] * R[2] + e2;
                 double ri = 1.0 / std::sqrt(r2), ri2 = ri * ri, ri3 = ri * ri2;
                 double m = mass[nd];
                 ax -= m * ri3 * R[0]; ay -= m * ri3 * R[1]; az -= m * ri3 * R[2];
-                if (q && nd >= n) {
+                if (q && nd >= n && use_quad[t]) {
                     const double* Q = q + 6 * nd;
                     double QR[3] = {Q[0] * R[0] + Q[1] * R[1] + Q[2] * R[2],
                                     Q[1] * R[0] + Q[3] * R[1] + Q[4] * R[2],
@@ -598,7 +618,7 @@ static void gravity_boxes_impl(const double* x, const double* y, const double* z
             }
             gax[s] = ax; gay[s] = ay; gaz[s] = az;
             if (ninter) ninter[s] = (int)acc_nodes.size();
-            if (nquad) nquad[s] = ncell;
+            if (nquad) nquad[s] = mono_alpha > 0.0 ? nquad_g : ncell;
         }
     }
 }
@@ -929,3 +949,12 @@ void orc_leapfrog_v(int n, double dt, double* vx, double* vy, double* vz, const 
 int orc_num_threads() { return omp_get_max_threads(); }
 
 }  // extern "C"
+
+extern "C" void orc_gravity_boxes_mono(const double* x, const double* y, const double* z, const double* mass,
+                                       const double* q, const int* child, const int* level, const int* sorted,
+                                       int n, int gsize, int nsub, double radius, double theta, double eps2,
+                                       const double* amag, double alpha, double mono_alpha, double* gax,
+                                       double* gay, double* gaz, int* ninter, int* nquad) {
+    gravity_boxes_impl(x, y, z, mass, q, child, level, sorted, n, gsize, nsub, radius, theta, eps2, nullptr, 0.0,
+                       amag, alpha, 3, gax, gay, gaz, ninter, nquad, mono_alpha);
+}

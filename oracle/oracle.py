@@ -82,6 +82,9 @@ def lib():
         L.orc_gravity_boxes_rel.argtypes = [_d, _d, _d, _d, _d, _i, _i, _i, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, _d,
                                             ctypes.c_double, _d, ctypes.c_double, ctypes.c_int, _d, _d, _d, _i, _i]
+        L.orc_gravity_boxes_mono.argtypes = [_d, _d, _d, _d, _d, _i, _i, _i, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, _d,
+                                             ctypes.c_double, ctypes.c_double, _d, _d, _d, _i, _i]
         _lib = L
     return _lib
 
@@ -322,4 +325,19 @@ def gravity_boxes_rel(tree, sorted_perm, radius, theta, eps2, q, amag, alpha, lp
                                 _p(tree.level, _i), _p(sp, _i), n, int(gsize), int(nsub), float(radius),
                                 float(theta), float(eps2), None, 0.0, _p(am), float(alpha), int(lpow),
                                 _p(ax), _p(ay), _p(az), _p(cnt, _i), _p(nq, _i))
+    return ax, ay, az, cnt, nq
+
+
+def gravity_boxes_mono(tree, sorted_perm, radius, theta, eps2, q, amag, alpha, mono_alpha, gsize=64, nsub=8):
+    """Relative-rule walk where accepted cells whose quadrupole term is below
+    mono_alpha |a| enter as monopoles (FP64); returns ax, ay, az, nodes,
+    cells with quadrupole (per particle)."""
+    n = tree.n
+    ax = np.zeros(n); ay = np.zeros(n); az = np.zeros(n)
+    cnt = np.zeros(n, dtype=np.int32); nq = np.zeros(n, dtype=np.int32)
+    sp = np.ascontiguousarray(sorted_perm, dtype=np.int32)
+    lib().orc_gravity_boxes_mono(_p(tree.x), _p(tree.y), _p(tree.z), _p(tree.m), _p(q), _p(tree.child, _i),
+                                 _p(tree.level, _i), _p(sp, _i), n, int(gsize), int(nsub), float(radius),
+                                 float(theta), float(eps2), _p(_f64(amag)), float(alpha), float(mono_alpha),
+                                 _p(ax), _p(ay), _p(az), _p(cnt, _i), _p(nq, _i))
     return ax, ay, az, cnt, nq
