@@ -3,20 +3,19 @@
 //
 // Neighbour search: the reference walks the tree once per particle with a
 // per-thread stack (SPH::fixedRadiusNN, src/sph/sph.cu:93-281).  Here a warp
-// walks once for 32 consecutive SFC-sorted particles: nodes whose particle
-// bounding box overlaps the group's search box (group box grown by each
-// lane's h) are opened, overlapping leaves and small cells are staged as
-// candidates in shared memory, and each lane then tests the staged
-// candidates with the reference's pair rule d^2 < h_i^2 && d^2 < h_j^2
-// (j != i), d^2 formed without FMA contraction like the reference build.  The
-// walk is conservative, so the neighbour set equals the brute-force set.
+// walks once for 32 consecutive SFC-sorted particles, lane-parallel over a
+// shared-memory stack, stages the particles of overlapping leaves and small
+// cells as candidates, keeps those that can reach one of the warp's four
+// 8-particle sub-groups, and tests each sub-group's particles only against
+// its own candidates with the reference's pair rule d^2 < h_i^2 && d^2 < h_j^2
+// (j != i), d^2 formed without FMA contraction like the reference build.  All
+// pruning is conservative, so the neighbour set equals the brute-force set.
 #include "sph.cuh"
 
 namespace {
 
 constexpr int kBlock = 128;
 constexpr int kWarps = kBlock / 32;
-constexpr int kCap = 512;     // staged candidates per warp
 constexpr int kSmall = 16;    // cells with at most this many particles are staged whole
 
 // ------------------------------------------------------------ kernels W
@@ -79,10 +78,50 @@ __device__ __forceinline__ size_t nb_index(long s, int k, int maxnb) {
 }
 
 // ------------------------------------------------------------ FRNN walk
+// One warp per 32 consecutive (sorted or listed) particles, lane = particle,
+// four sub-groups of 8 lanes.
+//
+// Traversal: lane-parallel over a per-warp stack in shared memory.  Every
+// step pops up to 32 nodes, one per lane; a node whose particle box misses
+// the group's search box (union of [x - h, x + h]), or whose box grown by
+// its largest h misses the group's points box, is dropped; leaves, cells of
+// at most kSmall particles and shared-key buckets become candidate ranges;
+// other cells push their children.  Stack bound as in the gravity list walk:
+// a pop of k nodes pushes at most 8k, and k is limited so that a depth-first
+// descent (7 per level, 22 levels) always fits on top of the stack.
+//
+// Candidates: the ranges are expanded 32 at a time; each candidate particle
+// is tested against the four sub-groups' boxes (search box, and points box
+// grown by h_j when smoothing lengths differ), both rounded outward to FP32
+// like the node boxes, so no pair that passes the exact test is dropped.
+// Candidates reaching some sub-group go to a shared-memory pool (x, y, z,
+// h_j^2, j) and to that sub-group's list.  A full pool is flushed: for each
+// sub-group, lane (8q + p) tests particle p of the sub-group against list
+// entry 4c + q, so the warp tests 32 pairs per step, and hits are written in
+// list order (ballot prefix over the 4 lanes of a particle).
+//
+// The pair rule is the reference's, d^2 < h_i^2 && d^2 < h_j^2 (j != i), d^2
+// formed without FMA contraction; the walk and the box tests are
+// conservative, so each neighbour set equals the brute-force set.
+//
 // mode 0: write lists (h_i = h[i], h_j = h[j]) for all particles; mode 1:
 // count only, with h_i = h[i], h_j = h[j] (the variable-h sweep passes the
 // sweep's snapshot as h), for the particles of `list` (list_count entries, in
 // sorted order, so 32 consecutive entries are still spatially close).
+constexpr int kStack = 512;
+constexpr int kReserve = 7 * 22 + 8;
+constexpr int kPool = 128;
+
+struct FrnnSmem {
+    int stk[kStack];
+    double cx[kPool], cy[kPool], cz[kPool], ch2[kPool];  // candidate position, h_j^2
+    int cj[kPool];                                        // candidate particle
+    unsigned char lst[4][kPool];                          // pool slots per sub-group
+    int rf[32], rend[32];                                 // staged ranges: first, end (prefix)
+    float4 slo[4], shi[4];                                // sub-group search boxes
+    float4 plo[4], phi[4];                                // sub-group points boxes
+};
+
 template <int MODE>
 __global__ void __launch_bounds__(kBlock) k_frnn(TreeDev T, int n, int maxnb, const double* __restrict__ sx,
                                                  const double* __restrict__ sy, const double* __restrict__ sz,
@@ -90,10 +129,11 @@ __global__ void __launch_bounds__(kBlock) k_frnn(TreeDev T, int n, int maxnb, co
                                                  const int* __restrict__ list_count,
                                                  const float* __restrict__ node_hmax, int* __restrict__ nbr,
                                                  int* __restrict__ noi, DevStatus* st) {
-    __shared__ int cand[kWarps][kCap];
+    __shared__ FrnnSmem smem[kWarps];
     if (st->code) return;
     const int M = *T.nodes;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
     const long g = ((long)blockIdx.x * kBlock + threadIdx.x) >> 5;
     long s = g * 32 + lane;
     bool valid = s < n;
@@ -105,17 +145,18 @@ __global__ void __launch_bounds__(kBlock) k_frnn(TreeDev T, int n, int maxnb, co
     }
     const bool active = valid;
     if (!__any_sync(MHPC_FULL, active)) return;
+    FrnnSmem& S = smem[w];
     double px = 0, py = 0, pz = 0, hi = 0;
     if (valid) { px = sx[s]; py = sy[s]; pz = sz[s]; hi = sh[s]; }
     const double hi2 = hi * hi;
+    // search box (x +- h) and points box, reduced over the sub-group (8
+    // lanes), stored rounded outward, then over the warp
     double lx = active ? px - hi : 1e300, ly = active ? py - hi : 1e300, lz = active ? pz - hi : 1e300;
     double ux = active ? px + hi : -1e300, uy = active ? py + hi : -1e300, uz = active ? pz + hi : -1e300;
-    // group points box (a neighbour j must also satisfy d < h_j, so nodes are
-    // tested against it grown by the node's largest h)
     double plx = active ? px : 1e300, ply = active ? py : 1e300, plz = active ? pz : 1e300;
     double pux = active ? px : -1e300, puy = active ? py : -1e300, puz = active ? pz : -1e300;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
+    for (int o = 1; o < 32; o <<= 1) {
         lx = fmin(lx, __shfl_xor_sync(MHPC_FULL, lx, o));
         ly = fmin(ly, __shfl_xor_sync(MHPC_FULL, ly, o));
         lz = fmin(lz, __shfl_xor_sync(MHPC_FULL, lz, o));
@@ -128,55 +169,189 @@ __global__ void __launch_bounds__(kBlock) k_frnn(TreeDev T, int n, int maxnb, co
         pux = fmax(pux, __shfl_xor_sync(MHPC_FULL, pux, o));
         puy = fmax(puy, __shfl_xor_sync(MHPC_FULL, puy, o));
         puz = fmax(puz, __shfl_xor_sync(MHPC_FULL, puz, o));
+        if (o == 4 && (lane & 7) == 0) {
+            const int q = lane >> 3;
+            S.slo[q] = make_float4(__double2float_rd(lx), __double2float_rd(ly), __double2float_rd(lz), 0.f);
+            S.shi[q] = make_float4(__double2float_ru(ux), __double2float_ru(uy), __double2float_ru(uz), 0.f);
+            S.plo[q] = make_float4(__double2float_rd(plx), __double2float_rd(ply), __double2float_rd(plz), 0.f);
+            S.phi[q] = make_float4(__double2float_ru(pux), __double2float_ru(puy), __double2float_ru(puz), 0.f);
+        }
     }
     const float qlx = __double2float_rd(lx), qly = __double2float_rd(ly), qlz = __double2float_rd(lz);
     const float qux = __double2float_ru(ux), quy = __double2float_ru(uy), quz = __double2float_ru(uz);
     const float rlx = __double2float_rd(plx), rly = __double2float_rd(ply), rlz = __double2float_rd(plz);
     const float rux = __double2float_ru(pux), ruy = __double2float_ru(puy), ruz = __double2float_ru(puz);
-    int k = 0;       // neighbours found by this lane
-    int cnt = 0;     // staged candidates (warp-uniform)
-    int* C = cand[w];
+    int k = 0;     // neighbours found for this lane's particle
+    int pool = 0;  // pool entries (warp-uniform)
+    int cnt0 = 0, cnt1 = 0, cnt2 = 0, cnt3 = 0;  // list entries per sub-group (warp-uniform)
     auto flush = [&]() {
         __syncwarp();
-        if (active) {
-            for (int c = 0; c < cnt; ++c) {
-                const int j = C[c];
-                if (j == s) continue;
-                const double dx = px - __ldg(sx + j), dy = py - __ldg(sy + j), dz = pz - __ldg(sz + j);
-                const double d = d2_exact(dx, dy, dz);
-                const double hj = __ldg(sh + j);
-                if (d < hi2 && d < hj * hj) {
-                    if (MODE == 0 && k < maxnb) nbr[nb_index(s, k, maxnb)] = j;
-                    ++k;
+        const int q = lane >> 3, p = lane & 7;
+#pragma unroll 1
+        for (int sg = 0; sg < 4; ++sg) {
+            const int cntg = sg == 0 ? cnt0 : sg == 1 ? cnt1 : sg == 2 ? cnt2 : cnt3;
+            const int src = 8 * sg + p;
+            const double ix = __shfl_sync(MHPC_FULL, px, src), iy = __shfl_sync(MHPC_FULL, py, src);
+            const double iz = __shfl_sync(MHPC_FULL, pz, src), ih2 = __shfl_sync(MHPC_FULL, hi2, src);
+            const int is = __shfl_sync(MHPC_FULL, (int)s, src);
+            const bool iact = __shfl_sync(MHPC_FULL, (int)active, src) != 0;
+            int kb = __shfl_sync(MHPC_FULL, k, src);
+            const unsigned pmask = 0x01010101u << p;
+            for (int c0 = 0; c0 < cntg; c0 += 4) {
+                const int c = c0 + q;
+                bool hit = false;
+                int j = 0;
+                if (iact && c < cntg) {
+                    const int slot = S.lst[sg][c];
+                    j = S.cj[slot];
+                    const double dx = ix - S.cx[slot], dy = iy - S.cy[slot], dz = iz - S.cz[slot];
+                    const double d = d2_exact(dx, dy, dz);
+                    hit = j != is && d < ih2 && d < S.ch2[slot];
+                }
+                const unsigned b = __ballot_sync(MHPC_FULL, hit) & pmask;
+                if (MODE == 0 && hit) {
+                    const int pos = kb + __popc(b & lt);
+                    if (pos < maxnb) nbr[nb_index(is, pos, maxnb)] = j;
+                }
+                kb += __popc(b);
+            }
+            // lane p (q = 0) holds particle 8 sg + p's count: its owner takes it
+            const int knew = __shfl_sync(MHPC_FULL, kb, p);
+            if (q == sg) k = knew;
+        }
+        __syncwarp();
+        pool = 0;
+        cnt0 = cnt1 = cnt2 = cnt3 = 0;
+    };
+    // the root's children: node 0 and its skip chain
+    int top = 0;
+    if (lane == 0) {
+        int c = 0;
+        while (c < M && top < 8) { S.stk[top++] = c; c = __ldg(&T.link[c].x); }
+        if (c < M) set_status(st, MHPC_ERR_DEPTH, 3);
+    }
+    top = __shfl_sync(MHPC_FULL, top, 0);
+    __syncwarp();
+    while (top > 0) {
+        const int room = (kStack - kReserve - top) / 7;
+        int kk = top < 32 ? top : 32;
+        if (kk > room) kk = room > 1 ? room : 1;
+        const bool act = lane < kk;
+        const int nd = act ? S.stk[top - 1 - lane] : 0;
+        __syncwarp();
+        top -= kk;
+        int rf = 0, rlen = 0, kmask = 0;
+        if (act) {
+            const int2 lk = __ldg(T.link + nd);
+            const float4 bl = __ldg(T.bmin + nd), bh = __ldg(T.bmax + nd);
+            bool overlap = !(bh.x < qlx || bl.x > qux || bh.y < qly || bl.y > quy || bh.z < qlz || bl.z > quz);
+            if (overlap && node_hmax) {
+                const float hn = __ldg(node_hmax + nd);
+                overlap = !(__fadd_ru(bh.x, hn) < rlx || __fadd_rd(bl.x, -hn) > rux || __fadd_ru(bh.y, hn) < rly ||
+                            __fadd_rd(bl.y, -hn) > ruy || __fadd_ru(bh.z, hn) < rlz || __fadd_rd(bl.z, -hn) > ruz);
+            }
+            if (overlap) {
+                rf = __ldg(T.first + nd);
+                if (lk.y & ND_LEAF) {
+                    rlen = 1;
+                } else {
+                    const int l = __ldg(T.last + nd);
+                    const int km = __ldg(T.kmask + nd);
+                    // small cells and shared-key buckets (all particles share
+                    // one key) are staged whole; other cells open
+                    if (l - rf + 1 <= kSmall || (km & 0x100)) rlen = l - rf + 1;
+                    else kmask = km & 0xff;
                 }
             }
         }
+        // push the children of opened cells
+        const int nkid = __popc(kmask);
+        int incl = nkid;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(MHPC_FULL, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(MHPC_FULL, incl, 31);
+        if (top + total > kStack) {
+            // unreachable by the bound on kk; stop instead of overrunning
+            if (lane == 0) set_status(st, MHPC_ERR_DEPTH, 4);
+            return;
+        }
+        if (nkid) {
+            const int4 k0 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)nd));
+            const int4 k1 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)nd) + 1);
+            const int all[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+            int wpos = top + incl - nkid;
+#pragma unroll
+            for (int d = 0; d < 8; ++d)
+                if ((kmask >> d) & 1) S.stk[wpos++] = all[d];
+        }
+        top += total;
+        // staged ranges: compact, with the running end of each
+        int rincl = rlen;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(MHPC_FULL, rincl, o);
+            if (lane >= o) rincl += v;
+        }
+        const int ncand = __shfl_sync(MHPC_FULL, rincl, 31);
+        const unsigned br = __ballot_sync(MHPC_FULL, rlen > 0);
+        const int nr = __popc(br);
+        if (rlen > 0) {
+            const int r = __popc(br & lt);
+            S.rf[r] = rf;
+            S.rend[r] = rincl;
+        }
         __syncwarp();
-        cnt = 0;
-    };
-    int nd = 0;
-    while (nd < M) {
-        const int2 lk = __ldg(T.link + nd);
-        const float4 bl = __ldg(T.bmin + nd), bh = __ldg(T.bmax + nd);
-        bool overlap = !(bh.x < qlx || bl.x > qux || bh.y < qly || bl.y > quy || bh.z < qlz || bl.z > quz);
-        if (overlap && node_hmax) {
-            const float hn = __ldg(node_hmax + nd);
-            overlap = !(__fadd_ru(bh.x, hn) < rlx || __fadd_rd(bl.x, -hn) > rux || __fadd_ru(bh.y, hn) < rly ||
-                        __fadd_rd(bl.y, -hn) > ruy || __fadd_ru(bh.z, hn) < rlz || __fadd_rd(bl.z, -hn) > ruz);
+        for (int c0 = 0; c0 < ncand; c0 += 32) {
+            if (pool + 32 > kPool) flush();
+            const int c = c0 + lane;
+            int mask = 0, j = 0;
+            double qx = 0, qy = 0, qz = 0, hj = 0;
+            if (c < ncand) {
+                int lo = 0, hi_r = nr - 1;
+                while (lo < hi_r) {
+                    const int mid = (lo + hi_r) >> 1;
+                    if (S.rend[mid] > c) hi_r = mid;
+                    else lo = mid + 1;
+                }
+                j = S.rf[lo] + c - (lo ? S.rend[lo - 1] : 0);
+                qx = __ldg(sx + j); qy = __ldg(sy + j); qz = __ldg(sz + j); hj = __ldg(sh + j);
+                const float xd = __double2float_rd(qx), xu = __double2float_ru(qx);
+                const float yd = __double2float_rd(qy), yu = __double2float_ru(qy);
+                const float zd = __double2float_rd(qz), zu = __double2float_ru(qz);
+                const float hf = __double2float_ru(hj);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float4 a = S.slo[q], b = S.shi[q];
+                    bool in = !(xu < a.x || xd > b.x || yu < a.y || yd > b.y || zu < a.z || zd > b.z);
+                    if (node_hmax) {
+                        const float4 e = S.plo[q], f = S.phi[q];
+                        in = in && !(__fadd_ru(xu, hf) < e.x || __fadd_rd(xd, -hf) > f.x ||
+                                     __fadd_ru(yu, hf) < e.y || __fadd_rd(yd, -hf) > f.y ||
+                                     __fadd_ru(zu, hf) < e.z || __fadd_rd(zd, -hf) > f.z);
+                    }
+                    mask |= (int)in << q;
+                }
+            }
+            const unsigned bp = __ballot_sync(MHPC_FULL, mask != 0);
+            if (mask) {
+                const int slot = pool + __popc(bp & lt);
+                S.cx[slot] = qx; S.cy[slot] = qy; S.cz[slot] = qz; S.ch2[slot] = hj * hj; S.cj[slot] = j;
+                const unsigned b0 = __ballot_sync(bp, mask & 1), b1 = __ballot_sync(bp, mask & 2);
+                const unsigned b2 = __ballot_sync(bp, mask & 4), b3 = __ballot_sync(bp, mask & 8);
+                if (mask & 1) S.lst[0][cnt0 + __popc(b0 & lt)] = (unsigned char)slot;
+                if (mask & 2) S.lst[1][cnt1 + __popc(b1 & lt)] = (unsigned char)slot;
+                if (mask & 4) S.lst[2][cnt2 + __popc(b2 & lt)] = (unsigned char)slot;
+                if (mask & 8) S.lst[3][cnt3 + __popc(b3 & lt)] = (unsigned char)slot;
+            }
+            const unsigned a0 = __ballot_sync(MHPC_FULL, mask & 1), a1 = __ballot_sync(MHPC_FULL, mask & 2);
+            const unsigned a2 = __ballot_sync(MHPC_FULL, mask & 4), a3 = __ballot_sync(MHPC_FULL, mask & 8);
+            cnt0 += __popc(a0); cnt1 += __popc(a1); cnt2 += __popc(a2); cnt3 += __popc(a3);
+            pool += __popc(bp);
         }
-        if (!overlap) { nd = lk.x; continue; }
-        const int f = __ldg(T.first + nd);
-        int len = 0;
-        if (lk.y & ND_LEAF) len = 1;
-        else {
-            const int l = __ldg(T.last + nd);
-            if (l - f + 1 <= kSmall) len = l - f + 1;
-        }
-        if (len == 0) { ++nd; continue; }
-        if (cnt + len > kCap) flush();
-        if (lane < len) C[cnt + lane] = f + lane;
-        cnt += len;
-        nd = lk.x;
+        __syncwarp();
     }
     flush();
     if (active) {

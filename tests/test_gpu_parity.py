@@ -372,6 +372,31 @@ def test_variable_h_matches_oracle(cuda):
     sim.close()
 
 
+def test_neighbour_lists_varying_h_and_shared_keys(cuda):
+    """Every particle's list equals the brute-force set when h varies by 4x
+    between neighbours (node and candidate pruning by h_j) and 40 particles
+    share one position (a shared-key bucket staged whole)."""
+    C = ics.rotating_cloud(20_000, seed=6)
+    n = len(C["x"])
+    C["sml"] = C["sml"] * np.random.default_rng(3).uniform(0.5, 2.0, n)
+    for k in ("x", "y", "z"):
+        C[k][7000:7040] = C[k][6000]
+    cfg = sph_cfg(integrate_sml=1, integrate_energy=0, max_num_interactions=600)
+    mat = material(interactions=60, eos_type=0, K=C["cs2"], gamma=1.0)
+    S = dict(C)
+    S["p"] = np.zeros(n)
+    S["cs"] = np.zeros(n)
+    sim = Miluphpc(cfg, S, materials=[mat], want_nnl=True)
+    sim.rhs(0)
+    off, nbr = O.frnn(C["x"], C["y"], C["z"], C["sml"])
+    noi = sim.numpy("noi")
+    assert np.array_equal(noi, np.diff(off))
+    nnl = sim.t["nnl"].cpu().numpy().reshape(n, cfg.max_num_interactions)
+    for i in range(n):
+        assert np.array_equal(np.sort(nnl[i, :noi[i]]), nbr[off[i]:off[i + 1]]), i
+    sim.close()
+
+
 def test_leapfrog_steps_match_oracle(cuda):
     n = 16_384
     P = ics.plummer(n, seed=8)
