@@ -370,7 +370,8 @@ __global__ void __launch_bounds__(kBlock) k_frnn(TreeDev T, int n, int maxnb, co
 // Per-lane count walk for sparse lists (later variable-h sweeps, where the
 // particles still iterating are scattered and a shared group box would be
 // large): every lane walks the tree for its own particle, pruning nodes whose
-// box does not come within h_i of it or whose largest h_j cannot reach it.
+// box does not come within h_i of it or whose largest h_j cannot reach it;
+// the particles of overlapping leaves and small cells are tested in a loop.
 __global__ void __launch_bounds__(kBlock) k_count_lane(TreeDev T, const double* __restrict__ sx,
                                                        const double* __restrict__ sy, const double* __restrict__ sz,
                                                        const double* __restrict__ sh, const int* __restrict__ list,
@@ -393,17 +394,20 @@ __global__ void __launch_bounds__(kBlock) k_count_lane(TreeDev T, const double* 
         const int2 lk = __ldg(T.link + nd);
         const float4 bl = __ldg(T.bmin + nd), bh = __ldg(T.bmax + nd);
         const float hn = __ldg(node_hmax + nd);
+        const int f = __ldg(T.first + nd), l = __ldg(T.last + nd);
         const bool overlap = !(bh.x < lx || bl.x > ux || bh.y < ly || bl.y > uy || bh.z < lz || bl.z > uz) &&
                              !(__fadd_ru(bh.x, hn) < fx0 || __fadd_rd(bl.x, -hn) > fx1 || __fadd_ru(bh.y, hn) < fy0 ||
                                __fadd_rd(bl.y, -hn) > fy1 || __fadd_ru(bh.z, hn) < fz0 || __fadd_rd(bl.z, -hn) > fz1);
         if (!overlap) { nd = lk.x; continue; }
-        if (lk.y & ND_LEAF) {
-            const int j = __ldg(T.first + nd);
-            if (j != s) {
+        if ((lk.y & ND_LEAF) || l - f + 1 <= kSmall) {
+            // a leaf or a small cell: test its particles directly (independent
+            // loads instead of one dependent node visit per particle)
+#pragma unroll 4
+            for (int j = f; j <= l; ++j) {
                 const double dx = px - __ldg(sx + j), dy = py - __ldg(sy + j), dz = pz - __ldg(sz + j);
                 const double d = d2_exact(dx, dy, dz);
                 const double hj = __ldg(sh + j);
-                if (d < hi2 && d < hj * hj) ++k;
+                k += (j != s && d < hi2 && d < hj * hj);
             }
             nd = lk.x;
         } else {
