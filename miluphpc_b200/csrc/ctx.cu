@@ -67,6 +67,11 @@ struct mhpc_ctx {
     // device mirror for mhpc_integrate_host
     mhpc_particles mirror;
     bool mirror_ready = false;
+    // mhpc_integrate_host, leapfrog: the drifted positions are copied out on
+    // copy_stream while the right-hand side runs (pos_out = host x, y, z)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_drift = nullptr;
+    double* pos_out[3] = {nullptr, nullptr, nullptr};
     std::vector<void*> allocs;
     MlpState* mlp = nullptr;
 };
@@ -446,6 +451,11 @@ int mhpc_ctx_destroy(mhpc_ctx* c) {
     for (int e = 0; e < EV_COUNT; ++e)
         if (c->ev[e]) cudaEventDestroy(c->ev[e]);
     if (c->mlp) mlp_destroy(c->mlp);
+    if (c->copy_stream) {
+        cudaStreamSynchronize(c->copy_stream);
+        cudaStreamDestroy(c->copy_stream);
+    }
+    if (c->ev_drift) cudaEventDestroy(c->ev_drift);
     if (c->mirror_ready) {
         double** ptrs[] = {&c->mirror.x, &c->mirror.y, &c->mirror.z, &c->mirror.mass, &c->mirror.vx, &c->mirror.vy,
                            &c->mirror.vz, &c->mirror.ax, &c->mirror.ay, &c->mirror.az, &c->mirror.g_ax,
@@ -536,6 +546,16 @@ int mhpc_integrate(mhpc_ctx* c, const mhpc_particles* p, int step, double* dt_ou
                 if (code) return code;
             }
             TRY(launch_leapfrog_x(*p, dt, s));
+            if (c->pos_out[0]) {
+                // positions are final after the drift: copy them out while the
+                // right-hand side (which only reads them) runs
+                const size_t b = sizeof(double) * p->n;
+                CUDA_TRY(cudaEventRecord(c->ev_drift, s));
+                CUDA_TRY(cudaStreamWaitEvent(c->copy_stream, c->ev_drift, 0));
+                const double* src[3] = {p->x, p->y, p->z};
+                for (int d = 0; d < 3; ++d)
+                    CUDA_TRY(cudaMemcpyAsync(c->pos_out[d], src[d], b, cudaMemcpyDeviceToHost, c->copy_stream));
+            }
             TRY(rhs_async(c, p, 1));
             TRY(launch_leapfrog_v(*p, dt, s));
         } break;
@@ -617,9 +637,22 @@ int mhpc_integrate_host(mhpc_ctx* c, mhpc_particles* h, int step, double* dt_out
     // leapfrog: step 0 computes the initial accelerations; later steps carry
     // the caller's g_a of the previous step
     if (c->cfg.integrator == 2) c->first_rhs_done = step != 0;
+    const bool overlap = c->cfg.integrator == 2 && h->x && h->y && h->z;
+    if (overlap) {
+        if (!c->copy_stream) {
+            CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+            CUDA_TRY(cudaEventCreateWithFlags(&c->ev_drift, cudaEventDisableTiming));
+        }
+        c->pos_out[0] = h->x; c->pos_out[1] = h->y; c->pos_out[2] = h->z;
+    }
     int rc = mhpc_integrate(c, &m, step, dt_out);
+    c->pos_out[0] = c->pos_out[1] = c->pos_out[2] = nullptr;
+    if (overlap) CUDA_TRY(cudaStreamSynchronize(c->copy_stream));
     if (rc) return rc;
-    std::vector<Pair> outp = {{m.x, h->x}, {m.y, h->y}, {m.z, h->z}, {m.vx, h->vx}, {m.vy, h->vy}, {m.vz, h->vz}};
+    std::vector<Pair> outp = {{m.vx, h->vx}, {m.vy, h->vy}, {m.vz, h->vz}};
+    if (!overlap) {
+        outp.push_back({m.x, h->x}); outp.push_back({m.y, h->y}); outp.push_back({m.z, h->z});
+    }
     if (c->cfg.gravity) {
         outp.push_back({m.g_ax, h->g_ax}); outp.push_back({m.g_ay, h->g_ay}); outp.push_back({m.g_az, h->g_az});
     }

@@ -5,7 +5,7 @@
 // cudaFree of temporary storage on every call (src/helper.cu:150-166).  This
 // sort is the library's own: one read of the keys builds all eight 8-bit digit
 // histograms, then each pass is a single "onesweep" kernel (tile ranking with
-// warp match/ballot, decoupled look-back across tiles, shared-memory staging so
+// warp ballots, decoupled look-back across tiles, shared-memory staging so
 // that the scatter writes runs of equal digits contiguously).  Scratch is
 // caller-provided; nothing is allocated per call.  Sorting is stable, so equal
 // keys keep ascending input position, which is the contract of the CUB call it
@@ -62,28 +62,33 @@ static SortScratch carve(void* base, int n) {
     return s;
 }
 
-// All eight digit histograms in one read of the keys; warp-aggregated shared
-// atomics, then one global atomic per bin per block.
+// Lanes of the warp holding the same 8-bit digit d: eight ballots, one per
+// digit bit (on B200 cheaper than a match instruction unless most lanes share
+// the digit).  Every lane of the warp must call it.
+__device__ __forceinline__ unsigned digit_peers(unsigned d) {
+    unsigned peers = MHPC_FULL;
+#pragma unroll
+    for (int b = 0; b < kRadixBits; ++b) {
+        const unsigned bb = __ballot_sync(MHPC_FULL, (d >> b) & 1u);
+        peers &= ((d >> b) & 1u) ? bb : ~bb;
+    }
+    return peers;
+}
+
+// All eight digit histograms in one read of the keys: plain shared-memory
+// atomics per key and digit (same-address conflicts within a warp are
+// resolved by the hardware faster than aggregating them first), then one
+// global atomic per bin per block.
 __global__ void __launch_bounds__(kBlock) k_hist(const uint64_t* __restrict__ keys, int n, unsigned* hist) {
     __shared__ unsigned sh[kPasses * kRadix];
     for (int i = threadIdx.x; i < kPasses * kRadix; i += kBlock) sh[i] = 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31;
     long stride = (long)gridDim.x * kBlock;
-    long nround = ((long)n + stride - 1) / stride;
-    for (long r = 0; r < nround; ++r) {
-        long i = r * stride + (long)blockIdx.x * kBlock + threadIdx.x;
-        bool valid = i < n;
-        unsigned vm = __ballot_sync(MHPC_FULL, valid);
-        uint64_t k = valid ? __ldg(keys + i) : 0;
-        if (valid) {
+    for (long i = (long)blockIdx.x * kBlock + threadIdx.x; i < n; i += stride) {
+        const uint64_t k = __ldg(keys + i);
 #pragma unroll
-            for (int p = 0; p < kPasses; ++p) {
-                unsigned d = (unsigned)(k >> (p * kRadixBits)) & (kRadix - 1);
-                unsigned peers = __match_any_sync(vm, d);
-                if (lane == __ffs(peers) - 1) atomicAdd(&sh[p * kRadix + d], __popc(peers));
-            }
-        }
+        for (int p = 0; p < kPasses; ++p)
+            atomicAdd(&sh[p * kRadix + ((unsigned)(k >> (p * kRadixBits)) & (kRadix - 1))], 1u);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < kPasses * kRadix; i += kBlock)
@@ -151,7 +156,8 @@ k_onesweep(const uint64_t* __restrict__ kin, const int* __restrict__ vin, uint64
         bool valid = idx < n;
         unsigned vm = __ballot_sync(MHPC_FULL, valid);
         unsigned d = (unsigned)(key[i] >> shift) & (kRadix - 1);
-        unsigned peers = valid ? __match_any_sync(vm, d) : (1u << lane);
+        unsigned peers = digit_peers(d) & vm;
+        if (!valid) peers = 1u << lane;
         int leader = __ffs(peers) - 1;
         unsigned b = 0;
         if (valid && lane == leader) b = S.whist[warp][d];

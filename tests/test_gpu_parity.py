@@ -397,6 +397,38 @@ def test_neighbour_lists_varying_h_and_shared_keys(cuda):
     sim.close()
 
 
+@pytest.mark.parametrize("pinned", [False, True])
+def test_integrate_host_matches_device(pinned, cuda):
+    """mhpc_integrate_host (host arrays in and out, positions copied out while
+    the right-hand side runs) gives the device path's state bit for bit."""
+    n = 20_000
+    P = ics.plummer(n, seed=9)
+    cfg = gravity_cfg(sfc=1, precision=1, theta_mixed=0.3, gravity_mac=1, mac_alpha=2e-3, time_step=0.01)
+    dev = Miluphpc(cfg, P)
+    for k in range(3):
+        dev.integrate(k)
+    hsim = Miluphpc(cfg, P)
+    fields = ["x", "y", "z", "mass", "vx", "vy", "vz", "g_ax", "g_ay", "g_az"]
+    host = {}
+    for f in fields:
+        t = torch.empty(n, dtype=torch.float64, pin_memory=pinned)
+        t.copy_(torch.as_tensor(P[f]) if f in P else torch.zeros(n, dtype=torch.float64))
+        host[f] = t
+    hp = _lib.Particles()
+    hp.n = n
+    hp.num_nodes = n
+    for f in fields:
+        setattr(hp, f, ctypes.cast(ctypes.c_void_p(host[f].data_ptr()), _lib.P_d))
+    L = _lib.load()
+    dt = ctypes.c_double()
+    for k in range(3):
+        _lib.check(L.mhpc_integrate_host(hsim.ctx, ctypes.byref(hp), k, ctypes.byref(dt)), "integrate_host")
+    for f in ["x", "y", "z", "vx", "vy", "vz", "g_ax", "g_ay", "g_az"]:
+        assert np.array_equal(host[f].numpy(), dev.numpy(f)), f
+    dev.close()
+    hsim.close()
+
+
 def test_leapfrog_steps_match_oracle(cuda):
     n = 16_384
     P = ics.plummer(n, seed=8)
