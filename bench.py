@@ -38,11 +38,13 @@ WORKLOADS = {
     "sedov2m": dict(kind="sph", nside=128, n=128 ** 3, sfc=0, dt_max=1e-4, seed=2),
     "sedov262k": dict(kind="sph", nside=64, n=64 ** 3, sfc=0, dt_max=1e-4, seed=2),
     # self-gravitating isothermal rotating cloud, variable h (60 +- 5), learned h
-    # (accuracy-matched on the cloud with h-tied softening, p99 <= 1e-3: mixed relative rule
-    # alpha = 1.2e-3 -> 8.4e-4 at 8.4M; plain FP64 v2 theta = 0.05 -> 9.8e-4, theta = 0.07 -> 2.9e-3)
+    # (accuracy-matched on the cloud with h-tied softening, p99 <= 1e-3 against the
+    # direct sum softened with the h the walk used: mixed relative rule alpha = 1.0e-3
+    # -> 8.1e-4 at 1M, 1.5e-3 at 8.4M (1.2e-3 -> 8.2e-4, 1.8e-3 -> 9.7e-4); plain
+    # FP64 v2 theta = 0.05 -> 9.7e-4 at 1M, theta = 0.07 -> 2.9e-3 at 8.4M)
     "cloud1m": dict(kind="cloud", n=1 << 20, sfc=1, dt=0.004, theta=0.5, theta_mixed=0.25, mac_alpha=1.0e-3,
                     theta_plain_matched=0.05, train_steps=20, train_iters=1500, seed=3),
-    "cloud8m": dict(kind="cloud", n=1 << 23, sfc=1, dt=0.002, theta=0.6, theta_mixed=0.25, mac_alpha=1.2e-3,
+    "cloud8m": dict(kind="cloud", n=1 << 23, sfc=1, dt=0.002, theta=0.6, theta_mixed=0.25, mac_alpha=1.5e-3,
                     theta_plain_matched=0.05, train_steps=20, train_iters=1500, seed=3),
     # the reference's own single-rank case: N = 131072, Lebesgue, leapfrog dt 0.025
     "plummer131k": dict(kind="gravity", n=131072, sfc=0, dt=0.025, eps2=1e-4, theta=0.5, theta_mixed=0.28,
@@ -162,7 +164,8 @@ def make_sim(wl, state, variant):
                                   theta=wl["theta"] if variant == "plain" else wl["theta_plain_matched"],
                                   theta_mixed=wl["theta_mixed"], learned_h=1 if mixed else 0,
                                   gravity_mac=1 if (mixed and wl.get("mac_alpha")) else 0,
-                                  mac_alpha=wl.get("mac_alpha") or 0.003)
+                                  mac_alpha=wl.get("mac_alpha") or 0.003,
+                                  mac_quad_alpha=wl.get("mac_quad_alpha", 0.0) if mixed else 0.0)
         return Miluphpc(cfg, state, materials=[material(interactions=60, alpha=1.0, beta=2.0, eos_type=0,
                                                         K=state["cs2"], gamma=1.0)])
     kw = dict(gravity=1, sph=0, integrator=2, time_step=wl["dt"], smoothing=wl["eps2"], sfc=wl["sfc"],
@@ -180,10 +183,11 @@ def make_sim(wl, state, variant):
     return Miluphpc(cfg, state)
 
 
-def force_error(sim, torch, eps2, ntarget=4096, seed=7, h_factor=0.0):
+def force_error(sim, torch, eps2, ntarget=4096, seed=7, h_factor=0.0, h=None):
     """Relative error of the walk's accelerations against FP64 direct summation
     on a seeded sample of targets, with the walk's softening rule (eps2 plus,
-    with h_factor, (h_factor h_i)^2 of the target)."""
+    with h_factor, (h_factor h_i)^2 of the target, h_i the smoothing length
+    the walk used: `h`, default the current one)."""
     from miluphpc_b200.miluphpc import direct_gravity
     n = sim.n
     rng = np.random.default_rng(seed)
@@ -191,7 +195,8 @@ def force_error(sim, torch, eps2, ntarget=4096, seed=7, h_factor=0.0):
     tgt = torch.as_tensor(tg, device=sim.device)
     e2t = None
     if h_factor > 0.0:
-        e2t = (h_factor * sim.t["sml"][:n][tgt.long()]) ** 2
+        hh = h if h is not None else sim.t["sml"][:n]
+        e2t = (h_factor * hh[tgt.long()]) ** 2
     dx, dy, dz = direct_gravity(sim.t["x"][:n], sim.t["y"][:n], sim.t["z"][:n], sim.t["mass"][:n], tgt, eps2,
                                 eps2_targets=e2t)
     g = [sim.t[k][:n][tgt.long()] for k in ("g_ax", "g_ay", "g_az")]
@@ -273,8 +278,11 @@ def run_ours(args, wl):
     elif wl["kind"] == "cloud":
         # explicit Euler moves the particles after its RHS: one more (untimed)
         # RHS makes the accelerations those of the current positions
+        # (the walk runs before the smoothing-length update of the same RHS:
+        # its softening uses the h the RHS started from)
+        h_walk = sim.t["sml"][:n].clone()
         sim.rhs(step)
-        ferr = force_error(sim, torch, 0.0, h_factor=0.5)
+        ferr = force_error(sim, torch, 0.0, h_factor=0.5, h=h_walk)
     learned = None
     if wl["kind"] == "cloud":
         learned = {"training": train_info, "target_band": "60 +- 5 (|n - 60| < 5)",

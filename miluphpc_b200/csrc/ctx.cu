@@ -178,8 +178,8 @@ int stage_tree(mhpc_ctx* c, const mhpc_particles* p) {
     TRY(tree_build(c->T, c->skey, c->scan_scratch, c->st, s));
     record(c, EV_TREE);
     const int want_quad = c->cfg.gravity && c->cfg.precision >= 1;
-    TRY(tree_upward(c->T, c->sx, c->sy, c->sz, c->sm, want_quad, c->cfg.sph ? 1 : 0, c->st, s));
-    if (want_quad) TRY(tree_mixed_nodes(c->T, c->ord, c->cfg.theta_mixed, c->st, s));
+    TRY(tree_upward(c->T, c->sx, c->sy, c->sz, c->sm, want_quad, c->cfg.sph ? 1 : 0, c->ord, c->cfg.theta_mixed,
+                    c->st, s));
     record(c, EV_COM);
     return MHPC_OK;
 }

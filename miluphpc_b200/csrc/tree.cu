@@ -239,11 +239,34 @@ __device__ __forceinline__ Kids cell_kids(const TreeDev& T, int p) {
     return K;
 }
 
+// Mixed-path walk record of one node (layout in tree.cuh): FP32 hi/lo split
+// of the centre of mass, the geometric opening criterion edge^2/theta (-1 for
+// leaves), the quadrupole, the link info with the child mask, and M l^3.
+__device__ __forceinline__ void put_wrec(const TreeDev& T, int i, double x, double y, double z, double m, int info,
+                                         int mask, float4 q0, float2 q1, double edge0, double inv_theta) {
+    const float hx = (float)x, hy = (float)y, hz = (float)z;
+    float crit = -1.f, ml3 = 0.f;
+    if (!(info & ND_LEAF)) {
+        const double e = ldexp(edge0, -(info & 0xff));
+        crit = (float)(e * e * inv_theta);
+        ml3 = (float)(m * e * e * e);
+    }
+    float4* w = T.wrec + 4 * (size_t)i;
+    w[0] = make_float4(hx, hy, hz, (float)m);
+    w[1] = make_float4((float)(x - (double)hx), (float)(y - (double)hy), (float)(z - (double)hz), crit);
+    w[2] = q0;
+    w[3] = make_float4(q1.x, q1.y, __int_as_float((info & 0x1ff) | (mask << 9)), ml3);
+}
+
+// Leaves: centre of mass = the particle; with want_quad (mixed walk) the walk
+// record as well (a leaf's quadrupole is zero and never read from quad0/1).
 __global__ void __launch_bounds__(256) k_upward_leaves(TreeDev T, const double* __restrict__ sx,
                                                        const double* __restrict__ sy, const double* __restrict__ sz,
                                                        const double* __restrict__ sm, int want_quad,
-                                                       int want_box, const DevStatus* st) {
+                                                       int want_box, const long long* __restrict__ ord,
+                                                       double inv_theta, const DevStatus* st) {
     if (st->code) return;
+    const double edge0 = want_quad ? ord_to_dbl(ord[1]) - ord_to_dbl(ord[0]) : 0.0;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < T.n; a += gridDim.x * blockDim.x) {
         const int leaf = T.leaf_node[a];
         const double px = __ldg(sx + a), py = __ldg(sy + a), pz = __ldg(sz + a), pm = __ldg(sm + a);
@@ -252,10 +275,9 @@ __global__ void __launch_bounds__(256) k_upward_leaves(TreeDev T, const double* 
             T.bmin[leaf] = make_float4(rd(px), rd(py), rd(pz), 0.f);
             T.bmax[leaf] = make_float4(ru(px), ru(py), ru(pz), 0.f);
         }
-        if (want_quad) {
-            T.quad0[leaf] = make_float4(0.f, 0.f, 0.f, 0.f);
-            T.quad1[leaf] = make_float2(0.f, 0.f);
-        }
+        if (want_quad)
+            put_wrec(T, leaf, px, py, pz, pm, __ldg(&T.link[leaf].y), 0, make_float4(0.f, 0.f, 0.f, 0.f),
+                     make_float2(0.f, 0.f), edge0, inv_theta);
     }
 }
 
@@ -264,8 +286,10 @@ __global__ void __launch_bounds__(256) k_upward_leaves(TreeDev T, const double* 
 // mass use explicitly rounded products and sums in slot order, so the result
 // is bit-identical to the level-wise sums of the reference.
 __global__ void __launch_bounds__(256) k_upward_level(TreeDev T, int L, int want_quad, int want_box,
+                                                      const long long* __restrict__ ord, double inv_theta,
                                                       const DevStatus* st) {
     if (st->code) return;
+    const double edge0 = want_quad ? ord_to_dbl(ord[1]) - ord_to_dbl(ord[0]) : 0.0;
     const int i0 = T.level_off[L], i1 = min(T.level_off[L + 1], T.cap_nodes);
     for (int i = i0 + blockIdx.x * blockDim.x + threadIdx.x; i < i1; i += gridDim.x * blockDim.x) {
         const int p = T.level_cells[i];
@@ -285,7 +309,8 @@ __global__ void __launch_bounds__(256) k_upward_level(TreeDev T, int L, int want
                 hi.x = fmaxf(hi.x, bh.x); hi.y = fmaxf(hi.y, bh.y); hi.z = fmaxf(hi.z, bh.z);
             }
         };
-        const int end = __ldg(&T.link[p].x);
+        const int2 lkp = __ldg(&T.link[p]);
+        const int end = lkp.x;
         if (K.mask & 0x100) {
             for (int c = p + 1; c < end; c = __ldg(&T.link[c].x)) add_com(c);
         } else {
@@ -329,8 +354,11 @@ __global__ void __launch_bounds__(256) k_upward_level(TreeDev T, int L, int want
                 for (int d = 0; d < 8; ++d)
                     if ((K.mask >> d) & 1) add_quad(K.id[d]);
             }
-            T.quad0[p] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
-            T.quad1[p] = make_float2((float)q[4], (float)q[5]);
+            const float4 q0 = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+            const float2 q1 = make_float2((float)q[4], (float)q[5]);
+            T.quad0[p] = q0;
+            T.quad1[p] = q1;
+            put_wrec(T, p, mx, my, mz, m, lkp.y, K.mask, q0, q1, edge0, inv_theta);
         }
     }
 }
@@ -362,38 +390,6 @@ __global__ void __launch_bounds__(256) k_hmax_level(TreeDev T, int L, const DevS
     }
 }
 
-__global__ void __launch_bounds__(256) k_mixed_nodes(TreeDev T, const long long* ord, double inv_theta,
-                                                     const DevStatus* st) {
-    if (st->code) return;
-    const double edge0 = ord_to_dbl(ord[1]) - ord_to_dbl(ord[0]);
-    int total = *T.nodes;
-    if (total > T.cap_nodes) total = T.cap_nodes;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-        const double4 c = T.com[i];
-        const int info = T.link[i].y;
-        const float hx = (float)c.x, hy = (float)c.y, hz = (float)c.z;
-        float crit = -1.f;
-        if (!(info & ND_LEAF)) {
-            const double e = ldexp(edge0, -(info & 0xff));
-            crit = (float)(e * e * inv_theta);
-        }
-        float4 q0 = make_float4(0.f, 0.f, 0.f, 0.f);
-        float2 q1 = make_float2(0.f, 0.f);
-        int mask = 0;
-        float ml3 = 0.f;
-        if (!(info & ND_LEAF)) {
-            q0 = T.quad0[i]; q1 = T.quad1[i]; mask = T.kmask[i];
-            const double e = ldexp(edge0, -(info & 0xff));
-            ml3 = (float)(c.w * e * e * e);
-        }
-        float4* w = T.wrec + 4 * (size_t)i;
-        w[0] = make_float4(hx, hy, hz, (float)c.w);
-        w[1] = make_float4((float)(c.x - (double)hx), (float)(c.y - (double)hy), (float)(c.z - (double)hz), crit);
-        w[2] = q0;
-        w[3] = make_float4(q1.x, q1.y, __int_as_float((info & 0x1ff) | (mask << 9)), ml3);
-    }
-}
-
 }  // namespace
 
 int tree_build(TreeDev& T, const uint64_t* skey, void* scan_scratch, DevStatus* st, cudaStream_t s) {
@@ -418,10 +414,13 @@ int tree_build(TreeDev& T, const uint64_t* skey, void* scan_scratch, DevStatus* 
 }
 
 int tree_upward(TreeDev& T, const double* sx, const double* sy, const double* sz, const double* sm,
-                int want_quad, int want_box, DevStatus* st, cudaStream_t s) {
-    k_upward_leaves<<<grid_for(T.n, 256, 148 * 16), 256, 0, s>>>(T, sx, sy, sz, sm, want_quad, want_box, st);
+                int want_quad, int want_box, const long long* ord, double theta, DevStatus* st, cudaStream_t s) {
+    const double inv_theta = want_quad ? 1.0 / theta : 0.0;
+    k_upward_leaves<<<grid_for(T.n, 256, 148 * 16), 256, 0, s>>>(T, sx, sy, sz, sm, want_quad, want_box, ord,
+                                                                  inv_theta, st);
     const int gl = grid_for(T.n / 2 + 1, 256, 148 * 16);
-    for (int L = MHPC_MAX_LEVEL; L >= 1; --L) k_upward_level<<<gl, 256, 0, s>>>(T, L, want_quad, want_box, st);
+    for (int L = MHPC_MAX_LEVEL; L >= 1; --L)
+        k_upward_level<<<gl, 256, 0, s>>>(T, L, want_quad, want_box, ord, inv_theta, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }
@@ -434,8 +433,3 @@ int tree_node_hmax(const TreeDev& T, const double* h, const DevStatus* st, cudaS
     return MHPC_OK;
 }
 
-int tree_mixed_nodes(TreeDev& T, const long long* ord, double theta, const DevStatus* st, cudaStream_t s) {
-    k_mixed_nodes<<<148 * 8, 256, 0, s>>>(T, ord, 1.0 / theta, st);
-    CUDA_TRY(cudaGetLastError());
-    return MHPC_OK;
-}

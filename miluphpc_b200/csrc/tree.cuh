@@ -50,10 +50,11 @@ struct TreeDev {
 };
 
 int tree_build(TreeDev& T, const uint64_t* skey, void* scan_scratch, DevStatus* st, cudaStream_t s);
-// Centres of mass (FP64), quadrupoles (want_quad) and particle bounding boxes
+// Centres of mass (FP64), quadrupoles and walk records (want_quad, mixed
+// walk: every node's wrec, whose geometric criterion uses theta and the root
+// edge from the device bounding box `ord`) and particle bounding boxes
 // (want_box, used by the neighbour search) of every cell, level by level.
 int tree_upward(TreeDev& T, const double* sx, const double* sy, const double* sz, const double* sm,
-                int want_quad, int want_box, DevStatus* st, cudaStream_t s);
+                int want_quad, int want_box, const long long* ord, double theta, DevStatus* st, cudaStream_t s);
 // T.hmax[node] = max h over the node's particles (h sorted, n entries).
 int tree_node_hmax(const TreeDev& T, const double* h, const DevStatus* st, cudaStream_t s);
-int tree_mixed_nodes(TreeDev& T, const long long* ord, double theta, const DevStatus* st, cudaStream_t s);
