@@ -41,6 +41,8 @@ struct mhpc_ctx {
     double *sx = nullptr, *sy = nullptr, *sz = nullptr, *sm = nullptr, *sh = nullptr;
     double *svx = nullptr, *svy = nullptr, *svz = nullptr, *se = nullptr, *srho = nullptr, *sp = nullptr,
            *scs = nullptr, *sbal = nullptr;
+    float4 *sf0 = nullptr, *sf1 = nullptr, *sf2 = nullptr;  // FP32 pair-sum views (mixed SPH)
+    float2* sf3 = nullptr;
     int* smat = nullptr;
     TreeDev T;
     int* nbr = nullptr;
@@ -246,6 +248,7 @@ int stage_sph(mhpc_ctx* c, const mhpc_particles* p) {
     S.vx = c->svx; S.vy = c->svy; S.vz = c->svz; S.e = c->se;
     S.mat = p->material_id ? c->smat : nullptr;
     S.rho = c->srho; S.p = c->sp; S.cs = c->scs; S.bal = c->sbal;
+    S.f0 = c->sf0; S.f1 = c->sf1; S.f2 = c->sf2; S.f3 = c->sf3;
     TRY(sph_frnn(c->T, P, S, c->nbr, c->noi, c->st, s));
     record(c, EV_FRNN);
     TRY(sph_density_eos(P, S, c->nbr, c->noi, c->perm, p->rho, p->p, p->cs, c->st, s));
@@ -405,6 +408,7 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
     if (cfg->sph) {
         A(c->svx, n); A(c->svy, n); A(c->svz, n); A(c->se, n); A(c->srho, n); A(c->sp, n); A(c->scs, n);
         A(c->sbal, n);
+        A(c->sf0, n); A(c->sf1, n); A(c->sf2, n); A(c->sf3, n);
         A(c->smat, n);
         size_t groups = (n + 31) / 32;
         A(c->nbr, groups * 32 * (size_t)c->maxnb);

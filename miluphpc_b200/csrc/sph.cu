@@ -69,6 +69,63 @@ __device__ __forceinline__ void skernel(int type, double r, double h, double& W,
     }
 }
 
+// FP32 forms of the same kernels for the mixed-precision pair sums (one
+// reciprocal of h, the rest products).
+__device__ __forceinline__ void skernel_f(int type, float r, float h, float& W, float& dWdr) {
+    const float ih = __frcp_rn(h);
+    const float q = r * ih, ih3 = ih * ih * ih, ih4 = ih3 * ih;
+    constexpr float kPi = 3.14159265358979f;
+    W = 0.f;
+    dWdr = 0.f;
+    switch (type) {
+        case 0: {
+            if (q <= 1.f && q >= 0.f) {
+                const float a = 1.f - q;
+                W = 15.f / kPi * ih3 * a * a * a;
+                dWdr = -45.f / kPi * ih4 * a * a;
+            }
+        } break;
+        case 1: {
+            const float f = 8.f / kPi * ih3;
+            if (q > 1.f) {
+            } else if (q > 0.5f) {
+                const float a = 1.f - q;
+                W = 2.f * f * a * a * a;
+                dWdr = -6.f * f * ih * a * a;
+            } else {
+                W = f * (6.f * q * q * q - 6.f * q * q + 1.f);
+                dWdr = 6.f * f * ih * (3.f * q * q - 2.f * q);
+            }
+        } break;
+        case 2: {
+            if (q < 1.f) {
+                const float a = 1.f - q;
+                W = 21.f / (2.f * kPi) * ih3 * a * a * a * a * (1.f + 4.f * q);
+                dWdr = -210.f / kPi * ih4 * q * a * a * a;
+            }
+        } break;
+        case 3: {
+            if (q < 1.f) {
+                const float a = 1.f - q, a5 = a * a * a * a * a;
+                W = 495.f / (32.f * kPi) * ih3 * a5 * a * (1.f + 6.f * q + 35.f / 3.f * q * q);
+                dWdr = -1485.f / (16.f * kPi) * ih4 * a5 * (1.f - 35.f * q * q + 105.f * q * q * q);
+            }
+        } break;
+        default: {
+            if (q < 1.f) {
+                const float a = 1.f - q, a7 = a * a * a * a * a * a * a;
+                W = 1365.f / (64.f * kPi) * ih3 * a7 * a * (1.f + 8.f * q + 25.f * q * q + 32.f * q * q * q);
+                dWdr = -15015.f / (32.f * kPi) * ih4 * q * a7 * (1.f + 7.f * q + 16.f * q * q);
+            }
+        } break;
+    }
+}
+
+// FP32 difference of two positions held as FP32 hi/lo splits of FP64 values
+__device__ __forceinline__ float3 rel_f(const float4& ah, const float4& al, const float4& bh, const float4& bl) {
+    return make_float3((ah.x - bh.x) + (al.x - bl.x), (ah.y - bh.y) + (al.y - bl.y), (ah.z - bh.z) + (al.z - bl.z));
+}
+
 __device__ __forceinline__ double d2_exact(double dx, double dy, double dz) {
     return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
 }
@@ -367,54 +424,150 @@ __global__ void __launch_bounds__(kBlock) k_frnn(TreeDev T, int n, int maxnb, co
     }
 }
 
-// Per-lane count walk for sparse lists (later variable-h sweeps, where the
-// particles still iterating are scattered and a shared group box would be
-// large): every lane walks the tree for its own particle, pruning nodes whose
-// box does not come within h_i of it or whose largest h_j cannot reach it;
-// the particles of overlapping leaves and small cells are tested in a loop.
-__global__ void __launch_bounds__(kBlock) k_count_lane(TreeDev T, const double* __restrict__ sx,
-                                                       const double* __restrict__ sy, const double* __restrict__ sz,
-                                                       const double* __restrict__ sh, const int* __restrict__ list,
-                                                       const int* __restrict__ list_count,
-                                                       const float* __restrict__ node_hmax, int* __restrict__ count,
-                                                       DevStatus* st) {
+// Count walk for sparse lists (later variable-h sweeps, where the particles
+// still iterating are scattered, so a shared group box would be large): 8
+// lanes per particle, 4 particles per warp.  Each particle has its own stack
+// in shared memory; every step its 8 lanes pop up to 8 nodes, prune those
+// whose box does not come within h_i of the particle or whose largest h_j
+// cannot reach it, push the children of the others, and test the particles
+// of overlapping leaves, small cells and shared-key buckets 8 at a time.
+// Same stack bound as the group walk (a pop of k nodes pushes at most 8k).
+constexpr int kSubStack = 256;
+constexpr int kSubReserve = 7 * 22 + 8;
+
+__global__ void __launch_bounds__(kBlock) k_count_sub(TreeDev T, const double* __restrict__ sx,
+                                                      const double* __restrict__ sy, const double* __restrict__ sz,
+                                                      const double* __restrict__ sh, const int* __restrict__ list,
+                                                      const int* __restrict__ list_count,
+                                                      const float* __restrict__ node_hmax, int* __restrict__ count,
+                                                      DevStatus* st) {
+    __shared__ int stk[kWarps][4][kSubStack];
+    __shared__ int rfs[kWarps][4][8], rends[kWarps][4][8];
     if (st->code) return;
     const int M = *T.nodes;
-    const long q = (long)blockIdx.x * kBlock + threadIdx.x;
-    if (q >= *list_count) return;
-    const int s = list[q];
-    const double px = sx[s], py = sy[s], pz = sz[s], hi = sh[s], hi2 = hi * hi;
-    const float lx = __double2float_rd(px - hi), ly = __double2float_rd(py - hi), lz = __double2float_rd(pz - hi);
-    const float ux = __double2float_ru(px + hi), uy = __double2float_ru(py + hi), uz = __double2float_ru(pz + hi);
-    const float fx0 = __double2float_rd(px), fy0 = __double2float_rd(py), fz0 = __double2float_rd(pz);
-    const float fx1 = __double2float_ru(px), fy1 = __double2float_ru(py), fz1 = __double2float_ru(pz);
-    int k = 0;
-    int nd = 0;
-    while (nd < M) {
-        const int2 lk = __ldg(T.link + nd);
-        const float4 bl = __ldg(T.bmin + nd), bh = __ldg(T.bmax + nd);
-        const float hn = __ldg(node_hmax + nd);
-        const int f = __ldg(T.first + nd), l = __ldg(T.last + nd);
-        const bool overlap = !(bh.x < lx || bl.x > ux || bh.y < ly || bl.y > uy || bh.z < lz || bl.z > uz) &&
-                             !(__fadd_ru(bh.x, hn) < fx0 || __fadd_rd(bl.x, -hn) > fx1 || __fadd_ru(bh.y, hn) < fy0 ||
-                               __fadd_rd(bl.y, -hn) > fy1 || __fadd_ru(bh.z, hn) < fz0 || __fadd_rd(bl.z, -hn) > fz1);
-        if (!overlap) { nd = lk.x; continue; }
-        if ((lk.y & ND_LEAF) || l - f + 1 <= kSmall) {
-            // a leaf or a small cell: test its particles directly (independent
-            // loads instead of one dependent node visit per particle)
-#pragma unroll 4
-            for (int j = f; j <= l; ++j) {
-                const double dx = px - __ldg(sx + j), dy = py - __ldg(sy + j), dz = pz - __ldg(sz + j);
-                const double d = d2_exact(dx, dy, dz);
-                const double hj = __ldg(sh + j);
-                k += (j != s && d < hi2 && d < hj * hj);
-            }
-            nd = lk.x;
-        } else {
-            ++nd;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, sg = lane >> 3, r = lane & 7;
+    const unsigned seg = 0xffu << (8 * sg);
+    const unsigned lt = (1u << lane) - 1u;
+    const long cnt = *list_count;
+    const long nwarps = (long)gridDim.x * kWarps;
+    // warp-stride loop over groups of 4 list entries (the grid does not
+    // depend on the list length, which only the device knows)
+    for (long gw = ((long)blockIdx.x * kBlock + threadIdx.x) >> 5; gw * 4 < cnt; gw += nwarps) {
+        const long q = gw * 4 + sg;
+        const bool valid = q < cnt;
+        const int s = valid ? list[q] : 0;
+        const double px = sx[s], py = sy[s], pz = sz[s], hi = sh[s], hi2 = hi * hi;
+        const float lx = __double2float_rd(px - hi), ly = __double2float_rd(py - hi), lz = __double2float_rd(pz - hi);
+        const float ux = __double2float_ru(px + hi), uy = __double2float_ru(py + hi), uz = __double2float_ru(pz + hi);
+        const float fx0 = __double2float_rd(px), fy0 = __double2float_rd(py), fz0 = __double2float_rd(pz);
+        const float fx1 = __double2float_ru(px), fy1 = __double2float_ru(py), fz1 = __double2float_ru(pz);
+        int* S = stk[w][sg];
+        int* RF = rfs[w][sg];
+        int* RE = rends[w][sg];
+        // the root's children: node 0 and its skip chain
+        int top = 0;
+        if (valid && r == 0) {
+            int c = 0;
+            while (c < M && top < 8) { S[top++] = c; c = __ldg(&T.link[c].x); }
+            if (c < M) set_status(st, MHPC_ERR_DEPTH, 5);
         }
+        top = __shfl_sync(MHPC_FULL, top, lane & ~7);
+        __syncwarp();
+        int k = 0;
+        while (__any_sync(MHPC_FULL, top > 0)) {
+            const int room = (kSubStack - kSubReserve - top) / 7;
+            int kk = top < 8 ? top : 8;
+            if (kk > room) kk = room > 1 ? room : 1;
+            if (top == 0) kk = 0;
+            const bool act = r < kk;
+            const int nd = act ? S[top - 1 - r] : 0;
+            __syncwarp();
+            top -= kk;
+            int rf = 0, rlen = 0, kmask = 0;
+            if (act) {
+                const int2 lk = __ldg(T.link + nd);
+                const float4 bl = __ldg(T.bmin + nd), bh = __ldg(T.bmax + nd);
+                const float hn = __ldg(node_hmax + nd);
+                const bool overlap =
+                    !(bh.x < lx || bl.x > ux || bh.y < ly || bl.y > uy || bh.z < lz || bl.z > uz) &&
+                    !(__fadd_ru(bh.x, hn) < fx0 || __fadd_rd(bl.x, -hn) > fx1 || __fadd_ru(bh.y, hn) < fy0 ||
+                      __fadd_rd(bl.y, -hn) > fy1 || __fadd_ru(bh.z, hn) < fz0 || __fadd_rd(bl.z, -hn) > fz1);
+                if (overlap) {
+                    rf = __ldg(T.first + nd);
+                    if (lk.y & ND_LEAF) {
+                        rlen = 1;
+                    } else {
+                        const int l = __ldg(T.last + nd);
+                        const int km = __ldg(T.kmask + nd);
+                        if (l - rf + 1 <= kSmall || (km & 0x100)) rlen = l - rf + 1;
+                        else kmask = km & 0xff;
+                    }
+                }
+            }
+            // push children (scan within the 8-lane segment)
+            const int nkid = __popc(kmask);
+            int incl = nkid;
+    #pragma unroll
+            for (int o = 1; o < 8; o <<= 1) {
+                const int v = __shfl_up_sync(MHPC_FULL, incl, o, 8);
+                if (r >= o) incl += v;
+            }
+            const int total = __shfl_sync(MHPC_FULL, incl, 7, 8);
+            const bool over = top + total > kSubStack;  // unreachable by the bound on kk
+            if (over && r == 0 && valid) set_status(st, MHPC_ERR_DEPTH, 6);
+            if (nkid && !over) {
+                const int4 k0 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)nd));
+                const int4 k1 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)nd) + 1);
+                const int all[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
+                int wpos = top + incl - nkid;
+    #pragma unroll
+                for (int d = 0; d < 8; ++d)
+                    if ((kmask >> d) & 1) S[wpos++] = all[d];
+            }
+            top = over ? 0 : top + total;
+            // staged ranges of this particle, with running ends
+            int rincl = rlen;
+    #pragma unroll
+            for (int o = 1; o < 8; o <<= 1) {
+                const int v = __shfl_up_sync(MHPC_FULL, rincl, o, 8);
+                if (r >= o) rincl += v;
+            }
+            const int ncand = __shfl_sync(MHPC_FULL, rincl, 7, 8);
+            const unsigned br = __ballot_sync(MHPC_FULL, rlen > 0) & seg;
+            const int nr = __popc(br);
+            if (rlen > 0) {
+                const int slot = __popc(br & lt);
+                RF[slot] = rf;
+                RE[slot] = rincl;
+            }
+            __syncwarp();
+            int maxc = ncand;
+            maxc = max(maxc, __shfl_xor_sync(MHPC_FULL, maxc, 8));
+            maxc = max(maxc, __shfl_xor_sync(MHPC_FULL, maxc, 16));
+            for (int c0 = 0; c0 < maxc; c0 += 8) {
+                const int c = c0 + r;
+                if (c < ncand) {
+                    int lo = 0, hr = nr - 1;
+                    while (lo < hr) {
+                        const int mid = (lo + hr) >> 1;
+                        if (RE[mid] > c) hr = mid;
+                        else lo = mid + 1;
+                    }
+                    const int j = RF[lo] + c - (lo ? RE[lo - 1] : 0);
+                    const double dx = px - __ldg(sx + j), dy = py - __ldg(sy + j), dz = pz - __ldg(sz + j);
+                    const double d = d2_exact(dx, dy, dz);
+                    const double hj = __ldg(sh + j);
+                    k += (j != s && d < hi2 && d < hj * hj);
+                }
+            }
+            __syncwarp();
+        }
+        k += __shfl_xor_sync(MHPC_FULL, k, 1);
+        k += __shfl_xor_sync(MHPC_FULL, k, 2);
+        k += __shfl_xor_sync(MHPC_FULL, k, 4);
+        if (valid && r == 0) count[s] = k;
+        __syncwarp();
     }
-    count[s] = k;
 }
 
 // ------------------------------------------------------- variable h update
@@ -617,6 +770,137 @@ __global__ void __launch_bounds__(kBlock) k_forces(SphParams P, SphSorted S, con
     if (dsmldt_o) dsmldt_o[o] = P.integrate_sml ? dh : 0.0;
 }
 
+// ----------------------------------------------- mixed precision (FP32 pairs)
+// Positions as FP32 hi/lo splits: x_hi = (float)x, x_lo = (float)(x - x_hi), so
+// that a neighbour difference (x_hi,i - x_hi,j) + (x_lo,i - x_lo,j) keeps FP32
+// relative accuracy of the difference itself at any distance from the origin.
+__global__ void k_pack_pos(SphSorted S, int n) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const double x = S.x[s], y = S.y[s], z = S.z[s];
+        const float hx = (float)x, hy = (float)y, hz = (float)z;
+        S.f0[s] = make_float4(hx, hy, hz, (float)S.h[s]);
+        S.f1[s] = make_float4((float)(x - (double)hx), (float)(y - (double)hy), (float)(z - (double)hz), (float)S.m[s]);
+    }
+}
+
+// EOS of one particle (calculateSoundSpeed, then calculatePressure, in the
+// reference's order: the ideal-gas sound speed uses the previous pressure)
+__device__ __forceinline__ void eos(const MatDev& M, double rho, double e, double& p, double& cs) {
+    switch (M.eos_type) {
+        case 0: cs = sqrt(M.K * pow(rho, M.gamma - 1.0)); break;
+        case 9: cs = sqrt(M.gamma * p / rho); break;
+        case 12: cs = 0.0; break;
+        default: break;
+    }
+    switch (M.eos_type) {
+        case 0: p = M.K * pow(rho, M.gamma); break;
+        case 1: p = (M.bulk / M.n_exp) * (pow(rho / M.rho0, M.n_exp) - 1.0); break;
+        case 3: p = 41255.407 * rho; break;
+        case 9: p = (M.gamma - 1) * rho * e; break;
+        case 12: p = cs * cs * rho; break;
+        default: break;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_density_eos_f32(SphParams P, SphSorted S, const int* __restrict__ nbr,
+                                                            const int* __restrict__ noi, const int* __restrict__ perm,
+                                                            double* rho_out, double* p_out, double* cs_out,
+                                                            DevStatus* st) {
+    if (st->code) return;
+    const long s = (long)blockIdx.x * kBlock + threadIdx.x;
+    if (s >= P.n) return;
+    double rho;
+    if (P.integrate_density) {
+        rho = S.rho[s];
+    } else {
+        const float4 a0 = S.f0[s], a1 = S.f1[s];
+        const float hi = a0.w;
+        float W, dWdr;
+        skernel_f(P.kernel, 0.f, hi, W, dWdr);
+        rho = (double)(a1.w * W);
+        const int k = min(noi[s], P.maxnb);
+        for (int q = 0; q < k; ++q) {
+            const int j = nbr[nb_index(s, q, P.maxnb)];
+            const float4 b0 = __ldg(S.f0 + j), b1 = __ldg(S.f1 + j);
+            const float3 d = rel_f(a0, a1, b0, b1);
+            const float r = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+            skernel_f(P.kernel, r, P.avg_h ? 0.5f * (hi + b0.w) : hi, W, dWdr);
+            rho += (double)(b1.w * W);
+        }
+        if (!(rho > 0.0)) set_status(st, MHPC_ERR_NAN, (int)s);
+    }
+    const int mid = S.mat ? S.mat[s] : 0;
+    double p = S.p[s], cs = S.cs[s];
+    eos(P.mat[mid], rho, S.e[s], p, cs);
+    S.rho[s] = rho;
+    S.p[s] = p;
+    S.cs[s] = cs;
+    S.f2[s] = make_float4((float)S.vx[s], (float)S.vy[s], (float)S.vz[s], (float)cs);
+    S.f3[s] = make_float2((float)rho, (float)(p / (rho * rho)));
+    const int o = perm[s];
+    rho_out[o] = rho;
+    p_out[o] = p;
+    cs_out[o] = cs;
+}
+
+__global__ void __launch_bounds__(kBlock) k_forces_f32(SphParams P, SphSorted S, const int* __restrict__ nbr,
+                                                       const int* __restrict__ noi, const int* __restrict__ perm,
+                                                       double* ax_o, double* ay_o, double* az_o, double* drhodt_o,
+                                                       double* dedt_o, double* dsmldt_o, DevStatus* st) {
+    if (st->code) return;
+    const long s = (long)blockIdx.x * kBlock + threadIdx.x;
+    if (s >= P.n) return;
+    const float4 a0 = S.f0[s], a1 = S.f1[s], v = S.f2[s];
+    const float2 rp = S.f3[s];
+    const float hi = a0.w, csi = v.w, rhoi = rp.x, pri = rp.y;
+    const int mid = S.mat ? S.mat[s] : 0;
+    const float alpha = (float)P.mat[mid].alpha, beta = (float)P.mat[mid].beta;
+    const float bali = P.balsara ? (float)S.bal[s] : 1.f;
+    double a0x = 0, a0y = 0, a0z = 0, drho = 0, de = 0, dh = 0;
+    const int k = min(noi[s], P.maxnb);
+    for (int q = 0; q < k; ++q) {
+        const int j = nbr[nb_index(s, q, P.maxnb)];
+        const float4 b0 = __ldg(S.f0 + j), b1 = __ldg(S.f1 + j), w = __ldg(S.f2 + j);
+        const float2 rpj = __ldg(S.f3 + j);
+        const float hj = b0.w, mj = b1.w, rhoj = rpj.x;
+        const float3 d = rel_f(a0, a1, b0, b1);
+        const float rr = d.x * d.x + d.y * d.y + d.z * d.z;
+        const float r = sqrtf(rr);
+        float W, dWdr;
+        skernel_f(P.kernel, r, P.avg_h ? 0.5f * (hi + hj) : hi, W, dWdr);
+        const float g = __fdividef(dWdr, r);
+        const float gx = g * d.x, gy = g * d.y, gz = g * d.z;
+        const float dvx = v.x - w.x, dvy = v.y - w.y, dvz = v.z - w.z;
+        const float vvnablaW = dvx * gx + dvy * gy + dvz * gz;
+        const float vr = dvx * d.x + dvy * d.y + dvz * d.z;
+        float pij = 0.f;
+        if (vr < 0.f) {
+            const float csbar = 0.5f * (csi + w.w);
+            const float smooth = 0.5f * (hi + hj);
+            float mu = __fdividef(smooth * vr, rr + smooth * smooth * 1e-2f);
+            if (P.balsara) mu *= 0.5f * (bali + (float)__ldg(S.bal + j));
+            pij = __fdividef((beta * mu - alpha * csbar) * mu, 0.5f * (rhoi + rhoj));
+        }
+        const float pf = -mj * (pri + rpj.y);
+        const float ajx = pf * gx, ajy = pf * gy, ajz = pf * gz;
+        const float vf = -mj * pij;
+        a0x += (double)(ajx + vf * gx);
+        a0y += (double)(ajy + vf * gy);
+        a0z += (double)(ajz + vf * gz);
+        const float mv = __fdividef(mj, rhoj) * vvnablaW;
+        drho += (double)(rhoi * mv);
+        if (P.integrate_sml) dh -= (double)(1.f / 3.f * hi * mv);
+        if (P.integrate_energy) de += (double)(0.5f * mj * pij * vvnablaW - 0.5f * (ajx * dvx + ajy * dvy + ajz * dvz));
+    }
+    const int o = perm[s];
+    ax_o[o] = a0x;
+    ay_o[o] = a0y;
+    az_o[o] = a0z;
+    if (drhodt_o) drhodt_o[o] = drho;
+    if (dedt_o) dedt_o[o] = P.integrate_energy ? de : 0.0;
+    if (dsmldt_o) dsmldt_o[o] = P.integrate_sml ? dh : 0.0;
+}
+
 __global__ void k_export_nnl(int n, int maxnb, const int* __restrict__ nbr, const int* __restrict__ noi,
                              const int* __restrict__ perm, int* nnl, int* noi_out) {
     for (long s = blockIdx.x * (long)blockDim.x + threadIdx.x; s < n; s += (long)gridDim.x * blockDim.x) {
@@ -671,9 +955,8 @@ int sph_variable_h(const TreeDev& T, const SphParams& P, const double* x, const 
             k_frnn<1><<<(int)blocks, kBlock, 0, s>>>(T, P.n, P.maxnb, x, y, z, B.hold, B.list, list_count, T.hmax,
                                                       nullptr, B.count, st);
         } else {
-            // later sweeps: the few particles still iterating, one walk per lane
-            k_count_lane<<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(T, x, y, z, B.hold, B.list, list_count,
-                                                                        T.hmax, B.count, st);
+            // later sweeps: the few particles still iterating, 8 lanes each
+            k_count_sub<<<148 * 16, kBlock, 0, s>>>(T, x, y, z, B.hold, B.list, list_count, T.hmax, B.count, st);
         }
         k_vh_update<<<g, 256, 0, s>>>(B.list, list_count, B.count, h, B.done, B.nit, target, tol, max_iter,
                                       P.maxnb);
@@ -689,6 +972,14 @@ int sph_variable_h(const TreeDev& T, const SphParams& P, const double* x, const 
 int sph_density_eos(const SphParams& P, const SphSorted& S, const int* nbr, const int* noi, const int* perm,
                     double* rho_out, double* p_out, double* cs_out, DevStatus* st, cudaStream_t s) {
     if (P.n <= 0) return MHPC_OK;
+    if (P.mixed) {
+        if (!S.f0 || !S.f1 || !S.f2 || !S.f3) return MHPC_ERR_ARG;
+        k_pack_pos<<<grid_for(P.n, 256, 148 * 8), 256, 0, s>>>(S, P.n);
+        k_density_eos_f32<<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(P, S, nbr, noi, perm, rho_out, p_out,
+                                                                        cs_out, st);
+        CUDA_TRY(cudaGetLastError());
+        return MHPC_OK;
+    }
     k_density_eos<<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(P, S, nbr, noi, perm, rho_out, p_out, cs_out, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
@@ -705,6 +996,13 @@ int sph_balsara(const SphParams& P, const SphSorted& S, const int* nbr, const in
 int sph_forces(const SphParams& P, const SphSorted& S, const int* nbr, const int* noi, const int* perm, double* ax,
                double* ay, double* az, double* drhodt, double* dedt, double* dsmldt, DevStatus* st, cudaStream_t s) {
     if (P.n <= 0) return MHPC_OK;
+    if (P.mixed) {
+        if (!S.f0 || !S.f1 || !S.f2 || !S.f3) return MHPC_ERR_ARG;
+        k_forces_f32<<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(P, S, nbr, noi, perm, ax, ay, az, drhodt, dedt,
+                                                                   dsmldt, st);
+        CUDA_TRY(cudaGetLastError());
+        return MHPC_OK;
+    }
     k_forces<<<(P.n + kBlock - 1) / kBlock, kBlock, 0, s>>>(P, S, nbr, noi, perm, ax, ay, az, drhodt, dedt, dsmldt,
                                                            st);
     CUDA_TRY(cudaGetLastError());

@@ -33,6 +33,11 @@ struct SphSorted {
     const int* mat;        // may be null
     double *rho, *p, *cs;  // sorted outputs of the density/EOS pass (p, cs hold previous values on entry)
     double* bal;           // sorted Balsara factors (written by sph_balsara, read by sph_forces)
+    // FP32 pair-sum views (mixed precision), written by sph_density_eos:
+    // f0 = (x_hi, y_hi, z_hi, h), f1 = (x_lo, y_lo, z_lo, m) with x = x_hi + x_lo
+    // (FP32 split of the FP64 position), f2 = (vx, vy, vz, c_s), f3 = (rho, p/rho^2)
+    float4 *f0, *f1, *f2;
+    float2* f3;
 };
 
 // Neighbour lists in sorted index space, group-transposed:
@@ -56,6 +61,9 @@ struct VhBuffers {
 int sph_variable_h(const TreeDev& T, const SphParams& P, const double* x, const double* y, const double* z,
                    double* h, const VhBuffers& B, int target, int tol, int max_iter, int sweeps, DevStatus* st,
                    cudaStream_t s);
+// Density (kernel sum over the lists) + EOS.  P.mixed: the pair sums in FP32 on
+// hi/lo-split relative positions with FP64 accumulation (and the FP32 views
+// of S filled for sph_forces); otherwise FP64 throughout.
 int sph_density_eos(const SphParams& P, const SphSorted& S, const int* nbr, const int* noi, const int* perm,
                     double* rho_out, double* p_out, double* cs_out, DevStatus* st, cudaStream_t s);
 // Balsara switch (SPH::Kernel::CalcDivvandCurlv, src/sph/kernel.cu:223-342, and
@@ -63,6 +71,8 @@ int sph_density_eos(const SphParams& P, const SphSorted& S, const int* nbr, cons
 // curl v from the neighbour lists, f_i into S.bal; after sph_density_eos.
 int sph_balsara(const SphParams& P, const SphSorted& S, const int* nbr, const int* noi, DevStatus* st,
                 cudaStream_t s);
+// Internal forces; P.mixed: pair terms in FP32 from the views sph_density_eos
+// filled, FP64 accumulation.
 int sph_forces(const SphParams& P, const SphSorted& S, const int* nbr, const int* noi, const int* perm,
                double* ax, double* ay, double* az, double* drhodt, double* dedt, double* dsmldt, DevStatus* st,
                cudaStream_t s);

@@ -354,6 +354,60 @@ def test_sph_sedov_matches_oracle(cuda):
     sim.close()
 
 
+@pytest.mark.parametrize("case", ["sedov", "cloud"])
+def test_sph_mixed_precision_pair_sums(case, cuda):
+    """FP32 pair sums (precision 1) against the FP64 oracle: density within a
+    relative 2e-6, accelerations and rates within 2e-5 of their largest
+    magnitude (FP32 pair terms, FP64 accumulation)."""
+    if case == "sedov":
+        S = _sedov_state(24)
+        cfg = sph_cfg(precision=1)
+        mat = material(interactions=60, alpha=1.0, beta=2.0, eos_type=9, gamma=5.0 / 3.0)
+        avg_h = False
+    else:
+        C = ics.rotating_cloud(20_000, seed=5)
+        S = dict(C)
+        n = len(S["x"])
+        S["sml"] = S["sml"] * np.random.default_rng(4).uniform(0.8, 1.25, n)
+        S["p"] = np.zeros(n)
+        S["cs"] = np.zeros(n)
+        S["e"] = np.zeros(n)
+        for k in ("vx", "vy", "vz"):
+            S[k] = S[k] + np.random.default_rng(5).normal(0.0, 0.05, n)
+        cfg = sph_cfg(precision=1, integrate_sml=1, integrate_energy=0, max_num_interactions=400)
+        mat = material(interactions=60, eos_type=0, K=C["cs2"], gamma=1.0)
+        avg_h = True
+    n = len(S["x"])
+    sim = Miluphpc(cfg, S, materials=[mat])
+    p_prev = np.zeros(n)
+    for call in range(2):
+        sim.rhs(call)
+        off, nbr = O.frnn(S["x"], S["y"], S["z"], S["sml"])
+        assert np.array_equal(sim.numpy("noi"), np.diff(off))
+        rho = O.density(S["x"], S["y"], S["z"], S["mass"], S["sml"], off, nbr, avg_h=avg_h)
+        np.testing.assert_allclose(sim.numpy("rho"), rho, rtol=2e-6)
+        if case == "sedov":
+            par = np.array([0.0, 5.0 / 3.0, 0.0, 0.0, 0.0])
+            p, cs = O.eos(9, par, rho, S["e"], p_prev)
+            alpha, beta = 1.0, 2.0
+        else:
+            par = np.array([float(C["cs2"]), 1.0, 0.0, 0.0, 0.0])
+            p, cs = O.eos(0, par, rho, S["e"], p_prev)
+            alpha, beta = 1.0, 2.0
+        np.testing.assert_allclose(sim.numpy("p"), p, rtol=1e-5, atol=1e-300)
+        np.testing.assert_allclose(sim.numpy("cs"), cs, rtol=1e-5, atol=1e-300)
+        ax, ay, az, drho, de, dh = O.forces(S["x"], S["y"], S["z"], S["vx"], S["vy"], S["vz"], S["mass"],
+                                            S["sml"], rho, p, cs, off, nbr, alpha, beta, avg_h=avg_h)
+        scale = np.abs(np.stack([ax, ay, az])).max()
+        for got, ref in ((sim.numpy("ax"), ax), (sim.numpy("ay"), ay), (sim.numpy("az"), az)):
+            np.testing.assert_allclose(got, ref, rtol=0, atol=2e-5 * scale)
+        np.testing.assert_allclose(sim.numpy("drhodt"), drho, rtol=0, atol=2e-5 * np.abs(drho).max())
+        if case == "sedov":
+            np.testing.assert_allclose(sim.numpy("dedt"), de, rtol=0, atol=2e-5 * np.abs(de).max())
+        p_prev = p
+    sim.close()
+
+
 def test_variable_h_matches_oracle(cuda):
     C = ics.rotating_cloud(20_000, seed=4)
     n = len(C["x"])
