@@ -221,6 +221,11 @@ def run_ours(args, wl):
     step = 0
     train_info = None
     warm = args.warmup
+    # total energy K + W before the first step (gravity-only workloads; W from
+    # mhpc_potential, the same tree potential at both ends)
+    e_start = None
+    if wl["kind"] == "gravity":
+        e_start = sim.diagnostics()["kinetic"] + sim.potential()
     if wl["kind"] == "cloud" and args.variant == "mixed":
         warm = max(warm, wl["train_steps"])
     for _ in range(warm):
@@ -276,6 +281,11 @@ def run_ours(args, wl):
     ms_max = float(t.item())
     value = n * world * args.steps / (ms_max / 1e3)
     last = sim.stats()
+    energy = None
+    if e_start is not None:
+        e_end = sim.diagnostics()["kinetic"] + sim.potential()
+        energy = {"E_start": e_start, "E_end": e_end, "rel_drift": (e_end - e_start) / abs(e_start),
+                  "steps": step, "potential": "tree walk, geometric rule theta_mixed, quadrupoles"}
     ferr = None
     if wl["kind"] == "gravity":
         ferr = force_error(sim, torch, wl["eps2"])
@@ -367,6 +377,7 @@ def run_ours(args, wl):
                 {"sph": "Sedov lattice", "cloud": "rotating cloud", "gravity": "Plummer"}[wl["kind"]]),
             "config": cfg_out,
             "force_error": ferr,
+            "energy": energy,
             "learned_h": learned,
             "stages_ms_mean": {k: round(v, 3) for k, v in stage_sum.items()},
             "tree_cells": last["cells"],

@@ -258,6 +258,16 @@ int mhpc_get_stats(mhpc_ctx* ctx, mhpc_stats* out);
  * angular momentum, out[8..10] centre of mass.  Synchronises. */
 int mhpc_diagnostics(mhpc_ctx* ctx, const mhpc_particles* p, double* out11);
 
+/* Gravitational potential phi_i (caller's order, into pot_dev when not NULL)
+ * and potential energy W = 1/2 sum m_i phi_i (into *energy_out when not NULL)
+ * of the particles' current positions: a tree build and the interaction-list
+ * walk with the geometric rule (theta_mixed) whatever the configured
+ * precision and opening rule, so that successive calls are comparable (energy
+ * drift).  The caller's accelerations are not touched.  Synchronises.  The
+ * reference has no potential on its path; this serves the energy diagnostics
+ * next to mhpc_diagnostics. */
+int mhpc_potential(mhpc_ctx* ctx, const mhpc_particles* p, double* pot_dev, double* energy_out);
+
 /* Miluphpc::removeParticles (src/miluphpc.cpp:3216-3348) with
  * ParticlesNS::Kernel::mark2remove (src/subdomain_key_tree/subdomain.cu:2161-2240):
  * removes the particles outside the region of config remove_particles_criterion

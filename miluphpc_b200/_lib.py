@@ -122,6 +122,7 @@ def load():
     L.mhpc_export_tree.argtypes = [c_void_p, c_int, P_i, P_i, P_d, P_d, P_d, P_d, P_i]
     L.mhpc_get_stats.argtypes = [c_void_p, ctypes.POINTER(Stats)]
     L.mhpc_diagnostics.argtypes = [c_void_p, ctypes.POINTER(Particles), P_d]
+    L.mhpc_potential.argtypes = [c_void_p, ctypes.POINTER(Particles), c_void_p, P_d]
     L.mhpc_remove_particles.argtypes = [c_void_p, ctypes.POINTER(Particles), P_i]
     L.mhpc_direct_gravity.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_double,
                                       c_void_p, c_void_p, c_void_p, c_void_p]
@@ -161,7 +162,7 @@ EXPORTS = [
     "mhpc_ctx_create", "mhpc_ctx_destroy", "mhpc_ctx_set_stream", "mhpc_ctx_set_config", "mhpc_rhs",
     "mhpc_rhs_async", "mhpc_ctx_status", "mhpc_integrate", "mhpc_integrate_host", "mhpc_stage_tree",
     "mhpc_stage_gravity", "mhpc_stage_sph", "mhpc_export_sorted", "mhpc_export_tree", "mhpc_get_stats",
-    "mhpc_diagnostics", "mhpc_direct_gravity", "mhpc_fp32_peak", "mhpc_mlp_reset", "mhpc_mlp_train", "mhpc_mlp_num_params",
+    "mhpc_diagnostics", "mhpc_potential", "mhpc_direct_gravity", "mhpc_fp32_peak", "mhpc_mlp_reset", "mhpc_mlp_train", "mhpc_mlp_num_params",
     "mhpc_mlp_forward_backward", "mhpc_mlp_get_params", "mhpc_mlp_set_params",
     "mhpc_remove_particles", "mhpc_direct_gravity_soft",
 ]

@@ -69,6 +69,10 @@ struct mhpc_ctx {
     // device mirror for mhpc_integrate_host
     mhpc_particles mirror;
     bool mirror_ready = false;
+    // mhpc_potential: the tree gets walk records whatever the precision; scratch
+    // for the potential and the walk's accelerations (allocated on first use)
+    bool force_wrec = false;
+    double* pot_scratch = nullptr;
     // mhpc_integrate_host, leapfrog: the drifted positions are copied out on
     // copy_stream while the right-hand side runs (pos_out = host x, y, z)
     cudaStream_t copy_stream = nullptr;
@@ -179,7 +183,7 @@ int stage_tree(mhpc_ctx* c, const mhpc_particles* p) {
     c->T.n = n;
     TRY(tree_build(c->T, c->skey, c->scan_scratch, c->st, s));
     record(c, EV_TREE);
-    const int want_quad = c->cfg.gravity && c->cfg.precision >= 1;
+    const int want_quad = c->cfg.gravity && (c->cfg.precision >= 1 || c->force_wrec);
     TRY(tree_upward(c->T, c->sx, c->sy, c->sz, c->sm, want_quad, c->cfg.sph ? 1 : 0, c->ord, c->cfg.theta_mixed,
                     c->st, s));
     record(c, EV_COM);
@@ -460,6 +464,7 @@ int mhpc_ctx_destroy(mhpc_ctx* c) {
         cudaStreamDestroy(c->copy_stream);
     }
     if (c->ev_drift) cudaEventDestroy(c->ev_drift);
+    if (c->pot_scratch) cudaFree(c->pot_scratch);
     if (c->mirror_ready) {
         double** ptrs[] = {&c->mirror.x, &c->mirror.y, &c->mirror.z, &c->mirror.mass, &c->mirror.vx, &c->mirror.vy,
                            &c->mirror.vz, &c->mirror.ax, &c->mirror.ay, &c->mirror.az, &c->mirror.g_ax,
@@ -831,6 +836,42 @@ int mhpc_diagnostics(mhpc_ctx* c, const mhpc_particles* p, double* out) {
     CUDA_TRY(cudaMemcpyAsync(out, c->diag_out, sizeof(double) * 11, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     return MHPC_OK;
+}
+
+int mhpc_potential(mhpc_ctx* c, const mhpc_particles* p, double* pot_dev, double* energy_out) {
+    if (!c || !p) return MHPC_ERR_ARG;
+    if (!c->cfg.gravity) return MHPC_ERR_CONFIG;
+    TRY(check_particles(c, p));
+    const int n = p->n;
+    if (n == 0) {
+        if (energy_out) *energy_out = 0.0;
+        return MHPC_OK;
+    }
+    cudaStream_t s = c->stream;
+    if (!c->pot_scratch) CUDA_TRY(cudaMalloc(&c->pot_scratch, sizeof(double) * 4 * (size_t)c->cap));
+    double* pot = pot_dev ? pot_dev : c->pot_scratch;
+    double* acc = c->pot_scratch + c->cap;  // accelerations of this walk (not the caller's g_a)
+    CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevStatus), s));
+    c->force_wrec = true;
+    const int rc = stage_tree(c, p);
+    c->force_wrec = false;
+    TRY(rc);
+    GravParams G;
+    std::memset(&G, 0, sizeof(G));
+    G.n = n;
+    G.eps2 = c->cfg.smoothing;
+    G.h_factor = (c->cfg.softening_mode == 1) ? c->cfg.softening_h_factor : 0.0;
+    G.G = c->cfg.si_units ? 6.67430e-11 : 1.0;
+    G.ord = c->ord;
+    G.theta = c->cfg.theta_mixed;  // geometric rule: the same opening rule at every call
+    G.pot = pot;
+    TRY(gravity_lists(c->T, G, c->sx, c->sy, c->sz, c->sh, c->perm, acc, acc + c->cap, acc + 2 * (size_t)c->cap,
+                      c->st, s));
+    if (energy_out) {
+        TRY(launch_potential_energy(n, p->mass, pot, c->diag_part, c->diag_out, s));
+        CUDA_TRY(cudaMemcpyAsync(energy_out, c->diag_out, sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    return read_status(c);
 }
 
 int mhpc_direct_gravity(const double* x, const double* y, const double* z, const double* m, int n, const int* targets,

@@ -290,11 +290,13 @@ struct ListSmem {
 // kGuard: some softened distance may be 0 (eps2 = 0), so 1/r is guarded; with
 // eps2 >= 1e-20 every r^2 >= eps2 keeps 1/r^3 finite and the guard is dropped
 // (it costs 11 % of the walk's instructions).
-template <bool kGuard>
+// kPot: also the potential, -(m/r + RQR/(2 r^5)) per cell and -m/r per leaf,
+// leaving out the particle's own leaf (R = 0 exactly).
+template <bool kGuard, bool kPot>
 __device__ __forceinline__ void eval_cells(const ListSmem& S, int count, const float (&rx)[2], const float (&ry)[2],
                                            const float (&rz)[2], const float (&e2)[2], double (&ax)[2],
-                                           double (&ay)[2], double (&az)[2]) {
-    float fx[2] = {0.f, 0.f}, fy[2] = {0.f, 0.f}, fz[2] = {0.f, 0.f};
+                                           double (&ay)[2], double (&az)[2], double (&ph)[2]) {
+    float fx[2] = {0.f, 0.f}, fy[2] = {0.f, 0.f}, fz[2] = {0.f, 0.f}, fp[2] = {0.f, 0.f};
 #pragma unroll 4
     for (int e = 0; e < count; ++e) {
         const float4 c = S.cpos[e];
@@ -317,17 +319,21 @@ __device__ __forceinline__ void eval_cells(const ListSmem& S, int count, const f
             fx[k] = fmaf(cc, Rx, fmaf(qx, ri5, fx[k]));
             fy[k] = fmaf(cc, Ry, fmaf(qy, ri5, fy[k]));
             fz[k] = fmaf(cc, Rz, fmaf(qz, ri5, fz[k]));
+            if (kPot) fp[k] -= fmaf(c.w, ri, 0.5f * rqr * ri5);
         }
     }
 #pragma unroll
-    for (int k = 0; k < 2; ++k) { ax[k] += fx[k]; ay[k] += fy[k]; az[k] += fz[k]; }
+    for (int k = 0; k < 2; ++k) {
+        ax[k] += fx[k]; ay[k] += fy[k]; az[k] += fz[k];
+        if (kPot) ph[k] += fp[k];
+    }
 }
 
-template <bool kGuard>
+template <bool kGuard, bool kPot>
 __device__ __forceinline__ void eval_leaves(const ListSmem& S, int count, const float (&rx)[2], const float (&ry)[2],
                                             const float (&rz)[2], const float (&e2)[2], double (&ax)[2],
-                                            double (&ay)[2], double (&az)[2]) {
-    float fx[2] = {0.f, 0.f}, fy[2] = {0.f, 0.f}, fz[2] = {0.f, 0.f};
+                                            double (&ay)[2], double (&az)[2], double (&ph)[2]) {
+    float fx[2] = {0.f, 0.f}, fy[2] = {0.f, 0.f}, fz[2] = {0.f, 0.f}, fp[2] = {0.f, 0.f};
 #pragma unroll 4
     for (int e = 0; e < count; ++e) {
         const float4 c = S.lpos[e];
@@ -340,15 +346,19 @@ __device__ __forceinline__ void eval_leaves(const ListSmem& S, int count, const 
             fx[k] = fmaf(-mri3, Rx, fx[k]);
             fy[k] = fmaf(-mri3, Ry, fy[k]);
             fz[k] = fmaf(-mri3, Rz, fz[k]);
+            if (kPot) fp[k] -= (Rx == 0.f && Ry == 0.f && Rz == 0.f) ? 0.f : c.w * ri;
         }
     }
 #pragma unroll
-    for (int k = 0; k < 2; ++k) { ax[k] += fx[k]; ay[k] += fy[k]; az[k] += fz[k]; }
+    for (int k = 0; k < 2; ++k) {
+        ax[k] += fx[k]; ay[k] += fy[k]; az[k] += fz[k];
+        if (kPot) ph[k] += fp[k];
+    }
 }
 
 constexpr int kListBlock = 128;
 
-template <bool kGuard, bool kRel>
+template <bool kGuard, bool kRel, bool kPot>
 __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams P, const double* __restrict__ sx,
                                                            const double* __restrict__ sy,
                                                            const double* __restrict__ sz,
@@ -442,7 +452,7 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
     }
     top = __shfl_sync(MHPC_FULL, top, 0);
     __syncwarp();
-    double ax[2] = {0.0, 0.0}, ay[2] = {0.0, 0.0}, az[2] = {0.0, 0.0};
+    double ax[2] = {0.0, 0.0}, ay[2] = {0.0, 0.0}, az[2] = {0.0, 0.0}, ph[2] = {0.0, 0.0};
     int ncell = 0, nleaf = 0;
     unsigned long long tested = 0, ncell_tot = 0, nleaf_tot = 0;
     while (top > 0) {
@@ -543,13 +553,13 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
         top += total;
         __syncwarp();
         if (ncell >= 32) {
-            eval_cells<kGuard>(S, ncell, rx, ry, rz, e2, ax, ay, az);
+            eval_cells<kGuard, kPot>(S, ncell, rx, ry, rz, e2, ax, ay, az, ph);
             ncell_tot += ncell;
             ncell = 0;
             __syncwarp();
         }
         if (nleaf >= 32) {
-            eval_leaves<kGuard>(S, nleaf, rx, ry, rz, e2, ax, ay, az);
+            eval_leaves<kGuard, kPot>(S, nleaf, rx, ry, rz, e2, ax, ay, az, ph);
             nleaf_tot += nleaf;
             nleaf = 0;
             __syncwarp();
@@ -575,7 +585,7 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
                 nleaf += __popc(ba);
                 __syncwarp();
                 if (nleaf >= 32) {
-                    eval_leaves<kGuard>(S, nleaf, rx, ry, rz, e2, ax, ay, az);
+                    eval_leaves<kGuard, kPot>(S, nleaf, rx, ry, rz, e2, ax, ay, az, ph);
                     nleaf_tot += nleaf;
                     nleaf = 0;
                     __syncwarp();
@@ -583,8 +593,8 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
             }
         }
     }
-    if (ncell) eval_cells<kGuard>(S, ncell, rx, ry, rz, e2, ax, ay, az);
-    if (nleaf) eval_leaves<kGuard>(S, nleaf, rx, ry, rz, e2, ax, ay, az);
+    if (ncell) eval_cells<kGuard, kPot>(S, ncell, rx, ry, rz, e2, ax, ay, az, ph);
+    if (nleaf) eval_leaves<kGuard, kPot>(S, nleaf, rx, ry, rz, e2, ax, ay, az, ph);
     ncell_tot += ncell;
     nleaf_tot += nleaf;
     unsigned nv = 0;
@@ -593,6 +603,7 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
         if (valid[k]) {
             const int o = __ldg(perm + s[k]);
             gax[o] = P.G * ax[k]; gay[o] = P.G * ay[k]; gaz[o] = P.G * az[k];
+            if (kPot) P.pot[o] = P.G * ph[k];
         }
         nv += __popc(__ballot_sync(MHPC_FULL, valid[k]));
     }
@@ -638,14 +649,21 @@ int gravity_lists(const TreeDev& T, const GravParams& P, const double* sx, const
     // the self-interaction has R = 0 and r^2 = eps2: 1/r^3 stays finite in
     // FP32 for eps2 >= 1e-20
     const bool guard = !(P.eps2 >= 1e-20), rel = P.rel_alpha > 0.0;
-    if (!guard && !rel)
-        k_grav_lists<false, false><<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st);
-    else if (!guard && rel)
-        k_grav_lists<false, true><<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st);
-    else if (guard && !rel)
-        k_grav_lists<true, false><<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st);
-    else
-        k_grav_lists<true, true><<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st);
+#define MHPC_LISTS(G_, R_, P_) \
+    k_grav_lists<G_, R_, P_><<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st)
+    if (P.pot) {
+        // potential (diagnostics): separate instantiations, the force walk stays as it is
+        if (!guard && !rel) MHPC_LISTS(false, false, true);
+        else if (!guard && rel) MHPC_LISTS(false, true, true);
+        else if (guard && !rel) MHPC_LISTS(true, false, true);
+        else MHPC_LISTS(true, true, true);
+    } else {
+        if (!guard && !rel) MHPC_LISTS(false, false, false);
+        else if (!guard && rel) MHPC_LISTS(false, true, false);
+        else if (guard && !rel) MHPC_LISTS(true, false, false);
+        else MHPC_LISTS(true, true, false);
+    }
+#undef MHPC_LISTS
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

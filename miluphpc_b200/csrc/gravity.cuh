@@ -11,6 +11,8 @@ struct GravParams {
     double rel_alpha;     // interaction-list walk: relative opening rule with this alpha (0 = off), reading
                           // the previous accelerations from the output arrays before overwriting them
     double quad_alpha;    // relative rule: accepted cells with M l^2 <= quad_alpha |a| d^4 enter as monopoles
+    double* pot;          // interaction-list walk: gravitational potential per particle (caller's order),
+                          // null = accelerations only
 };
 
 // Plain FP64 walk with the reference's computeForces_v2 semantics.

@@ -437,6 +437,40 @@ int launch_diagnostics(const mhpc_particles& p, int sph, double* part, double* o
 
 size_t diagnostics_scratch_doubles() { return 148 * 4 * kDiag + 16; }
 
+namespace {
+// W = 1/2 sum m_i phi_i: per-block partial sums, then one block adds them in
+// block order (deterministic)
+__global__ void __launch_bounds__(256) k_pot_part(int n, const double* __restrict__ m,
+                                                  const double* __restrict__ pot, double* part) {
+    double acc = 0.0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        acc += 0.5 * m[i] * pot[i];
+    __shared__ double sh[8];
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(MHPC_FULL, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double v = 0.0;
+        for (int q = 0; q < 8; ++q) v += sh[q];
+        part[blockIdx.x] = v;
+    }
+}
+
+__global__ void k_pot_final(int blocks, const double* part, double* out) {
+    double v = 0.0;
+    for (int b = 0; b < blocks; ++b) v += part[b];
+    out[0] = v;
+}
+}  // namespace
+
+int launch_potential_energy(int n, const double* m, const double* pot, double* part, double* out, cudaStream_t s) {
+    const int blocks = 148 * 4;
+    k_pot_part<<<blocks, 256, 0, s>>>(n, m, pot, part);
+    k_pot_final<<<1, 1, 0, s>>>(blocks, part, out);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
 int launch_direct(const double* x, const double* y, const double* z, const double* m, int n, const int* tg, int nt,
                   double eps2, const double* eps2_t, double* gax, double* gay, double* gaz, cudaStream_t s) {
     if (nt <= 0) return MHPC_OK;

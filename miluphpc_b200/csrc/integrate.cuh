@@ -33,5 +33,7 @@ int launch_compact_d(int n, const int* keep, const int* rank, const double* src,
 int launch_compact_i(int n, const int* keep, const int* rank, const int* src, int* dst, cudaStream_t s);
 int launch_diagnostics(const mhpc_particles& p, int sph, double* part, double* out, cudaStream_t s);
 size_t diagnostics_scratch_doubles();
+// W = 1/2 sum m_i phi_i into out[0] (part: diagnostics scratch).
+int launch_potential_energy(int n, const double* m, const double* pot, double* part, double* out, cudaStream_t s);
 int launch_direct(const double* x, const double* y, const double* z, const double* m, int n, const int* tg, int nt,
                   double eps2, const double* eps2_t, double* gax, double* gay, double* gaz, cudaStream_t s);

@@ -144,6 +144,16 @@ class Miluphpc:
         v = list(out)
         return dict(kinetic=v[0], internal=v[1], momentum=v[2:5], angular_momentum=v[5:8], com=v[8:11])
 
+    def potential(self, per_particle=False):
+        """Potential energy W = 1/2 sum m phi of the current positions (and, with
+        per_particle, the potential phi_i as a device tensor in particle order)."""
+        w = ctypes.c_double(0.0)
+        pot = torch.zeros(self.n, dtype=torch.float64, device=self.device) if per_particle else None
+        check(self.L.mhpc_potential(self.ctx, ctypes.byref(self._soa),
+                                    ctypes.c_void_p(pot.data_ptr()) if pot is not None else None,
+                                    ctypes.byref(w)), "potential")
+        return (w.value, pot) if per_particle else w.value
+
     def export_sorted(self):
         keys = torch.zeros(self.n, dtype=torch.int64, device=self.device)
         perm = torch.zeros(self.n, dtype=torch.int32, device=self.device)

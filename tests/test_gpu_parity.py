@@ -451,6 +451,31 @@ def test_neighbour_lists_varying_h_and_shared_keys(cuda):
     sim.close()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_potential_matches_direct_sum(precision, cuda):
+    """mhpc_potential: per-particle potential of the list walk (geometric rule,
+    quadrupoles) against FP64 direct summation on a sample, W = 1/2 sum m phi
+    against the sample estimate, and the caller's accelerations untouched."""
+    n = 20_000
+    P = ics.plummer(n, seed=11)
+    cfg = gravity_cfg(sfc=1, precision=precision, theta_mixed=0.3, smoothing=1e-4)
+    sim = Miluphpc(cfg, P)
+    sim.rhs(0)
+    g0 = sim.numpy("g_ax").copy()
+    w, pot = sim.potential(per_particle=True)
+    assert np.array_equal(sim.numpy("g_ax"), g0)
+    tg = np.arange(0, n, 7)
+    _, _, _, ref = O.direct(P["x"], P["y"], P["z"], P["mass"], tg, 1e-4)
+    got = pot.cpu().numpy()[tg]
+    err = np.abs(got - ref) / np.abs(ref)
+    assert np.percentile(err, 99) < 1e-3, np.percentile(err, 99)
+    w_ref = 0.5 * np.sum(P["mass"][tg] * ref) * n / len(tg)
+    assert abs(w - w_ref) / abs(w_ref) < 2e-2  # sample estimate of the sum
+    w_full = 0.5 * float(np.sum(P["mass"] * pot.cpu().numpy()))
+    assert abs(w - w_full) <= 1e-12 * abs(w_full)
+    sim.close()
+
+
 @pytest.mark.parametrize("pinned", [False, True])
 def test_integrate_host_matches_device(pinned, cuda):
     """mhpc_integrate_host (host arrays in and out, positions copied out while
