@@ -290,6 +290,74 @@ struct ListSmem {
 // kGuard: some softened distance may be 0 (eps2 = 0), so 1/r is guarded; with
 // eps2 >= 1e-20 every r^2 >= eps2 keeps 1/r^3 finite and the guard is dropped
 // (it costs 11 % of the walk's instructions).
+// Packed form of the two evaluations for sm_100's paired FP32 instructions:
+// a lane's two particles are the halves of a float2, so every multiply/add of
+// the interaction is one paired instruction.  Each half is rounded exactly like
+// the scalar form (same operations in the same order; negations are exact).
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+
+template <bool kGuard>
+__device__ __forceinline__ float2 rsqrt2(float2 r2) {
+    float2 ri;
+    ri.x = kGuard ? (r2.x > 0.f ? rsqrtf(r2.x) : 0.f) : rsqrtf(r2.x);
+    ri.y = kGuard ? (r2.y > 0.f ? rsqrtf(r2.y) : 0.f) : rsqrtf(r2.y);
+    return ri;
+}
+
+template <bool kGuard>
+__device__ __forceinline__ void eval_cells_x2(const ListSmem& S, int count, const float (&rx)[2],
+                                              const float (&ry)[2], const float (&rz)[2], const float (&e2)[2],
+                                              double (&ax)[2], double (&ay)[2], double (&az)[2]) {
+    const float2 PX = make_float2(rx[0], rx[1]), PY = make_float2(ry[0], ry[1]), PZ = make_float2(rz[0], rz[1]);
+    const float2 E2 = make_float2(e2[0], e2[1]);
+    float2 fx = bc2(0.f), fy = bc2(0.f), fz = bc2(0.f);
+#pragma unroll 4
+    for (int e = 0; e < count; ++e) {
+        const float4 c = S.cpos[e];
+        const float4 a0 = S.cq0[e];
+        const float2 a1 = S.cq1[e];
+        const float2 Rx = __fadd2_rn(PX, bc2(-c.x)), Ry = __fadd2_rn(PY, bc2(-c.y)), Rz = __fadd2_rn(PZ, bc2(-c.z));
+        const float2 r2 = __ffma2_rn(Rx, Rx, __ffma2_rn(Ry, Ry, __ffma2_rn(Rz, Rz, E2)));
+        const float2 ri = rsqrt2<kGuard>(r2);
+        const float2 ri2 = __fmul2_rn(ri, ri);
+        const float2 ri3 = __fmul2_rn(ri, ri2);
+        const float2 ri5 = __fmul2_rn(ri3, ri2);
+        const float2 qx = __ffma2_rn(bc2(a0.x), Rx, __ffma2_rn(bc2(a0.y), Ry, __fmul2_rn(bc2(a0.z), Rz)));
+        const float2 qy = __ffma2_rn(bc2(a0.y), Rx, __ffma2_rn(bc2(a0.w), Ry, __fmul2_rn(bc2(a1.x), Rz)));
+        const float2 qz = __ffma2_rn(bc2(a0.z), Rx, __ffma2_rn(bc2(a1.x), Ry, __fmul2_rn(bc2(a1.y), Rz)));
+        const float2 rqr = __ffma2_rn(qx, Rx, __ffma2_rn(qy, Ry, __fmul2_rn(qz, Rz)));
+        // -(m/r^3 + 5/2 RQR/r^7)
+        const float2 cc = __ffma2_rn(bc2(-c.w), ri3, __fmul2_rn(__fmul2_rn(__fmul2_rn(bc2(-2.5f), rqr), ri5), ri2));
+        fx = __ffma2_rn(cc, Rx, __ffma2_rn(qx, ri5, fx));
+        fy = __ffma2_rn(cc, Ry, __ffma2_rn(qy, ri5, fy));
+        fz = __ffma2_rn(cc, Rz, __ffma2_rn(qz, ri5, fz));
+    }
+    ax[0] += fx.x; ay[0] += fy.x; az[0] += fz.x;
+    ax[1] += fx.y; ay[1] += fy.y; az[1] += fz.y;
+}
+
+template <bool kGuard>
+__device__ __forceinline__ void eval_leaves_x2(const ListSmem& S, int count, const float (&rx)[2],
+                                               const float (&ry)[2], const float (&rz)[2], const float (&e2)[2],
+                                               double (&ax)[2], double (&ay)[2], double (&az)[2]) {
+    const float2 PX = make_float2(rx[0], rx[1]), PY = make_float2(ry[0], ry[1]), PZ = make_float2(rz[0], rz[1]);
+    const float2 E2 = make_float2(e2[0], e2[1]);
+    float2 fx = bc2(0.f), fy = bc2(0.f), fz = bc2(0.f);
+#pragma unroll 4
+    for (int e = 0; e < count; ++e) {
+        const float4 c = S.lpos[e];
+        const float2 Rx = __fadd2_rn(PX, bc2(-c.x)), Ry = __fadd2_rn(PY, bc2(-c.y)), Rz = __fadd2_rn(PZ, bc2(-c.z));
+        const float2 r2 = __ffma2_rn(Rx, Rx, __ffma2_rn(Ry, Ry, __ffma2_rn(Rz, Rz, E2)));
+        const float2 ri = rsqrt2<kGuard>(r2);
+        const float2 nm = __fmul2_rn(bc2(-c.w), __fmul2_rn(__fmul2_rn(ri, ri), ri));  // -m / r^3
+        fx = __ffma2_rn(nm, Rx, fx);
+        fy = __ffma2_rn(nm, Ry, fy);
+        fz = __ffma2_rn(nm, Rz, fz);
+    }
+    ax[0] += fx.x; ay[0] += fy.x; az[0] += fz.x;
+    ax[1] += fx.y; ay[1] += fy.y; az[1] += fz.y;
+}
+
 // kPot: also the potential, -(m/r + RQR/(2 r^5)) per cell and -m/r per leaf,
 // leaving out the particle's own leaf (R = 0 exactly).
 template <bool kGuard, bool kPot>
@@ -354,6 +422,23 @@ __device__ __forceinline__ void eval_leaves(const ListSmem& S, int count, const 
         ax[k] += fx[k]; ay[k] += fy[k]; az[k] += fz[k];
         if (kPot) ph[k] += fp[k];
     }
+}
+
+// the packed forms for the force walk, the scalar forms when the potential is wanted
+constexpr bool kPackedEval = true;
+template <bool kGuard, bool kPot>
+__device__ __forceinline__ void eval_cells_sel(const ListSmem& S, int count, const float (&rx)[2], const float (&ry)[2],
+                                               const float (&rz)[2], const float (&e2)[2], double (&ax)[2],
+                                               double (&ay)[2], double (&az)[2], double (&ph)[2]) {
+    if (kPackedEval && !kPot) eval_cells_x2<kGuard>(S, count, rx, ry, rz, e2, ax, ay, az);
+    else eval_cells<kGuard, kPot>(S, count, rx, ry, rz, e2, ax, ay, az, ph);
+}
+template <bool kGuard, bool kPot>
+__device__ __forceinline__ void eval_leaves_sel(const ListSmem& S, int count, const float (&rx)[2], const float (&ry)[2],
+                                                const float (&rz)[2], const float (&e2)[2], double (&ax)[2],
+                                                double (&ay)[2], double (&az)[2], double (&ph)[2]) {
+    if (kPackedEval && !kPot) eval_leaves_x2<kGuard>(S, count, rx, ry, rz, e2, ax, ay, az);
+    else eval_leaves<kGuard, kPot>(S, count, rx, ry, rz, e2, ax, ay, az, ph);
 }
 
 constexpr int kListBlock = 128;
@@ -553,13 +638,13 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
         top += total;
         __syncwarp();
         if (ncell >= 32) {
-            eval_cells<kGuard, kPot>(S, ncell, rx, ry, rz, e2, ax, ay, az, ph);
+            eval_cells_sel<kGuard, kPot>(S, ncell, rx, ry, rz, e2, ax, ay, az, ph);
             ncell_tot += ncell;
             ncell = 0;
             __syncwarp();
         }
         if (nleaf >= 32) {
-            eval_leaves<kGuard, kPot>(S, nleaf, rx, ry, rz, e2, ax, ay, az, ph);
+            eval_leaves_sel<kGuard, kPot>(S, nleaf, rx, ry, rz, e2, ax, ay, az, ph);
             nleaf_tot += nleaf;
             nleaf = 0;
             __syncwarp();
@@ -585,7 +670,7 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
                 nleaf += __popc(ba);
                 __syncwarp();
                 if (nleaf >= 32) {
-                    eval_leaves<kGuard, kPot>(S, nleaf, rx, ry, rz, e2, ax, ay, az, ph);
+                    eval_leaves_sel<kGuard, kPot>(S, nleaf, rx, ry, rz, e2, ax, ay, az, ph);
                     nleaf_tot += nleaf;
                     nleaf = 0;
                     __syncwarp();
@@ -593,8 +678,8 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
             }
         }
     }
-    if (ncell) eval_cells<kGuard, kPot>(S, ncell, rx, ry, rz, e2, ax, ay, az, ph);
-    if (nleaf) eval_leaves<kGuard, kPot>(S, nleaf, rx, ry, rz, e2, ax, ay, az, ph);
+    if (ncell) eval_cells_sel<kGuard, kPot>(S, ncell, rx, ry, rz, e2, ax, ay, az, ph);
+    if (nleaf) eval_leaves_sel<kGuard, kPot>(S, nleaf, rx, ry, rz, e2, ax, ay, az, ph);
     ncell_tot += ncell;
     nleaf_tot += nleaf;
     unsigned nv = 0;
