@@ -282,8 +282,10 @@ struct ListSmem {
     float4 cq0[kListCap];   // cell: Qxx Qxy Qxz Qyy
     float2 cq1[kListCap];   // cell: Qyz Qzz
     float4 lpos[kListCap];  // leaf: x, y, z, m
-    float4 blo[kListSub];
-    float4 bhi[kListSub];
+    // sub-boxes, one array per component so that sub-boxes b, b+1 load as a
+    // float2: lower corner, NEGATED upper corner, alpha |a|_min, quad_alpha |a|_min
+    float bx0[kListSub], by0[kListSub], bz0[kListSub], bw0[kListSub];
+    float nbx1[kListSub], nby1[kListSub], nbz1[kListSub], bw1[kListSub];
     int defer[32];
 };
 
@@ -295,6 +297,7 @@ struct ListSmem {
 // the interaction is one paired instruction.  Each half is rounded exactly like
 // the scalar form (same operations in the same order; negations are exact).
 __device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 ld2(const float* a, int e) { return *reinterpret_cast<const float2*>(a + e); }
 
 template <bool kGuard>
 __device__ __forceinline__ float2 rsqrt2(float2 r2) {
@@ -521,9 +524,10 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
             bz1 = fmaxf(bz1, __shfl_xor_sync(MHPC_FULL, bz1, o));
         }
         if ((lane & 7) == 0) {
-            S.blo[4 * k + (lane >> 3)] = make_float4(bx0, by0, bz0, amin);
+            const int b = 4 * k + (lane >> 3);
+            S.bx0[b] = bx0; S.by0[b] = by0; S.bz0[b] = bz0; S.bw0[b] = amin;
             // bhi.w: quad_alpha |a|_min of the sub-box (monopole threshold)
-            S.bhi[4 * k + (lane >> 3)] = make_float4(bx1, by1, bz1, kRel ? amin * qratio : 0.f);
+            S.nbx1[b] = -bx1; S.nby1[b] = -by1; S.nbz1[b] = -bz1; S.bw1[b] = kRel ? amin * qratio : 0.f;
         }
     }
     const double edge0 = ord_to_dbl(P.ord[1]) - ord_to_dbl(P.ord[0]);
@@ -576,20 +580,29 @@ __global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams
                 // quad_alpha |a| for every sub-box makes the cell a monopole
                 bool mono = kRel;
                 const float ml2 = m * l2;
+                // sub-boxes in pairs on paired FP32 instructions (each half rounded
+                // like the scalar form); the max/compare steps stay scalar
+                const float2 NX = bc2(nx), NY = bc2(ny), NZ = bc2(nz), MNX = bc2(-nx), MNY = bc2(-ny), MNZ = bc2(-nz);
 #pragma unroll
-                for (int b = 0; b < kListSub; ++b) {
-                    const float4 lo = S.blo[b], hi = S.bhi[b];
-                    const float dx = fmaxf(fmaxf(lo.x - nx, nx - hi.x), 0.f);
-                    const float dy = fmaxf(fmaxf(lo.y - ny, ny - hi.y), 0.f);
-                    const float dz = fmaxf(fmaxf(lo.z - nz, nz - hi.z), 0.f);
-                    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                for (int b = 0; b < kListSub; b += 2) {
+                    const float2 ax0 = __fadd2_rn(ld2(S.bx0, b), MNX), ax1 = __fadd2_rn(NX, ld2(S.nbx1, b));
+                    const float2 ay0 = __fadd2_rn(ld2(S.by0, b), MNY), ay1 = __fadd2_rn(NY, ld2(S.nby1, b));
+                    const float2 az0 = __fadd2_rn(ld2(S.bz0, b), MNZ), az1 = __fadd2_rn(NZ, ld2(S.nbz1, b));
+                    const float2 dx = make_float2(fmaxf(fmaxf(ax0.x, ax1.x), 0.f), fmaxf(fmaxf(ax0.y, ax1.y), 0.f));
+                    const float2 dy = make_float2(fmaxf(fmaxf(ay0.x, ay1.x), 0.f), fmaxf(fmaxf(ay0.y, ay1.y), 0.f));
+                    const float2 dz = make_float2(fmaxf(fmaxf(az0.x, az1.x), 0.f), fmaxf(fmaxf(az0.y, az1.y), 0.f));
+                    const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
                     if (kRel) {
                         // safety bound d >= l, then M l^3 <= alpha |a| d^5
                         // (d2 = 0 gives NaN: not accepted)
-                        ok = ok && l2 <= d2 && w3.w <= lo.w * (d2 * d2) * (d2 * rsqrtf(d2));
-                        mono = mono && ml2 <= hi.w * (d2 * d2);
+                        const float2 d4 = __fmul2_rn(d2, d2);
+                        const float2 d1 = __fmul2_rn(d2, make_float2(rsqrtf(d2.x), rsqrtf(d2.y)));
+                        const float2 lim = __fmul2_rn(__fmul2_rn(ld2(S.bw0, b), d4), d1);
+                        const float2 qlim = __fmul2_rn(ld2(S.bw1, b), d4);
+                        ok = ok && l2 <= d2.x && l2 <= d2.y && w3.w <= lim.x && w3.w <= lim.y;
+                        mono = mono && ml2 <= qlim.x && ml2 <= qlim.y;
                     } else {
-                        ok = ok && lp.w <= d2;
+                        ok = ok && lp.w <= d2.x && lp.w <= d2.y;
                     }
                 }
                 // accepted monopoles go to the leaf list (monopole evaluation)
