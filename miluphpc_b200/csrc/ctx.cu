@@ -401,11 +401,11 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
     T.n = 0;
     T.cap_nodes = c->cap_nodes;
     A(T.dl, n); A(T.cnt, n); A(T.off, n + 1); A(T.leaf_node, n);
-    A(T.link, M); A(T.first, M); A(T.last, M); A(T.parent, M); A(T.nchild, M);
+    A(T.link, M); A(T.first, M); A(T.last, M);
     A(T.kids, 8 * M); A(T.kmask, M);
     A(T.com, M); A(T.bmin, M); A(T.bmax, M); A(T.hmax, M);
     A(T.level_cells, M); A(T.level_off, 64);
-    A(T.root_nchild, 1); A(T.nodes, 1);
+    A(T.nodes, 1);
     if (cfg->gravity) {
         A(T.quad0, M); A(T.quad1, M); A(T.wrec, 4 * M);
     }

@@ -112,10 +112,8 @@ __global__ void __launch_bounds__(256) k_nodes(TreeDev T, const uint64_t* __rest
             T.link[node] = make_int2(T.off[b + 1], L);
             T.first[node] = a;
             T.last[node] = b;
-            T.parent[node] = par;
             if (par >= T.cap_nodes) set_status(st, MHPC_ERR_NODE_POOL, par);
-            else if (par >= 0) { atomicAdd(&T.nchild[par], 1); add_kid(T, par, node, ka, L); }
-            else atomicAdd(T.root_nchild, 1);
+            else if (par >= 0) add_kid(T, par, node, ka, L);
         }
         const int node = o + c;
         if (node >= T.cap_nodes) { set_status(st, MHPC_ERR_NODE_POOL, node); continue; }
@@ -131,26 +129,19 @@ __global__ void __launch_bounds__(256) k_nodes(TreeDev T, const uint64_t* __rest
         T.link[node] = make_int2(node + 1, (P + 1) | ND_LEAF);
         T.first[node] = a;
         T.last[node] = a;
-        T.parent[node] = par;
-        T.nchild[node] = 0;
         T.leaf_node[a] = node;
         if (par >= T.cap_nodes) set_status(st, MHPC_ERR_NODE_POOL, par);
-        else if (par >= 0) { atomicAdd(&T.nchild[par], 1); add_kid(T, par, node, ka, P + 1); }
-        else atomicAdd(T.root_nchild, 1);
+        else if (par >= 0) add_kid(T, par, node, ka, P + 1);
         if (P + 1 > MHPC_MAX_LEVEL) atomicMax(&st->max_level, P + 1);
     }
 }
 
 __global__ void k_zero_cells(TreeDev T) {
-    // nchild of cells must be zero before k_nodes counts; cells are the
-    // non-leaf nodes, whose ids are unknown before the scan, so clear all.
+    // child masks of cells must be zero before k_nodes sets their bits; cells
+    // are the non-leaf nodes, whose ids are unknown before the scan, so clear all.
     int total = *T.nodes;
     if (total > T.cap_nodes) total = T.cap_nodes;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-        T.nchild[i] = 0;
-        T.kmask[i] = 0;
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) *T.root_nchild = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) T.kmask[i] = 0;
 }
 
 __global__ void k_copy_total(TreeDev T) { *T.nodes = T.off[T.n]; }

@@ -26,8 +26,6 @@ struct TreeDev {
     int2* link;         // [cap] (skip, level | ND_LEAF)
     int* first;         // [cap] first sorted particle of the node
     int* last;          // [cap] last sorted particle of the node
-    int* parent;        // [cap] parent node, -1 for root children
-    int* nchild;        // [cap] number of children
     int* kids;          // [cap * 8] children by key digit (valid where kmask has the bit)
     int* kmask;         // [cap] bit d: slot d used; 0x100: children without a digit (shared keys)
     double4* com;       // [cap] centre of mass (x, y, z, m)
@@ -45,7 +43,6 @@ struct TreeDev {
     int* level_cells;   // [cap] cell ids grouped by level (any order within a level)
     int* level_off;     // [64] level_off[L] = start of level L's cells (L = 1..21, [22] = end);
                         // [32 + L] = fill cursors while the lists are built
-    int* root_nchild;   // [1]
     int* nodes;         // [1] total nodes (= off[n]), device copy
 };
 
