@@ -401,7 +401,7 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
     T.n = 0;
     T.cap_nodes = c->cap_nodes;
     A(T.dl, n); A(T.cnt, n); A(T.off, n + 1); A(T.leaf_node, n);
-    A(T.link, M); A(T.first, M); A(T.last, M);
+    A(T.link, M); A(T.first, M); A(T.last, M); A(T.parent, M);
     A(T.kids, 8 * M); A(T.kmask, M);
     A(T.com, M); A(T.bmin, M); A(T.bmax, M); A(T.hmax, M);
     A(T.level_cells, M); A(T.level_off, 64);

@@ -574,9 +574,15 @@ __global__ void __launch_bounds__(kBlock) k_count_sub(TreeDev T, const double* _
 // Convergence rule and update of fixedRadiusNN_variableSML
 // (src/sph/sph.cu:911-933): stop when nit > max_iter or |n - target| < tol,
 // provided n < maxnb; otherwise h *= 0.5 (1 + (target / max(n,1))^(1/3)).
+//
+// The sweep's counts are complete when this runs, so the new h goes straight
+// into the snapshot too (hold), and a larger h raises the largest-h bound of
+// the particle's leaf and ancestors (grow-only, stopping at the first ancestor
+// already as large; a bound left larger than the subtree's h only prunes less).
 __global__ void k_vh_update(const int* __restrict__ list, const int* __restrict__ list_count,
-                            const int* __restrict__ count, double* h, int* done, int* nit, int target, int tol,
-                            int max_iter, int maxnb) {
+                            const int* __restrict__ count, double* h, double* hold, int* done, int* nit, int target,
+                            int tol, int max_iter, int maxnb, float* node_hmax, const int* __restrict__ leaf_node,
+                            const int* __restrict__ parent) {
     const int m = *list_count;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x) {
         const int i = list[q];
@@ -586,7 +592,16 @@ __global__ void k_vh_update(const int* __restrict__ list, const int* __restrict_
             done[i] = 1;
         } else {
             const int cc = c < 1 ? 1 : c;
-            h[i] *= 0.5 * (1.0 + pow((double)target / (double)cc, 1. / 3.));
+            const double h0 = h[i];
+            const double hn = h0 * (0.5 * (1.0 + pow((double)target / (double)cc, 1. / 3.)));
+            h[i] = hn;
+            hold[i] = hn;
+            if (hn > h0) {
+                // positive floats order like their bit patterns
+                const int v = __float_as_int(__double2float_ru(hn));
+                for (int nd = leaf_node[i]; nd >= 0; nd = parent[nd])
+                    if (atomicMax(reinterpret_cast<int*>(node_hmax + nd), v) >= v) break;
+            }
         }
     }
 }
@@ -940,16 +955,18 @@ int sph_variable_h(const TreeDev& T, const SphParams& P, const double* x, const 
     const long blocks = (((long)P.n + 31) / 32 * 32 + kBlock - 1) / kBlock;
     const int g = grid_for(P.n, 256, 148 * 16);
     const int* list_count = B.off + P.n;
+    // Jacobi snapshot of h and the largest-h bounds; k_vh_update keeps both
+    // current from then on
+    k_copy<<<g, 256, 0, s>>>(P.n, h, B.hold);
+    int rc0 = tree_node_hmax(T, B.hold, st, s);
+    if (rc0) return rc0;
     for (int it = 0; it < sweeps; ++it) {
-        // Jacobi snapshot of h, then the list of particles still iterating
-        k_copy<<<g, 256, 0, s>>>(P.n, h, B.hold);
+        // the list of particles still iterating
         k_flags<<<g, 256, 0, s>>>(P.n, B.done, B.flags);
         int rc = scan_exclusive_i32(B.flags, B.off, P.n, B.scan_scratch, s);
         if (rc) return rc;
         k_compact<<<g, 256, 0, s>>>(P.n, B.flags, B.off, B.list);
         if (it == 1) k_record_active<<<1, 1, 0, s>>>(list_count, P.n, st);
-        rc = tree_node_hmax(T, B.hold, st, s);
-        if (rc) return rc;
         if (it == 0) {
             // first sweep: (nearly) every particle, group walks
             k_frnn<1><<<(int)blocks, kBlock, 0, s>>>(T, P.n, P.maxnb, x, y, z, B.hold, B.list, list_count, T.hmax,
@@ -958,8 +975,8 @@ int sph_variable_h(const TreeDev& T, const SphParams& P, const double* x, const 
             // later sweeps: the few particles still iterating, 8 lanes each
             k_count_sub<<<148 * 16, kBlock, 0, s>>>(T, x, y, z, B.hold, B.list, list_count, T.hmax, B.count, st);
         }
-        k_vh_update<<<g, 256, 0, s>>>(B.list, list_count, B.count, h, B.done, B.nit, target, tol, max_iter,
-                                      P.maxnb);
+        k_vh_update<<<g, 256, 0, s>>>(B.list, list_count, B.count, h, B.hold, B.done, B.nit, target, tol, max_iter,
+                                      P.maxnb, T.hmax, T.leaf_node, T.parent);
     }
     k_flags<<<g, 256, 0, s>>>(P.n, B.done, B.flags);
     int rc = scan_exclusive_i32(B.flags, B.off, P.n, B.scan_scratch, s);

@@ -112,6 +112,7 @@ __global__ void __launch_bounds__(256) k_nodes(TreeDev T, const uint64_t* __rest
             T.link[node] = make_int2(T.off[b + 1], L);
             T.first[node] = a;
             T.last[node] = b;
+            T.parent[node] = par;
             if (par >= T.cap_nodes) set_status(st, MHPC_ERR_NODE_POOL, par);
             else if (par >= 0) add_kid(T, par, node, ka, L);
         }
@@ -129,6 +130,7 @@ __global__ void __launch_bounds__(256) k_nodes(TreeDev T, const uint64_t* __rest
         T.link[node] = make_int2(node + 1, (P + 1) | ND_LEAF);
         T.first[node] = a;
         T.last[node] = a;
+        T.parent[node] = par;
         T.leaf_node[a] = node;
         if (par >= T.cap_nodes) set_status(st, MHPC_ERR_NODE_POOL, par);
         else if (par >= 0) add_kid(T, par, node, ka, P + 1);

@@ -26,6 +26,7 @@ struct TreeDev {
     int2* link;         // [cap] (skip, level | ND_LEAF)
     int* first;         // [cap] first sorted particle of the node
     int* last;          // [cap] last sorted particle of the node
+    int* parent;        // [cap] parent node, -1 for root children
     int* kids;          // [cap * 8] children by key digit (valid where kmask has the bit)
     int* kmask;         // [cap] bit d: slot d used; 0x100: children without a digit (shared keys)
     double4* com;       // [cap] centre of mass (x, y, z, m)
