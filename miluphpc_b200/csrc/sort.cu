@@ -362,12 +362,9 @@ int sort_pairs_u64(const uint64_t* keys_in, const int* vals_in, uint64_t* keys_o
     CUDA_TRY(cudaGetLastError());
     k_hist_scan<<<kPasses, kRadix, 0, s>>>(S.hist);
     CUDA_TRY(cudaGetLastError());
-    static bool attr_set = false;
+    // per device (a process may drive several GPUs); a cheap host call
     size_t smem = sizeof(OnesweepSmem);
-    if (!attr_set) {
-        CUDA_TRY(cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
-    }
+    CUDA_TRY(cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const uint64_t* kin = keys_in;
     const int* vin = vals_in;
     for (int p = 0; p < kPasses; ++p) {
