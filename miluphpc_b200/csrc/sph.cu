@@ -180,7 +180,9 @@ struct FrnnSmem {
 };
 
 template <int MODE>
-__global__ void __launch_bounds__(kBlock) k_frnn(TreeDev T, int n, int maxnb, const double* __restrict__ sx,
+// 6 blocks per SM (the register cap costs a few spilled values, the extra
+// warps hide more of the walk's latency)
+__global__ void __launch_bounds__(kBlock, 6) k_frnn(TreeDev T, int n, int maxnb, const double* __restrict__ sx,
                                                  const double* __restrict__ sy, const double* __restrict__ sz,
                                                  const double* __restrict__ sh, const int* __restrict__ list,
                                                  const int* __restrict__ list_count,
