@@ -208,6 +208,9 @@ int stage_gravity(mhpc_ctx* c, const mhpc_particles* p) {
         G.theta = c->cfg.theta_mixed;
         TRY(gravity_mixed(c->T, G, c->sx, c->sy, c->sz, c->sh, c->perm, p->g_ax, p->g_ay, p->g_az, c->st,
                           c->stream));
+    } else if (c->cfg.gravity_force_version == 2) {
+        G.theta = c->cfg.theta;
+        TRY(gravity_v1(c->T, G, c->sh, c->perm, p->g_ax, p->g_ay, p->g_az, c->st, c->stream));
     } else {
         G.theta = c->cfg.theta;
         TRY(gravity_v2(c->T, G, c->sx, c->sy, c->sz, c->sh, c->perm, p->g_ax, p->g_ay, p->g_az, c->st,

@@ -90,6 +90,71 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_v2(const double4* __restric
     }
 }
 
+// computeForces_v1 semantics (src/gravity/gravity.cu:252-396, gravityForceVersion
+// 2): every particle walks the tree on its own (one thread per particle,
+// stackless over the pre-order and skip links; the reference keeps a stack of
+// child slots, which visits the nodes in the same order for Lebesgue keys).
+// A node other than the particle's own leaf is accepted when it is a leaf or
+// d^2 theta^2 > cellSize(level), cellSize(1) = radius^2, quartered per level;
+// accepted nodes add m d / |d|^3 with |d| = sqrt(d^2), d^2 formed as dx^2 +
+// eps2 + dy^2 + dz^2 in that order, all products and sums explicitly rounded
+// like the reference's -fmad=false build.
+__global__ void __launch_bounds__(kWalkBlock) k_grav_v1(const double4* __restrict__ com, const int2* __restrict__ link,
+                                                        const int* __restrict__ nodes_total,
+                                                        const int* __restrict__ leaf_node, GravParams P,
+                                                        const double* __restrict__ sh, const int* __restrict__ perm,
+                                                        double* __restrict__ gax, double* __restrict__ gay,
+                                                        double* __restrict__ gaz, DevStatus* st) {
+    if (st->code) return;
+    const int M = *nodes_total;
+    const long s = (long)blockIdx.x * kWalkBlock + threadIdx.x;
+    const bool valid = s < P.n;
+    unsigned long long ninter = 0, nvisit = 0;
+    if (valid) {
+        const int self = __ldg(leaf_node + s);
+        const double4 pc = ldg_d4(com + self);
+        double e2 = P.eps2;
+        if (P.h_factor > 0.0) { const double e = P.h_factor * __ldg(sh + s); e2 += e * e; }
+        const double radius = 0.5 * (ord_to_dbl(P.ord[1]) - ord_to_dbl(P.ord[0]));
+        const double cs1 = radius * radius, th2 = P.theta * P.theta;
+        double ax = 0, ay = 0, az = 0;
+        int nd = 0;
+        while (nd < M) {
+            const int2 lk = __ldg(link + nd);
+            ++nvisit;
+            if (nd == self) { nd = lk.x; continue; }
+            const double4 c = ldg_d4(com + nd);
+            const double dx = c.x - pc.x, dy = c.y - pc.y, dz = c.z - pc.z;
+            double d = __dadd_rn(__dmul_rn(dx, dx), e2);
+            d = __dadd_rn(d, __dmul_rn(dy, dy));
+            d = __dadd_rn(d, __dmul_rn(dz, dz));
+            const bool leaf = lk.y & ND_LEAF;
+            if (leaf || __dmul_rn(d, th2) > ldexp(cs1, -2 * ((lk.y & 0xff) - 1))) {
+                const double r = __dsqrt_rn(d);
+                const double f = __ddiv_rn(c.w, __dmul_rn(__dmul_rn(r, r), r));
+                ax = __dadd_rn(ax, __dmul_rn(f, dx));
+                ay = __dadd_rn(ay, __dmul_rn(f, dy));
+                az = __dadd_rn(az, __dmul_rn(f, dz));
+                ++ninter;
+                nd = lk.x;
+            } else {
+                ++nd;
+            }
+        }
+        const int o = __ldg(perm + s);
+        gax[o] = P.G * ax; gay[o] = P.G * ay; gaz[o] = P.G * az;
+    }
+    // statistics, one atomic per warp
+    for (int o = 16; o > 0; o >>= 1) {
+        ninter += __shfl_xor_sync(MHPC_FULL, ninter, o);
+        nvisit += __shfl_xor_sync(MHPC_FULL, nvisit, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&st->interactions, ninter);
+        atomicAdd(&st->nodes_visited, nvisit);
+    }
+}
+
 // -------------------------------------------------------------- mixed FP32
 // The group's centre c (FP64, centre of its bounding box) is subtracted once;
 // lanes hold their position relative to c in FP32, nodes are stored as
@@ -721,6 +786,15 @@ int gravity_v2(const TreeDev& T, const GravParams& P, const double* sx, const do
     long groups = ((long)P.n + 31) / 32;
     long blocks = (groups * 32 + kWalkBlock - 1) / kWalkBlock;
     k_grav_v2<<<(int)blocks, kWalkBlock, 0, s>>>(T.com, T.link, T.nodes, P, sx, sy, sz, sh, perm, gax, gay, gaz, st);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int gravity_v1(const TreeDev& T, const GravParams& P, const double* sh, const int* perm, double* gax, double* gay,
+               double* gaz, DevStatus* st, cudaStream_t s) {
+    if (P.n <= 0) return MHPC_OK;
+    const long blocks = ((long)P.n + kWalkBlock - 1) / kWalkBlock;
+    k_grav_v1<<<(int)blocks, kWalkBlock, 0, s>>>(T.com, T.link, T.nodes, T.leaf_node, P, sh, perm, gax, gay, gaz, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

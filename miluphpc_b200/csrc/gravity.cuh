@@ -19,6 +19,10 @@ struct GravParams {
 int gravity_v2(const TreeDev& T, const GravParams& P, const double* sx, const double* sy, const double* sz,
                const double* sh, const int* perm, double* gax, double* gay, double* gaz, DevStatus* st,
                cudaStream_t s);
+// Plain FP64 walk with the reference's computeForces_v1 semantics (one walk
+// per particle).
+int gravity_v1(const TreeDev& T, const GravParams& P, const double* sh, const int* perm, double* gax, double* gay,
+               double* gaz, DevStatus* st, cudaStream_t s);
 // Mixed FP32 walk, per-lane vote: hi/lo node positions relative to the group
 // centre, every particle of the warp votes on each cell, monopole + quadrupole,
 // FP64 flush of FP32 partial sums (precision 2).

@@ -194,6 +194,26 @@ def test_gravity_v2_matches_oracle(curve, theta, cuda):
     sim.close()
 
 
+@pytest.mark.parametrize("curve", [0, 1])
+def test_gravity_v1_matches_oracle(curve, cuda):
+    """gravityForceVersion 2 (computeForces_v1 semantics): the same accepted
+    nodes as the oracle's per-particle walk; for Lebesgue keys the visiting
+    order is the reference's child-slot order, so the sums agree to rounding."""
+    n = 20_000
+    P = ics.plummer(n, seed=6)
+    cfg = gravity_cfg(sfc=curve, theta=0.5, smoothing=1e-4, gravity_force_version=2)
+    sim = Miluphpc(cfg, P)
+    sim.rhs(0)
+    gx, gy, gz = sim.numpy("g_ax"), sim.numpy("g_ay"), sim.numpy("g_az")
+    bb = O.bbox(P["x"], P["y"], P["z"])
+    T = O.Tree(P["x"], P["y"], P["z"], P["mass"], bb)
+    ox, oy, oz, cnt = O.gravity_v1(T, 0.5 * (bb[1] - bb[0]), 0.5, 1e-4)
+    e = rel_err(gx, gy, gz, ox, oy, oz)
+    assert e.max() < (1e-14 if curve == 0 else 1e-11), e.max()
+    assert sim.stats()["gravity_interactions"] == int(cnt.sum())
+    sim.close()
+
+
 @pytest.mark.parametrize("precision,theta", [(1, 0.3), (2, 0.25)])
 def test_gravity_mixed_accuracy(precision, theta, cuda):
     """Both mixed walks: p99 <= 1e-3 against FP64 direct summation and close
