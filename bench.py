@@ -59,6 +59,19 @@ def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def job_rate(ms_local, n_per_rank, steps, world, device):
+    """Whole-job particle-steps/s of `world` replicas of n_per_rank particles:
+    the slowest replica's device time (max over ranks) bounds the job.
+    Returns (value, max ms); every rank takes part in the reduction."""
+    import torch
+    t = torch.tensor([ms_local], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    return n_per_rank * world * steps / (ms_max / 1e3), ms_max
+
+
 class ClockSampler:
     """nvidia-smi samples during the timed region."""
 
@@ -275,11 +288,7 @@ def run_ours(args, wl):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     clk = clocks.stop()
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = n * world * args.steps / (ms_max / 1e3)
+    value, ms_max = job_rate(ms, n, args.steps, world, dev)
     last = sim.stats()
     energy = None
     if e_start is not None:
@@ -541,8 +550,10 @@ def run_reference(args, wl):
         return None
     per_step = []
     cb = None
-    for _ in range(args.warmup if args.warmup < 1 else 1):
-        pass
+    # one untimed sample stands for the warm-up steps (each sample is ~10 s of
+    # CPU work; W of them would not fit the run's few minutes)
+    if args.warmup > 0:
+        cpu_baseline(wl, args, sample_groups=args.cpu_sample_groups)
     for s in range(max(1, args.steps)):
         cb = cpu_baseline(wl, args, sample_groups=args.cpu_sample_groups)
         per_step.append(cb["value"])
