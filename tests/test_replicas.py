@@ -40,7 +40,7 @@ def _worker(rank, world, port, out):
 
 def test_job_rate_is_the_slowest_replica_over_two_gloo_ranks():
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(_worker, args=(2, port, out), nprocs=2, join=True)
         res = dict(out)
