@@ -206,6 +206,25 @@ def test_info_and_cfg_parsers():
     assert _lib.load().mhpc_materials_from_cfg(bad.encode(), mats, 8, ctypes.byref(cnt)) == 8
 
 
+def test_info_extension_keys(tmp_path):
+    """The .info keys of this library's options (opening rule, monopole cells,
+    Balsara switch, force version, precision) parse into mhpc_config, and an
+    invalid opening-rule setting is a status code."""
+    info = tmp_path / "ext.info"
+    info.write_text("; extension keys\nintegrator 2\ntheta 0.5\nprecision 1\nthetaMixed 0.28\n"
+                    "gravityMac 1\nmacAlpha 0.0018\nmacQuadAlpha 3e-4\nbalsaraSwitch true\n"
+                    "gravityForceVersion 2\nsfc 1\n")
+    cfg = _lib.default_config()
+    _lib.check(_lib.load().mhpc_config_from_info(str(info).encode(), ctypes.byref(cfg)))
+    assert cfg.precision == 1 and cfg.theta_mixed == pytest.approx(0.28)
+    assert cfg.gravity_mac == 1 and cfg.mac_alpha == pytest.approx(1.8e-3)
+    assert cfg.mac_quad_alpha == pytest.approx(3e-4) and cfg.balsara == 1
+    assert cfg.gravity_force_version == 2 and cfg.sfc == 1
+    bad = tmp_path / "bad.info"
+    bad.write_text("gravityMac 1\nmacAlpha 0\n")
+    assert _lib.load().mhpc_config_from_info(str(bad).encode(), ctypes.byref(_lib.default_config())) == 8
+
+
 def test_generators_shapes_and_seeds():
     a = ics.plummer(1000, seed=1)
     b = ics.plummer(1000, seed=1)
