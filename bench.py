@@ -412,27 +412,30 @@ def hbm_peak_gbs():
 
 
 def launches_per_step(variant, kind="gravity"):
-    # per RHS: bbox, bbox_finish, keys, hist, hist_scan, 8 onesweep, gather,
-    # lcp, count, 4 scan, copy_total, zero_cells, nodes, upward
-    tree = 2 + 1 + 2 + 8 + 1 + 2 + 4 + 3 + 1
+    """This library's kernel launches in one timed step (counted from the
+    launch sequence; the ncu launch lists in profiles/ show the same)."""
+    # every RHS: bbox, bbox_finish, keys, hist, hist_scan, 8 onesweep (13), gather (1),
+    # tree: lcp, count, 4 scan, copy_total, zero_cells, nodes, 3 level-list kernels (12),
+    # upward: leaves + 21 levels (22)
+    tree = 13 + 1 + 12 + 22
+    mixed = variant == "mixed"
     if kind == "sph":
-        # frnn, density_eos, forces, export noi; predictor-corrector: two RHS,
-        # max_sml + dt_blocks + dt_final, predictor, corrector
-        rhs = tree + 4
-        return 2 * rhs + 3 + 2
-    rhs = tree + 1  # walk
-    if variant == "mixed":
-        rhs += 1  # mixed node conversion
+        # frnn, (mixed: position pack), density+EOS, forces; noi export on the
+        # first RHS only; predictor-corrector: 3 step-size kernels, predictor, corrector
+        rhs = tree + 1 + (1 if mixed else 0) + 2
+        return (rhs + 1) + rhs + 3 + 2
+    grav = tree + 1  # + the walk
     if kind == "cloud":
-        # variable h: 7 sweeps x (copy, flags, 4 scan, compact, count walk,
-        # update) + 1 record, final flags + scan + record, scatter; SPH: frnn,
-        # density, forces, noi export, band stats; learned: apply, collect,
-        # features; explicit Euler update
-        vh = 7 * 9 + 1 + 6 + 1
-        sphk = 5
-        learned = 3 if variant == "mixed" else 0
-        return rhs + vh + sphk + learned + 1
-    return rhs + 2  # leapfrog updateX, updateV
+        # variable h: snapshot copy, largest-h bounds (leaves + 21 levels), 7 sweeps x
+        # (flags, 4 scan, compact, count walk, update), record, final flags + 4 scan +
+        # record, scatter of h; list walk with its own bounds (22 + 1); (mixed:
+        # position pack) density, forces, noi export, band statistics; learned h:
+        # apply, collect, features; explicit Euler update
+        vh = 1 + 22 + 7 * 8 + 1 + 6 + 1
+        sphk = 23 + (1 if mixed else 0) + 4
+        learned = 3 if mixed else 0
+        return grav + vh + sphk + learned + 1
+    return grav + 2  # leapfrog updateX, updateV
 
 
 def run_e2e(args, wl, sim, state, torch, step0):
