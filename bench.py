@@ -350,7 +350,8 @@ def run_ours(args, wl):
                     "work_unit": "%d flop per accepted monopole interaction + %d per quadrupole term"
                                  % (FLOP_MONO, FLOP_QUAD),
                     "kernel_ms_per_launch": round(kms, 3), "interactions_per_launch": inter / args.steps}
-        cpu = cpu_baseline(wl, args) if not args.no_cpu_baseline else None
+        # CPU baseline: rank 0 of a single-GPU run only
+        cpu = cpu_baseline(wl, args) if (not args.no_cpu_baseline and world == 1) else None
         if sph:
             cfg_out = {"workload": args.workload, "n_particles": n, "variant": args.variant,
                        "integrator": "predictor-corrector", "kernel": "cubic spline", "h": "fixed 2.5 dx",
