@@ -29,11 +29,12 @@ sys.path.insert(0, ROOT)
 
 WORKLOADS = {
     # Plummer at scale, precision form: N = 2^24, Hilbert keys, leapfrog dt 0.01
+    # (plain FP64 v2 at theta 0.15: p99 7.5e-4 against the mixed run's 8.0e-4)
     "plummer16m": dict(kind="gravity", n=1 << 24, sfc=1, dt=0.01, eps2=1e-4, theta=0.5, theta_mixed=0.28,
-                       mac_alpha=1.8e-3, mac_quad_alpha=3e-4, theta_plain_matched=0.1, seed=1),
+                       mac_alpha=1.8e-3, mac_quad_alpha=3e-4, theta_plain_matched=0.15, seed=1, drift_steps=50),
     # profiling case of the walk: node data (~190 MB) larger than L2
     "plummer2m": dict(kind="gravity", n=1 << 21, sfc=1, dt=0.01, eps2=1e-4, theta=0.5, theta_mixed=0.28,
-                      mac_alpha=1.8e-3, mac_quad_alpha=3e-4, theta_plain_matched=0.1, seed=1),
+                      mac_alpha=1.8e-3, mac_quad_alpha=3e-4, theta_plain_matched=0.15, seed=1, drift_steps=50),
     # Sedov blast, SPH only: 128^3 lattice, fixed h = 2.5 dx, predictor-corrector
     "sedov2m": dict(kind="sph", nside=128, n=128 ** 3, sfc=0, dt_max=1e-4, seed=2),
     "sedov262k": dict(kind="sph", nside=64, n=64 ** 3, sfc=0, dt_max=1e-4, seed=2),
@@ -48,7 +49,7 @@ WORKLOADS = {
                     theta_plain_matched=0.05, train_steps=20, train_iters=1500, seed=3),
     # the reference's own single-rank case: N = 131072, Lebesgue, leapfrog dt 0.025
     "plummer131k": dict(kind="gravity", n=131072, sfc=0, dt=0.025, eps2=1e-4, theta=0.5, theta_mixed=0.28,
-                        mac_alpha=1.8e-3, mac_quad_alpha=3e-4, theta_plain_matched=0.1, seed=1),
+                        mac_alpha=1.8e-3, mac_quad_alpha=3e-4, theta_plain_matched=0.15, seed=1, drift_steps=10),
 }
 
 FLOP_MONO = 19   # flop per accepted particle-node monopole interaction
@@ -175,10 +176,11 @@ def make_sim(wl, state, variant):
                                   smoothing_kernel=1, integrate_energy=0,
                                   precision=wl.get("mixed_precision", 1) if mixed else 0,
                                   theta=wl["theta"] if variant == "plain" else wl["theta_plain_matched"],
-                                  theta_mixed=wl["theta_mixed"], learned_h=1 if mixed else 0,
+                                  theta_mixed=wl["theta_mixed"], learned_h=1 if (mixed and wl.get("learned", 1)) else 0,
                                   gravity_mac=1 if (mixed and wl.get("mac_alpha")) else 0,
                                   mac_alpha=wl.get("mac_alpha") or 0.003,
-                                  mac_quad_alpha=wl.get("mac_quad_alpha", 0.0) if mixed else 0.0)
+                                  mac_quad_alpha=wl.get("mac_quad_alpha", 0.0) if mixed else 0.0,
+                                  sml_band_rounds=wl.get("band_rounds", 8))
         return Miluphpc(cfg, state, materials=[material(interactions=60, alpha=1.0, beta=2.0, eos_type=0,
                                                         K=state["cs2"], gamma=1.0)])
     kw = dict(gravity=1, sph=0, integrator=2, time_step=wl["dt"], smoothing=wl["eps2"], sfc=wl["sfc"],
@@ -220,6 +222,99 @@ def force_error(sim, torch, eps2, ntarget=4096, seed=7, h_factor=0.0, h=None):
             "targets": int(len(tg))}
 
 
+def cloud_energy(sim, torch):
+    """Conserved quantities of the isothermal cloud: E = K + W + U with U =
+    sum m c_s^2 ln rho (the isothermal internal energy, c_s^2 = K of the
+    gamma = 1 polytrope; rho from the last right-hand side), W from the tree
+    potential with the walk's h-tied softening, and the angular momentum."""
+    d = sim.diagnostics()
+    w = sim.potential()
+    n = sim.n
+    cs2 = float(sim.materials[0].polytropic_K)
+    rho = sim.t["rho"][:n]
+    u = float((sim.t["mass"][:n] * cs2 * torch.log(torch.clamp(rho, min=1e-300))).sum().item()) \
+        if bool((rho > 0).all().item()) else float("nan")
+    return {"E": d["kinetic"] + w + u, "L": d["angular_momentum"]}
+
+
+def timed_steps(sim, step, steps, torch, per_step_stats=False):
+    """`steps` integration steps bracketed by CUDA events on the library's
+    stream (the current torch stream).  Returns (ms, next step, per-step
+    statistics or None); with per_step_stats every step's status counters are
+    read (one stream synchronisation per step)."""
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = [] if per_step_stats else None
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        sim.integrate(step)
+        step += 1
+        if per_step_stats:
+            stats.append(sim.stats())
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), step, stats
+
+
+def cloud_run(args, wl, variant, learned, torch):
+    """One cloud variant: the same seeded cloud, train_steps warm-up steps (the
+    learned variant trains its predictor on them), one more step, then
+    `cloud_steps` timed steps with per-step statistics; drift of E and L over
+    the timed steps; force error of an extra untimed right-hand side."""
+    import ctypes
+    from miluphpc_b200 import _lib
+    state = plummer_state(wl, 0)
+    w = dict(wl, learned=learned, band_rounds=args.band_rounds)
+    sim = make_sim(w, state, variant)
+    step = 0
+    for _ in range(wl["train_steps"]):
+        sim.integrate(step)
+        step += 1
+    train = None
+    if variant == "mixed" and learned:
+        L = _lib.load()
+        l0, l1 = ctypes.c_float(), ctypes.c_float()
+        t0 = time.perf_counter()
+        _lib.check(L.mhpc_mlp_train(sim.ctx, 1, 1e-3, ctypes.byref(l0)), "mlp_train")
+        _lib.check(L.mhpc_mlp_train(sim.ctx, wl["train_iters"], 1e-3, ctypes.byref(l1)), "mlp_train")
+        train = {"plain_steps": wl["train_steps"], "iters": wl["train_iters"] + 1, "loss_first": l0.value,
+                 "loss_last": l1.value, "seconds": round(time.perf_counter() - t0, 3)}
+    sim.integrate(step)
+    step += 1
+    c0 = cloud_energy(sim, torch)
+    ms, step, st = timed_steps(sim, step, args.cloud_steps, torch, per_step_stats=True)
+    c1 = cloud_energy(sim, torch)
+    n = sim.n
+    h_walk = sim.t["sml"][:n].clone()
+    sim.rhs(step)
+    ferr = force_error(sim, torch, 0.0, h_factor=0.5, h=h_walk)
+    fb = [s["predictor_fallback"] for s in st]
+    ob = [s["sml_out_of_band"] for s in st]
+    obb = [s["sml_band_before"] for s in st]
+    l0n = float(np.linalg.norm(c0["L"]))
+    out = {"ms_per_step": ms / args.cloud_steps, "value": n * args.cloud_steps / (ms / 1e3),
+           "steps": args.cloud_steps, "force_error": ferr,
+           "gravity_theta": wl["theta_mixed"] if variant == "mixed" else wl["theta_plain_matched"],
+           "opening_rule": ("relative, alpha %g (geometric theta %.2f on the first RHS)" % (wl["mac_alpha"],
+                                                                                        wl["theta_mixed"]))
+           if variant == "mixed" else "v2 geometric (FP64)",
+           "sph_pair_sums": "FP32 on hi/lo splits, FP64 accumulation" if variant == "mixed" else "FP64",
+           "learned_h": bool(variant == "mixed" and learned),
+           "band_rule": "reference iteration (max 5 updates, |n - 60| < 5) + %d repair rounds" % w["band_rounds"],
+           "out_of_band_before_repair_rate": float(np.mean(obb)) / n if min(obb) >= 0 else None,
+           "final_out_of_band_rate": float(np.mean(ob)) / n, "final_out_of_band_max": int(max(ob)),
+           "final_out_of_band_last_step": int(ob[-1]),
+           "energy_rel_drift": (c1["E"] - c0["E"]) / abs(c0["E"]),
+           "angular_momentum_rel_drift": float(np.linalg.norm(np.subtract(c1["L"], c0["L"]))) / l0n
+           if l0n > 0 else None,
+           "stages_ms_last_step": {k: round(v, 3) for k, v in st[-1]["ms_stage"].items()}}
+    if variant == "mixed" and learned:
+        out["first_sweep_fallback_rate"] = float(np.mean(fb)) / n
+        out["training"] = train
+    sim.close()
+    return out
+
+
 def run_ours(args, wl):
     import torch
     import torch.distributed as dist
@@ -239,12 +334,18 @@ def run_ours(args, wl):
     e_start = None
     if wl["kind"] == "gravity":
         e_start = sim.diagnostics()["kinetic"] + sim.potential()
-    if wl["kind"] == "cloud" and args.variant == "mixed":
+    learned_on = wl["kind"] == "cloud" and args.variant == "mixed" and wl.get("learned", 1)
+    if wl["kind"] == "cloud":
+        # the same start for every variant: train_steps plain steps (the
+        # learned variant trains on them), then one more step
         warm = max(warm, wl["train_steps"])
     for _ in range(warm):
         sim.integrate(step)
         step += 1
-    if wl["kind"] == "cloud" and args.variant == "mixed":
+    if wl["kind"] == "cloud" and not learned_on:
+        sim.integrate(step)
+        step += 1
+    if learned_on:
         # train on the (features, converged h) pairs of the plain steps, then one
         # more step so that the first timed step starts from predictions
         import ctypes
@@ -263,35 +364,27 @@ def run_ours(args, wl):
         dist.barrier()
     clocks = ClockSampler(local)
     clocks.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    kern_ms, inter, quad = [], 0.0, 0.0
     sph = wl["kind"] == "sph"
-    fallback, out_band, unconv, stage_sum = [], [], [], {}
-    torch.cuda.synchronize()
     # NVTX range "timed": profilers can select the timed steps' launches
-    # (ncu --nvtx --nvtx-include "timed/")
+    # (ncu --nvtx --nvtx-include "timed/"); the timed loop reads no statistics
+    # (no host synchronisation between steps), the last timed step's counters
+    # and stage events are read after it
     torch.cuda.nvtx.range_push("timed")
-    e0.record()
-    for _ in range(args.steps):
-        sim.integrate(step)
-        st = sim.stats()
-        kern_ms.append(st["ms_stage"]["forces" if sph else "gravity"])
-        inter += st["gravity_interactions"]
-        quad += st["gravity_quad_interactions"]
-        fallback.append(st["predictor_fallback"])
-        out_band.append(st["sml_out_of_band"])
-        for k, v in st["ms_stage"].items():
-            stage_sum[k] = stage_sum.get(k, 0.0) + v / args.steps
-        step += 1
-    e1.record()
+    ms, step, per_step = timed_steps(sim, step, args.steps, torch, per_step_stats=wl["kind"] == "cloud")
     torch.cuda.nvtx.range_pop()
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
     clk = clocks.stop()
     value, ms_max = job_rate(ms, n, args.steps, world, dev)
     last = sim.stats()
+    kern_ms = last["ms_stage"]["forces" if sph else "gravity"]
+    inter = last["gravity_interactions"]
+    quad = last["gravity_quad_interactions"]
+    # energy drift over drift_steps steps in all (the steps after the timed
+    # region run untimed)
     energy = None
     if e_start is not None:
+        while step < wl.get("drift_steps", 0):
+            sim.integrate(step)
+            step += 1
         e_end = sim.diagnostics()["kinetic"] + sim.potential()
         energy = {"E_start": e_start, "E_end": e_end, "rel_drift": (e_end - e_start) / abs(e_start),
                   "steps": step, "potential": "tree walk, geometric rule theta_mixed, quadrupoles"}
@@ -308,16 +401,38 @@ def run_ours(args, wl):
         ferr = force_error(sim, torch, 0.0, h_factor=0.5, h=h_walk)
     learned = None
     if wl["kind"] == "cloud":
+        fallback = [s["predictor_fallback"] for s in per_step]
+        out_band = [s["sml_out_of_band"] for s in per_step]
         learned = {"training": train_info, "target_band": "60 +- 5 (|n - 60| < 5)",
+                   "band_repair_rounds": wl.get("band_rounds", 8),
+                   "out_of_band_before_repair_per_step": [s["sml_band_before"] for s in per_step],
                    "first_sweep_fallback_per_step": fallback,
                    "fallback_rate": float(np.mean(fallback)) / n,
                    "final_out_of_band_per_step": out_band,
                    "out_of_band_rate": float(np.mean(out_band)) / n}
     # end to end through the public C ABI with host buffers (pinned)
     e2e = run_e2e(args, wl, sim, state, torch, step)
+    sim.close()
+    del sim
     out = None
+    compare = rank == 0 and world == 1 and not args.no_compare
+    vs_plain = None
+    if compare and wl["kind"] == "gravity":
+        vs_plain = {wl_name(args): plain_compare(args, wl, state, value, ferr, torch)}
+    del state
+    if compare and args.workload == "plummer16m" and args.cloud_steps > 0:
+        vs_plain = vs_plain or {}
+        cw = dict(WORKLOADS["cloud8m"])
+        runs = {"mixed_learned": cloud_run(args, cw, "mixed", 1, torch),
+                "mixed_no_learned": cloud_run(args, cw, "mixed", 0, torch),
+                "plain": cloud_run(args, cw, "plain_matched", 0, torch)}
+        runs["speedup_vs_plain"] = runs["mixed_learned"]["value"] / runs["plain"]["value"]
+        runs["learned_h_gain"] = runs["mixed_learned"]["value"] / runs["mixed_no_learned"]["value"]
+        runs["workload"] = "cloud8m: rotating isothermal cloud N = 2^23, gravity (eps_i = h_i / 2) + SPH, " \
+                           "variable h 60 +- 5, explicit Euler dt %g, %d warm-up steps" % (cw["dt"],
+                                                                                         cw["train_steps"] + 1)
+        vs_plain["cloud8m"] = runs
     if rank == 0:
-        kms = float(np.mean(kern_ms))
         traffic = load_traffic(args.workload, args.variant)
         if sph:
             # internal forces: the particle's own state read once (FP64: x,y,z,v,m,h,rho,p,c_s = 88 B;
@@ -328,7 +443,7 @@ def run_ours(args, wl):
             own = 56.0 if mixed else 88.0
             nb = float(last.get("mean_noi") or 0.0)
             nbytes = (own + 40.0 + 4.0 * nb) * n
-            achieved = nbytes / (kms / 1e3) / 1e9
+            achieved = nbytes / (kern_ms / 1e3) / 1e9
             peak = hbm_peak_gbs()
             roof = {"kernel": "k_forces_f32" if mixed else "k_forces", "bound": "hbm", "achieved": round(achieved, 1),
                     "peak": peak["value"], "unit": "GB/s", "frac": round(achieved / peak["value"], 4),
@@ -336,60 +451,51 @@ def run_ours(args, wl):
                     "work_unit": "%d B state read + 40 B written + 4 B per neighbour-list entry, per particle"
                                  % own,
                     "gathered_bytes_per_launch": round(nb * n * own),
-                    "kernel_ms_per_launch": round(kms, 3), "mean_neighbours": nb}
+                    "kernel_ms_per_launch": round(kern_ms, 3), "mean_neighbours": nb}
         else:
-            flops = (inter * FLOP_MONO + quad * FLOP_QUAD) / args.steps
-            achieved = flops / (kms / 1e3) / 1e12
+            flops = inter * FLOP_MONO + quad * FLOP_QUAD
+            achieved = flops / (kern_ms / 1e3) / 1e12
             peak = fp32_peak_tflops(torch)
             kname = ("k_grav_lists" if wl.get("mixed_precision", 1) == 1 else "k_grav_mixed") \
                 if args.variant == "mixed" else "k_grav_v2"
             roof = {"kernel": kname, "bound": "fp32",
                     "achieved": round(achieved, 3), "peak": round(peak, 3), "unit": "TFLOP/s",
                     "frac": round(achieved / peak, 4) if peak > 0 else None, "traffic": traffic,
-                    "peak_source": "measured on this GPU by mhpc_fp32_peak (dependent FFMA chains)",
+                    "peak_source": "FP32 FMA rate of the paired FFMA2 instruction on every SM "
+                                   "(148 SMs x 128 lanes x 2 flop x the SM clock, measured by mhpc_fp32_peak)",
                     "work_unit": "%d flop per accepted monopole interaction + %d per quadrupole term"
                                  % (FLOP_MONO, FLOP_QUAD),
-                    "kernel_ms_per_launch": round(kms, 3), "interactions_per_launch": inter / args.steps}
+                    "kernel_ms_per_launch": round(kern_ms, 3), "launch": "the last timed step's walk",
+                    "interactions_per_launch": inter}
         # CPU baseline: rank 0 of a single-GPU run only
         cpu = cpu_baseline(wl, args) if (not args.no_cpu_baseline and world == 1) else None
-        if sph:
-            cfg_out = {"workload": args.workload, "n_particles": n, "variant": args.variant,
-                       "integrator": "predictor-corrector", "kernel": "cubic spline", "h": "fixed 2.5 dx",
-                       "dt_max": wl["dt_max"], "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "inputs larger than L2 (state %.0f MB)" % (n * 8 * 14 / 1e6)}
+        method = {"variant": args.variant}
+        if wl["kind"] == "gravity":
+            method["theta"] = wl["theta_mixed"] if args.variant == "mixed" else \
+                (wl["theta_plain_matched"] if args.variant == "plain_matched" else wl["theta"])
+            method["opening_rule"] = ("relative: d >= l and M l^3 <= %g |a_prev| d^5, monopole cells below "
+                                      "%g |a_prev| d^4 / l^2 (geometric theta %.2f on the first RHS)"
+                                      % (wl["mac_alpha"], wl.get("mac_quad_alpha", 0.0), wl["theta_mixed"])) \
+                if args.variant == "mixed" and wl.get("mac_alpha") and wl.get("mixed_precision", 1) == 1 \
+                else "geometric"
         elif wl["kind"] == "cloud":
-            cfg_out = {"workload": args.workload, "n_particles": n, "variant": args.variant,
-                       "gravity_theta": wl["theta_mixed"] if args.variant == "mixed" else
-                       (wl["theta_plain_matched"] if args.variant == "plain_matched" else wl["theta"]),
-                       "softening": "eps_i = h_i / 2", "sph": "cubic spline, isothermal (polytropic gamma 1)",
-                       "variable_h": "target 60 +- 5, Jacobi sweeps" + (" from learned h" if args.variant == "mixed"
-                                                                         else ""),
-                       "sfc": "hilbert", "integrator": "explicit euler", "dt": wl["dt"],
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "inputs larger than L2 (state %.0f MB)" % (n * 8 * 14 / 1e6)}
-        else:
-            cfg_out = {"workload": args.workload, "n_particles": n, "variant": args.variant,
-                       "theta": wl["theta_mixed"] if args.variant == "mixed" else
-                       (wl["theta_plain_matched"] if args.variant == "plain_matched" else wl["theta"]),
-                       "sfc": "hilbert" if wl["sfc"] else "lebesgue", "integrator": "leapfrog", "dt": wl["dt"],
-                       "eps2": wl["eps2"], "parallelism": "replicas" if world > 1 else "single",
-                       "opening_rule": ("relative: d >= l and M l^3 <= %g |a_prev| d^5 (geometric theta %.2f on "
-                                        "the first RHS)" % (wl["mac_alpha"], wl["theta_mixed"]))
-                       if args.variant == "mixed" and wl.get("mac_alpha") and wl.get("mixed_precision", 1) == 1
-                       else "geometric",
-                       "l2": "inputs larger than L2 (positions alone %.0f MB)" % (n * 24 / 1e6)}
+            method["gravity_theta"] = wl["theta_mixed"] if args.variant == "mixed" else \
+                (wl["theta_plain_matched"] if args.variant == "plain_matched" else wl["theta"])
+            method["learned_h"] = bool(learned_on)
         out = {
-            "metric": "particle-steps/s on 1 B200: mixed/learned vs plain at rel. force err <=1e-3",
+            "metric": METRIC,
             "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if args.variant == "mixed" else "f64",
             "data": "synthetic (seeded %s generator, no dataset)" % (
                 {"sph": "Sedov lattice", "cloud": "rotating cloud", "gravity": "Plummer"}[wl["kind"]]),
-            "config": cfg_out,
+            "config": workload_config(args, wl, world),
+            "method": method,
             "force_error": ferr,
             "energy": energy,
             "learned_h": learned,
-            "stages_ms_mean": {k: round(v, 3) for k, v in stage_sum.items()},
+            "vs_plain": vs_plain,
+            "stages_ms_last_step": {k: round(v, 3) for k, v in last["ms_stage"].items()},
             "tree_cells": last["cells"],
             "roofline": roof,
             "cpu_baseline": cpu,
@@ -397,11 +503,55 @@ def run_ours(args, wl):
             "gpu_launches": args.steps * launches_per_step(args.variant, wl["kind"]),
             "clocks": clk,
         }
-    sim.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     return out
+
+
+METRIC = "particle-steps/s on 1 B200: mixed/learned vs plain at rel. force err <=1e-3"
+
+
+def wl_name(args):
+    return args.workload
+
+
+def workload_config(args, wl, world):
+    """The workload (identical in both arms of the bench: this library's and
+    the reference's); the arm's method is reported separately."""
+    n = wl["n"]
+    base = {"workload": args.workload, "n_particles": n, "parallelism": "replicas" if world > 1 else "single",
+            "accuracy": "p99 relative force error <= 1e-3 against FP64 direct summation (4096 seeded targets)"}
+    if wl["kind"] == "sph":
+        base.update({"integrator": "predictor-corrector", "kernel": "cubic spline", "h": "fixed 2.5 dx",
+                     "dt_max": wl["dt_max"], "l2": "inputs larger than L2 (state %.0f MB)" % (n * 8 * 14 / 1e6)})
+    elif wl["kind"] == "cloud":
+        base.update({"softening": "eps_i = h_i / 2", "sph": "cubic spline, isothermal (polytropic gamma 1)",
+                     "variable_h": "target 60 +- 5", "sfc": "hilbert", "integrator": "explicit euler",
+                     "dt": wl["dt"], "l2": "inputs larger than L2 (state %.0f MB)" % (n * 8 * 14 / 1e6)})
+    else:
+        base.update({"sfc": "hilbert" if wl["sfc"] else "lebesgue", "integrator": "leapfrog", "dt": wl["dt"],
+                     "eps2": wl["eps2"], "l2": "inputs larger than L2 (positions alone %.0f MB)" % (n * 24 / 1e6)})
+    return base
+
+
+def plain_compare(args, wl, state, mixed_value, mixed_ferr, torch):
+    """The plain FP64 walk (computeForces_v2 semantics) on the same workload
+    at the opening parameter whose p99 force error matches the mixed run's."""
+    sim = make_sim(wl, state, "plain_matched")
+    step = 0
+    for _ in range(max(1, args.plain_warmup)):
+        sim.integrate(step)
+        step += 1
+    ms, step, _ = timed_steps(sim, step, args.plain_steps, torch)
+    ferr = force_error(sim, torch, wl["eps2"])
+    sim.close()
+    value = wl["n"] * args.plain_steps / (ms / 1e3)
+    return {"mixed": {"value": mixed_value, "force_error_p99": mixed_ferr["p99"] if mixed_ferr else None},
+            "plain": {"value": value, "ms_per_step": ms / args.plain_steps, "steps": args.plain_steps,
+                      "theta": wl["theta_plain_matched"], "force_error": ferr, "walk": "FP64 v2 (warp vote)"},
+            "speedup_vs_plain": mixed_value / value,
+            "p99_ratio_plain_over_mixed": (ferr["p99"] / mixed_ferr["p99"]) if mixed_ferr else None}
 
 
 def hbm_peak_gbs():
@@ -564,12 +714,13 @@ def run_reference(args, wl):
     value = float(np.median(per_step))
     return {
         "impl": "reference",
-        "metric": "particle-steps/s on 1 B200: mixed/learned vs plain at rel. force err <=1e-3",
+        "metric": METRIC,
         "value": value, "unit": "particle-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded Plummer sampler, no dataset)",
-        "config": {"workload": args.workload, "n_particles": wl["n"], "variant": "reference v2 FP64 (oracle port)",
-                   "theta": wl["theta_plain_matched"], "sfc": "hilbert" if wl["sfc"] else "lebesgue"},
+        "ms_per_step": 1e3 * wl["n"] / value, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded Plummer sampler, no dataset)",
+        "config": workload_config(args, wl, world),
+        "method": {"variant": "reference algorithm (computeForces_v2 semantics, FP64) restated by the CPU oracle",
+                   "theta": wl["theta_plain_matched"], "opening_rule": "geometric"},
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cb["cores"], "kind": "port",
                          "sample": cb["sample"]},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -586,6 +737,12 @@ def main():
     ap.add_argument("--variant", default="mixed", choices=["mixed", "plain", "plain_matched"])
     ap.add_argument("--cpu-sample-groups", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the plain FP64 comparison runs (single-GPU runs only make them)")
+    ap.add_argument("--plain-steps", type=int, default=3, help="timed steps of the plain FP64 comparison")
+    ap.add_argument("--plain-warmup", type=int, default=1)
+    ap.add_argument("--cloud-steps", type=int, default=100,
+                    help="timed steps of each cloud8m comparison run (0: no cloud comparison)")
     ap.add_argument("--theta-mixed", type=float, default=None, help="override the mixed walk's opening parameter")
     ap.add_argument("--theta-plain", type=float, default=None,
                     help="override the accuracy-matched opening parameter of the plain FP64 walk")
@@ -593,6 +750,9 @@ def main():
                     help="relative opening rule of the list walk (0: geometric rule only)")
     ap.add_argument("--mac-quad-alpha", type=float, default=None,
                     help="relative rule: cells with a small quadrupole term enter as monopoles (0: never)")
+    ap.add_argument("--learned", type=int, default=1, help="cloud workloads, mixed variant: learned-h predictor on/off")
+    ap.add_argument("--band-rounds", type=int, default=8,
+                    help="cloud workloads: neighbour-band repair rounds after the variable-h iteration (0: none)")
     ap.add_argument("--mixed-walk", default="lists", choices=["lists", "vote"],
                     help="mixed walk: interaction lists (precision 1) or per-lane vote (precision 2)")
     args = ap.parse_args()
@@ -606,6 +766,8 @@ def main():
     if args.theta_plain is not None:
         wl["theta_plain_matched"] = args.theta_plain
     wl["mixed_precision"] = 1 if args.mixed_walk == "lists" else 2
+    wl["learned"] = args.learned
+    wl["band_rounds"] = args.band_rounds
     if args.impl == "reference":
         out = run_reference(args, wl)
     else:

@@ -95,6 +95,12 @@ typedef struct mhpc_config {
     double mac_quad_alpha;     /* relative rule only: an accepted cell whose quadrupole term is small,
                                   M l^2 <= mac_quad_alpha |a| d^4 for every sub-box, enters as a monopole
                                   (0: every accepted cell with its quadrupole) */
+    int sml_band_rounds;       /* variable h: rounds of the neighbour-band repair after the reference's
+                                  iteration (0: none, the reference's behaviour).  Each round, every
+                                  particle whose final count misses |n - target| < tol takes, with the
+                                  other h frozen, the h giving it target + tol - 2 (from above) or
+                                  target - tol + 2 (from below) neighbours; lists and counts are updated
+                                  pair by pair.  Not in the reference. */
 } mhpc_config;
 
 /* Material (include/materials/material.cuh:123-150), one entry of the
@@ -169,7 +175,11 @@ int mhpc_sort_pairs(const uint64_t* keys_in, const int* vals_in, uint64_t* keys_
  * (about 16 MB, held on every GPU that loads the library until the process
  * exits).  Larger n returns MHPC_ERR_CAPACITY.  The first call on a device
  * looks up the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture.  All calls share
+ * current; make that first call before any stream capture.  The address is
+ * kept for the life of the process: after cudaDeviceReset (or anything else
+ * that destroys and recreates the device's primary context) the library's
+ * module may load at another address, so do not call this entry point on that
+ * device again in the same process.  All calls share
  * the one array, so calls whose work overlaps on the GPU (other streams, other
  * host threads) race and must be serialised by the caller.  status_dev
  * (optional, device int) receives MHPC_OK or MHPC_ERR_TIMEOUT in stream order.
@@ -184,7 +194,11 @@ typedef struct mhpc_ctx mhpc_ctx;
 
 /* Allocates every workspace buffer for up to `capacity` particles once
  * (replaces the handlers' cudaMalloc, src/particle_handler.cpp:148+ and
- * src/subdomain_key_tree/tree_handler.cpp:6-36); no call below allocates. */
+ * src/subdomain_key_tree/tree_handler.cpp:6-36).  No call below allocates
+ * device memory, with two stated exceptions: mhpc_integrate_host allocates its
+ * device mirror of the state on its first call, and mhpc_fp32_peak allocates
+ * and frees a small buffer.  A gravity context also holds 4 * capacity
+ * doubles for mhpc_potential. */
 int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg,
                     const mhpc_material* materials, int num_materials);
 int mhpc_ctx_destroy(mhpc_ctx* ctx);
@@ -195,10 +209,12 @@ int mhpc_ctx_set_config(mhpc_ctx* ctx, const mhpc_config* cfg);
  * (include/miluphpc.h:478, src/miluphpc.cpp:387-562) on one GPU: bbox, keys,
  * sort, tree, centres of mass, gravity (if cfg->gravity && self_gravity),
  * SPH neighbour search, density, sound speed, pressure and internal forces
- * (if cfg->sph).  Results land in the SoA.  Synchronises the stream once at
- * the end to read the device status word; *ms_out (optional) receives the
- * device time of the call. */
-int mhpc_rhs(mhpc_ctx* ctx, const mhpc_particles* p, int step, int self_gravity, float* ms_out);
+ * (if cfg->sph).  Results land in the SoA.  Runs on `stream`, which becomes
+ * the context's stream (as mhpc_ctx_set_stream).  Synchronises the stream
+ * once at the end to read the device status word; *ms_out (optional)
+ * receives the device time of the call (the reference's rhs() returns the
+ * summed kernel milliseconds). */
+int mhpc_rhs(mhpc_ctx* ctx, const mhpc_particles* p, int step, int self_gravity, void* stream, float* ms_out);
 /* Same without the final synchronisation: the status is read by
  * mhpc_ctx_status().  Capturable into a CUDA graph. */
 int mhpc_rhs_async(mhpc_ctx* ctx, const mhpc_particles* p, int step, int self_gravity);
@@ -215,10 +231,69 @@ int mhpc_integrate(mhpc_ctx* ctx, const mhpc_particles* p, int step, double* dt_
  * context's device mirror (allocated on first use). */
 int mhpc_integrate_host(mhpc_ctx* ctx, mhpc_particles* host, int step, double* dt_out);
 
-/* Sub-stages (the reference's Launch:: wrappers), stream-ordered, no sync. */
-int mhpc_stage_tree(mhpc_ctx* ctx, const mhpc_particles* p);    /* bbox+keys+sort+tree+COM */
-int mhpc_stage_gravity(mhpc_ctx* ctx, const mhpc_particles* p); /* needs stage_tree */
-int mhpc_stage_sph(mhpc_ctx* ctx, const mhpc_particles* p);     /* needs stage_tree */
+/* Sub-stages, one per group of the reference's Launch:: wrappers (which
+ * take the device Tree / Particles and return kernel milliseconds after a
+ * device synchronisation, include/cuda_utils/cuda_launcher.cuh:114-141).
+ * Here each is stream-ordered on the context's stream with no
+ * synchronisation; the status word is read by mhpc_ctx_status().  Called in
+ * the order below they make up mhpc_rhs_async; a call whose inputs the
+ * previous stages did not produce for this particle count returns
+ * MHPC_ERR_ARG.  mhpc_bbox, mhpc_keys and mhpc_sort_pairs above are the
+ * stateless forms of the first three steps. */
+/* bbox (TreeNS::computeBoundingBox, tree.cu:302-437), keys (getParticleKeys,
+ * subdomain.cu:849-894), sort (sortArray, helper.cu:150-166), gather into
+ * SFC order, and the octree (TreeNS::buildTree, tree.cu:768-1082); resets the
+ * status word as the start of a right-hand side. */
+int mhpc_tree_build(mhpc_ctx* ctx, const mhpc_particles* p);
+/* TreeNS::calculateCentersOfMass (tree.cu:1416-1497, all levels), with the
+ * mixed walks' quadrupoles and node records (gravity contexts whose
+ * precision is >= 1) and the node boxes / largest h below each node (SPH). */
+int mhpc_com(mhpc_ctx* ctx, const mhpc_particles* p);
+/* Gravity::computeForces_v2 / _v1 (gravity.cu:726-903 / 252-396) or the
+ * mixed walk: precision -1 the configured one, 0 plain FP64
+ * (gravity_force_version selects v2 or v1), 1 interaction lists, 2 per-lane
+ * vote; 1 and 2 need a context whose configured precision is >= 1. */
+int mhpc_gravity(mhpc_ctx* ctx, const mhpc_particles* p, int precision);
+/* SPH::fixedRadiusNN_variableSML (sph.cu:739-961, Jacobi form) when
+ * variable_h, started from the learned prediction when predictor (the
+ * context needs cfg->learned_h), then SPH::fixedRadiusNN (sph.cu:93-281). */
+int mhpc_frnn(mhpc_ctx* ctx, const mhpc_particles* p, int variable_h, int predictor);
+/* calculateDensity (density.cu:8-72), calculateSoundSpeed (soundspeed.cu:
+ * 38-97), calculatePressure (pressure.cu:5-87), and the Balsara factors
+ * (kernel.cu:223-342) when configured. */
+int mhpc_density_eos(mhpc_ctx* ctx, const mhpc_particles* p);
+/* SPH::Kernel::internalForces (internal_forces.cu:4-668); also writes nnl /
+ * noi when the SoA has them, the band statistic, and the learned features. */
+int mhpc_forces(mhpc_ctx* ctx, const mhpc_particles* p);
+/* Coarser groupings of the same stages. */
+int mhpc_stage_tree(mhpc_ctx* ctx, const mhpc_particles* p);    /* mhpc_tree_build + mhpc_com */
+int mhpc_stage_gravity(mhpc_ctx* ctx, const mhpc_particles* p); /* mhpc_gravity(ctx, p, -1) */
+int mhpc_stage_sph(mhpc_ctx* ctx, const mhpc_particles* p);     /* frnn + density_eos + forces as configured */
+
+/* Integrator update kernels alone (no right-hand side), FP64, stream-ordered
+ * on the context's stream, with the context's physics switches.
+ * half 0: LeapfrogNS::Kernel::updateX (device_leapfrog.cu:4-30), drift and
+ * g_a_old = g_a; half 1: updateV (device_leapfrog.cu:32-58), kick with the
+ * mean of g_a and g_a_old. */
+int mhpc_integrate_leapfrog(mhpc_ctx* ctx, const mhpc_particles* p, double dt, int half);
+/* ExplicitEulerNS::Kernel::update (device_explicit_euler.cu:4-54). */
+int mhpc_integrate_euler(mhpc_ctx* ctx, const mhpc_particles* p, double dt);
+/* PredictorCorrectorEulerNS::Kernel::setTimeStep (device_predictor_corrector_
+ * euler.cu:300-470): the step size, capped by max_time_step and time_left,
+ * into *dt_dev (device).  Reads g_a (gravity), a, c_s, rho, drho/dt (SPH),
+ * h and v of every particle. */
+int mhpc_integrate_pc_step_size(mhpc_ctx* ctx, const mhpc_particles* p, double time_left, double* dt_dev);
+/* PredictorCorrectorEulerNS::Kernel::predictor (device_predictor_corrector_
+ * euler.cu:206-270): the Euler-predicted state of p into q (the reference's
+ * IntegratedParticles) with the step *dt_dev; g_a is read (zero arrays
+ * without gravity, as in the reference). */
+int mhpc_integrate_pc_predictor(mhpc_ctx* ctx, const mhpc_particles* p, const mhpc_particles* q,
+                                const double* dt_dev);
+/* PredictorCorrectorEulerNS::Kernel::corrector (device_predictor_corrector_
+ * euler.cu:130-205): p advanced with the mean of its rates and those of q
+ * (the right-hand side evaluated on q). */
+int mhpc_integrate_pc_corrector(mhpc_ctx* ctx, const mhpc_particles* p, const mhpc_particles* q,
+                                const double* dt_dev);
 
 /* Parity exports (synchronise the stream). */
 /* Sorted keys and the permutation tree->sorted (device pointers, n entries). */
@@ -248,7 +323,11 @@ typedef struct mhpc_stats {
     int sml_out_of_band;       /* particles whose final count misses the band */
     int predictor_used;        /* particles whose learned h was accepted */
     int predictor_fallback;    /* particles that fell back to the plain iteration */
-    float ms_stage[12];        /* bbox_keys, sort, tree, com, gravity, frnn, sml, density, forces, integrate, mlp, other */
+    float ms_stage[12];        /* bbox_keys, sort, tree, com, gravity, frnn (list walk), sml (variable-h
+                                  iteration), density, forces, band (band repair), unused, total */
+    int sml_band_before;       /* particles out of the band before the band repair (-1: no repair ran) */
+    int sml_band_skipped;      /* band repair rounds skipped because their pair changes overflowed the
+                                  event buffer (4 per particle) */
 } mhpc_stats;
 int mhpc_get_stats(mhpc_ctx* ctx, mhpc_stats* out);
 
@@ -295,8 +374,9 @@ int mhpc_direct_gravity_soft(const double* x, const double* y, const double* z, 
                              const int* targets, int nt, double eps2, const double* eps2_targets, double* gax,
                              double* gay, double* gaz, void* stream);
 
-/* Measured FP32 FMA throughput of the current device in TFLOP/s (dependent
- * FFMA chains on every SM; the roofline denominator of the FP32 walk).
+/* Measured FP32 FMA throughput of the current device in TFLOP/s (independent
+ * chains of the paired FFMA2 instruction, the form the mixed walk issues, on
+ * every SM; the roofline denominator of the FP32 walk).
  * Allocates and frees a small buffer; synchronises. */
 int mhpc_fp32_peak(double* tflops);
 

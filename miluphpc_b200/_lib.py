@@ -42,6 +42,7 @@ class Config(ctypes.Structure):
         ("precision", c_int), ("theta_mixed", c_double), ("learned_h", c_int), ("softening_mode", c_int),
         ("softening_h_factor", c_double), ("node_pool_factor", c_double),
         ("gravity_mac", c_int), ("mac_alpha", c_double), ("balsara", c_int), ("mac_quad_alpha", c_double),
+        ("sml_band_rounds", c_int),
     ]
 
 
@@ -72,11 +73,12 @@ class Stats(ctypes.Structure):
         ("bbox", c_double * 6), ("radius", c_double), ("gravity_interactions", c_double),
         ("gravity_nodes_visited", c_double), ("gravity_quad_interactions", c_double), ("max_noi", c_int), ("mean_noi", c_double),
         ("sml_sweeps", c_int), ("sml_out_of_band", c_int), ("predictor_used", c_int),
-        ("predictor_fallback", c_int), ("ms_stage", c_float * 12),
+        ("predictor_fallback", c_int), ("ms_stage", c_float * 12), ("sml_band_before", c_int),
+        ("sml_band_skipped", c_int),
     ]
 
 
-STAGES = ["bbox_keys", "sort", "tree", "com", "gravity", "frnn", "sml", "density", "forces", "integrate", "mlp",
+STAGES = ["bbox_keys", "sort", "tree", "com", "gravity", "frnn", "sml", "density", "forces", "band", "unused",
           "total"]
 
 _lib = None
@@ -110,7 +112,7 @@ def load():
     L.mhpc_ctx_destroy.argtypes = [c_void_p]
     L.mhpc_ctx_set_stream.argtypes = [c_void_p, c_void_p]
     L.mhpc_ctx_set_config.argtypes = [c_void_p, ctypes.POINTER(Config)]
-    L.mhpc_rhs.argtypes = [c_void_p, ctypes.POINTER(Particles), c_int, c_int, P_f]
+    L.mhpc_rhs.argtypes = [c_void_p, ctypes.POINTER(Particles), c_int, c_int, c_void_p, P_f]
     L.mhpc_rhs_async.argtypes = [c_void_p, ctypes.POINTER(Particles), c_int, c_int]
     L.mhpc_ctx_status.argtypes = [c_void_p]
     L.mhpc_integrate.argtypes = [c_void_p, ctypes.POINTER(Particles), c_int, P_d]
@@ -118,6 +120,16 @@ def load():
     L.mhpc_stage_tree.argtypes = [c_void_p, ctypes.POINTER(Particles)]
     L.mhpc_stage_gravity.argtypes = [c_void_p, ctypes.POINTER(Particles)]
     L.mhpc_stage_sph.argtypes = [c_void_p, ctypes.POINTER(Particles)]
+    PP = ctypes.POINTER(Particles)
+    for f in ("mhpc_tree_build", "mhpc_com", "mhpc_density_eos", "mhpc_forces"):
+        getattr(L, f).argtypes = [c_void_p, PP]
+    L.mhpc_gravity.argtypes = [c_void_p, PP, c_int]
+    L.mhpc_frnn.argtypes = [c_void_p, PP, c_int, c_int]
+    L.mhpc_integrate_leapfrog.argtypes = [c_void_p, PP, c_double, c_int]
+    L.mhpc_integrate_euler.argtypes = [c_void_p, PP, c_double]
+    L.mhpc_integrate_pc_step_size.argtypes = [c_void_p, PP, c_double, c_void_p]
+    L.mhpc_integrate_pc_predictor.argtypes = [c_void_p, PP, PP, c_void_p]
+    L.mhpc_integrate_pc_corrector.argtypes = [c_void_p, PP, PP, c_void_p]
     L.mhpc_export_sorted.argtypes = [c_void_p, c_void_p, c_void_p]
     L.mhpc_export_tree.argtypes = [c_void_p, c_int, P_i, P_i, P_d, P_d, P_d, P_d, P_i]
     L.mhpc_get_stats.argtypes = [c_void_p, ctypes.POINTER(Stats)]
@@ -165,4 +177,7 @@ EXPORTS = [
     "mhpc_diagnostics", "mhpc_potential", "mhpc_direct_gravity", "mhpc_fp32_peak", "mhpc_mlp_reset", "mhpc_mlp_train", "mhpc_mlp_num_params",
     "mhpc_mlp_forward_backward", "mhpc_mlp_get_params", "mhpc_mlp_set_params",
     "mhpc_remove_particles", "mhpc_direct_gravity_soft",
+    "mhpc_tree_build", "mhpc_com", "mhpc_gravity", "mhpc_frnn", "mhpc_density_eos", "mhpc_forces",
+    "mhpc_integrate_leapfrog", "mhpc_integrate_euler", "mhpc_integrate_pc_step_size",
+    "mhpc_integrate_pc_predictor", "mhpc_integrate_pc_corrector",
 ]

@@ -27,7 +27,9 @@ struct DevStatus {
     int predictor_fallback;
     int sml_unconverged;
     unsigned long long quad_interactions;  // accepted cells with a quadrupole term
-    int pad[4];
+    int sml_band_before;                   // out-of-band particles before the band repair
+    int sml_band_skipped;                  // band repair rounds skipped (event buffer full)
+    int pad[2];
 };
 
 __device__ __forceinline__ void set_status(DevStatus* st, int code, int detail) {

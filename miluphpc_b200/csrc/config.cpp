@@ -161,6 +161,23 @@ double num(const std::shared_ptr<Val>& g, const char* key, double def) {
     return std::atof(it->second->s.c_str());
 }
 
+// libconfig literal types: a float has a decimal point or an exponent
+bool is_float_literal(const std::string& w) {
+    if (w.empty()) return false;
+    bool digit = false;
+    for (char c : w) digit |= std::isdigit((unsigned char)c) != 0;
+    return digit && (w.find('.') != std::string::npos || w.find('e') != std::string::npos ||
+                     w.find('E') != std::string::npos);
+}
+
+bool is_int_literal(const std::string& w) {
+    size_t i = (!w.empty() && (w[0] == '-' || w[0] == '+')) ? 1 : 0;
+    if (i >= w.size()) return false;
+    for (; i < w.size(); ++i)
+        if (!std::isdigit((unsigned char)w[i])) return false;
+    return true;
+}
+
 std::shared_ptr<Val> sub(const std::shared_ptr<Val>& g, const char* key) {
     if (!g || g->kind != Val::Group) return nullptr;
     auto it = g->g.find(key);
@@ -196,6 +213,7 @@ void mhpc_config_default(mhpc_config* c) {
     c->mac_alpha = 0.003;
     c->balsara = 0;
     c->mac_quad_alpha = 0.0;
+    c->sml_band_rounds = 0;
 }
 
 int mhpc_config_from_info(const char* path, mhpc_config* c) {
@@ -242,6 +260,8 @@ int mhpc_config_from_info(const char* path, mhpc_config* c) {
     f("macAlpha", &c->mac_alpha);
     b("balsaraSwitch", &c->balsara);
     f("macQuadAlpha", &c->mac_quad_alpha);
+    i("smlBandRounds", &c->sml_band_rounds);
+    if (c->sml_band_rounds < 0) return MHPC_ERR_CONFIG;
     if (c->gravity_mac < 0 || c->gravity_mac > 1 || (c->gravity_mac == 1 && c->mac_alpha <= 0))
         return MHPC_ERR_CONFIG;
     if (c->integrator < 0 || c->integrator > 2 || c->sfc < 0 || c->sfc > 1 || c->theta <= 0 ||
@@ -273,24 +293,42 @@ int mhpc_materials_from_cfg(const char* path, mhpc_material* out, int cap, int* 
         if (id > maxid) maxid = id;
     }
     if (maxid != nmat - 1 || nmat > cap) return MHPC_ERR_CONFIG;
+    // The reference reads every float through one variable `temp` declared
+    // before the loop over materials (material_handler.cpp:80-134) with
+    // libconfig's config_setting_lookup_float, which leaves it unchanged when
+    // the setting is missing or is not a float (an integer literal, without
+    // libconfig's auto-convert option): such a field takes the value of the
+    // previous float read.  Integer fields (ID, interactions, eos type) are
+    // read with config_setting_lookup_int, which likewise needs an integer
+    // literal and otherwise leaves the field as it was (zero here).
+    double temp = 0.0;
+    auto lookup_float = [&](const std::shared_ptr<Val>& g, const char* key) {
+        auto v = sub(g, key);
+        if (v && v->kind == Val::Scalar && is_float_literal(v->s)) temp = std::atof(v->s.c_str());
+        return temp;
+    };
+    auto lookup_int = [&](const std::shared_ptr<Val>& g, const char* key) {
+        auto v = sub(g, key);
+        return (v && v->kind == Val::Scalar && is_int_literal(v->s)) ? std::atoi(v->s.c_str()) : 0;
+    };
     for (auto& m : mats->l) {
         int id = (int)num(m, "ID", 0);
         mhpc_material& o = out[id];
         std::memset(&o, 0, sizeof(o));
         o.id = id;
-        o.interactions = (int)num(m, "interactions", 0);
-        o.sml = num(m, "sml", 0.0);
+        o.interactions = lookup_int(m, "interactions");
+        o.sml = lookup_float(m, "sml");
         auto av = sub(m, "artificial_viscosity");
-        o.alpha = num(av, "alpha", 0.0);
-        o.beta = num(av, "beta", 0.0);
+        o.alpha = lookup_float(av, "alpha");
+        o.beta = lookup_float(av, "beta");
         auto eos = sub(m, "eos");
-        o.eos_type = (int)num(eos, "type", 0);
-        o.polytropic_K = num(eos, "polytropic_K", 0.0);
-        o.polytropic_gamma = num(eos, "polytropic_gamma", 0.0);
-        o.rho_0 = num(eos, "rho_0", 0.0);
-        o.bulk_modulus = num(eos, "bulk_modulus", 0.0);
-        o.n = num(eos, "n", 0.0);
-        o.shear_modulus = num(eos, "shear_modulus", 0.0);
+        o.eos_type = lookup_int(eos, "type");
+        o.polytropic_K = lookup_float(eos, "polytropic_K");
+        o.polytropic_gamma = lookup_float(eos, "polytropic_gamma");
+        o.rho_0 = lookup_float(eos, "rho_0");
+        o.bulk_modulus = lookup_float(eos, "bulk_modulus");
+        o.n = lookup_float(eos, "n");
+        o.shear_modulus = lookup_float(eos, "shear_modulus");
     }
     *count = nmat;
     return MHPC_OK;

@@ -19,7 +19,8 @@
 #include "sph.cuh"
 #include "tree.cuh"
 
-enum Stage { EV_START, EV_KEYS, EV_SORT, EV_TREE, EV_COM, EV_GRAV, EV_SML, EV_FRNN, EV_DENS, EV_FORCES, EV_END, EV_COUNT };
+enum Stage { EV_START, EV_KEYS, EV_SORT, EV_TREE, EV_COM, EV_GRAV, EV_SML, EV_LISTS, EV_FRNN, EV_DENS, EV_FORCES, EV_END,
+             EV_COUNT };
 
 struct mhpc_ctx {
     int cap = 0, cell_cap = 0, cap_nodes = 0, maxnb = 180;
@@ -57,6 +58,18 @@ struct mhpc_ctx {
     cudaEvent_t ev[EV_COUNT];
     bool ev_recorded[EV_COUNT];
     bool first_rhs_done = false;
+    // stage bookkeeping for the per-stage exports: particle count of the last
+    // tree build and of the last neighbour lists, multipoles present, the last
+    // neighbour search started from the learned prediction
+    int tree_n = -1, lists_n = -1;
+    bool com_ready = false, quad_ready = false, frnn_learned = false;
+    // neighbour-band repair: pair-change events, their counters, and whether
+    // the last neighbour search ran the repair
+    int2* band_ev = nullptr;
+    int band_cap = 0;
+    int* band_ctr = nullptr;
+    double* band_h0 = nullptr;
+    bool band_ran = false;
     // particle count of the last gravity walk, -1 before the first: the
     // relative opening rule reads that walk's accelerations from g_ax/g_ay/g_az
     int grav_prev_n = -1;
@@ -142,6 +155,9 @@ void record(mhpc_ctx* c, int e) {
     c->ev_recorded[e] = true;
 }
 
+// softening_mode 1 with a positive factor: eps_i = softening_h_factor * h_i
+bool h_softening(const mhpc_config& cfg) { return cfg.softening_mode == 1 && cfg.softening_h_factor > 0.0; }
+
 int check_particles(const mhpc_ctx* c, const mhpc_particles* p) {
     if (!p) return MHPC_ERR_ARG;
     if (p->n < 0) return MHPC_ERR_ARG;
@@ -149,13 +165,16 @@ int check_particles(const mhpc_ctx* c, const mhpc_particles* p) {
     if (p->n == 0) return MHPC_OK;
     if (!p->x || !p->y || !p->z || !p->mass) return MHPC_ERR_ARG;
     if (c->cfg.gravity && (!p->g_ax || !p->g_ay || !p->g_az)) return MHPC_ERR_ARG;
+    // h-tied softening reads every particle's smoothing length
+    if (c->cfg.gravity && h_softening(c->cfg) && !p->sml) return MHPC_ERR_ARG;
     if (c->cfg.sph && (!p->sml || !p->rho || !p->p || !p->cs || !p->ax || !p->ay || !p->az || !p->vx || !p->vy ||
                        !p->vz || !p->e))
         return MHPC_ERR_ARG;
     return MHPC_OK;
 }
 
-int stage_tree(mhpc_ctx* c, const mhpc_particles* p) {
+// bounding box, keys, sort, gather into SFC order, tree build
+int stage_tree_build(mhpc_ctx* c, const mhpc_particles* p) {
     const int n = p->n;
     cudaStream_t s = c->stream;
     TRY(launch_bbox(p->x, p->y, p->z, n, c->ord, c->st, s));
@@ -170,41 +189,65 @@ int stage_tree(mhpc_ctx* c, const mhpc_particles* p) {
     double* dst[] = {c->sx, c->sy, c->sz, c->sm};
     for (int a = 0; a < 4; ++a) { L.src[a] = src[a]; L.dst[a] = dst[a]; }
     L.count = 4;
-    if (c->cfg.sph || (c->cfg.gravity && c->cfg.softening_h_factor > 0.0 && p->sml)) {
+    if (c->cfg.sph || (c->cfg.gravity && h_softening(c->cfg))) {
         L.src[L.count] = p->sml; L.dst[L.count++] = c->sh;
     }
     if (c->cfg.sph) {
         const double* s2[] = {p->vx, p->vy, p->vz, p->e, p->rho, p->p, p->cs};
         double* d2[] = {c->svx, c->svy, c->svz, c->se, c->srho, c->sp, c->scs};
         for (int a = 0; a < 7; ++a) { L.src[L.count] = s2[a]; L.dst[L.count++] = d2[a]; }
-        if (p->material_id) { L.isrc = p->material_id; L.idst = c->smat; }
+        if (p->material_id) {
+            // ids index the material table: out-of-range ids are an argument error
+            L.isrc = p->material_id; L.idst = c->smat; L.imax = c->nmat; L.st = c->st;
+        }
     }
     TRY(launch_gather(n, c->perm, L, s));
     c->T.n = n;
     TRY(tree_build(c->T, c->skey, c->scan_scratch, c->st, s));
     record(c, EV_TREE);
-    const int want_quad = c->cfg.gravity && (c->cfg.precision >= 1 || c->force_wrec);
-    TRY(tree_upward(c->T, c->sx, c->sy, c->sz, c->sm, want_quad, c->cfg.sph ? 1 : 0, c->ord, c->cfg.theta_mixed,
-                    c->st, s));
-    record(c, EV_COM);
+    c->tree_n = n;
+    c->com_ready = c->quad_ready = false;
     return MHPC_OK;
 }
 
-int stage_gravity(mhpc_ctx* c, const mhpc_particles* p) {
+// TreeNS::Kernel::calculateCentersOfMass (src/subdomain_key_tree/tree.cu:1416-1497)
+// for all levels, plus the mixed walks' multipoles and walk records and the
+// SPH node boxes, on the tree of the last stage_tree_build
+int stage_com(mhpc_ctx* c) {
+    const int want_quad = c->cfg.gravity && (c->cfg.precision >= 1 || c->force_wrec);
+    TRY(tree_upward(c->T, c->sx, c->sy, c->sz, c->sm, want_quad, c->cfg.sph ? 1 : 0, c->ord, c->cfg.theta_mixed,
+                    c->st, c->stream));
+    record(c, EV_COM);
+    c->com_ready = true;
+    c->quad_ready = want_quad;
+    return MHPC_OK;
+}
+
+int stage_tree(mhpc_ctx* c, const mhpc_particles* p) {
+    TRY(stage_tree_build(c, p));
+    return stage_com(c);
+}
+
+// precision: -1 the configured one, otherwise 0 plain FP64, 1 interaction
+// lists, 2 per-lane vote (the mixed walks need the multipoles of stage_com)
+int stage_gravity(mhpc_ctx* c, const mhpc_particles* p, int precision = -1) {
+    if (precision < 0) precision = c->cfg.precision;
+    if (precision > 2) return MHPC_ERR_ARG;
+    if (precision >= 1 && !c->quad_ready) return MHPC_ERR_ARG;
     GravParams G;
     std::memset(&G, 0, sizeof(G));
     G.n = p->n;
     G.eps2 = c->cfg.smoothing;
-    G.h_factor = (c->cfg.softening_mode == 1) ? c->cfg.softening_h_factor : 0.0;
+    G.h_factor = h_softening(c->cfg) ? c->cfg.softening_h_factor : 0.0;
     G.G = c->cfg.si_units ? 6.67430e-11 : 1.0;
     G.ord = c->ord;
-    if (c->cfg.precision == 1) {
+    if (precision == 1) {
         G.theta = c->cfg.theta_mixed;
         G.rel_alpha = (c->cfg.gravity_mac == 1 && c->grav_prev_n == p->n) ? c->cfg.mac_alpha : 0.0;
         G.quad_alpha = G.rel_alpha > 0.0 ? c->cfg.mac_quad_alpha : 0.0;
         TRY(gravity_lists(c->T, G, c->sx, c->sy, c->sz, c->sh, c->perm, p->g_ax, p->g_ay, p->g_az, c->st,
                           c->stream));
-    } else if (c->cfg.precision == 2) {
+    } else if (precision == 2) {
         G.theta = c->cfg.theta_mixed;
         TRY(gravity_mixed(c->T, G, c->sx, c->sy, c->sz, c->sh, c->perm, p->g_ax, p->g_ay, p->g_az, c->st,
                           c->stream));
@@ -221,13 +264,28 @@ int stage_gravity(mhpc_ctx* c, const mhpc_particles* p) {
     return MHPC_OK;
 }
 
-int stage_sph(mhpc_ctx* c, const mhpc_particles* p) {
+int sph_target(const mhpc_ctx* c) { return c->mats[0].interactions > 0 ? c->mats[0].interactions : 50; }
+
+SphSorted sph_sorted(mhpc_ctx* c, const mhpc_particles* p) {
+    SphSorted S;
+    S.x = c->sx; S.y = c->sy; S.z = c->sz; S.m = c->sm; S.h = c->sh;
+    S.vx = c->svx; S.vy = c->svy; S.vz = c->svz; S.e = c->se;
+    S.mat = p->material_id ? c->smat : nullptr;
+    S.rho = c->srho; S.p = c->sp; S.cs = c->scs; S.bal = c->sbal;
+    S.f0 = c->sf0; S.f1 = c->sf1; S.f2 = c->sf2; S.f3 = c->sf3;
+    return S;
+}
+
+// SPH::fixedRadiusNN_variableSML (src/sph/sph.cu:739-961, Jacobi form) when
+// variable_h, starting from the learned prediction when `predictor`, then
+// SPH::fixedRadiusNN (src/sph/sph.cu:93-281): the neighbour lists
+int stage_frnn(mhpc_ctx* c, const mhpc_particles* p, bool variable_h, bool learned) {
     const int n = p->n;
     cudaStream_t s = c->stream;
     SphParams P = sph_params(c, n);
-    const int target = c->mats[0].interactions > 0 ? c->mats[0].interactions : 50;
-    const bool learned = c->cfg.learned_h && c->mlp;
-    if (c->cfg.variable_sml) {
+    const int target = sph_target(c);
+    c->frnn_learned = learned && variable_h;
+    if (variable_h) {
         CUDA_TRY(cudaMemsetAsync(c->vh_done, 0, sizeof(int) * n, s));
         CUDA_TRY(cudaMemsetAsync(c->vh_nit, 0xff, sizeof(int) * n, s));  // nit starts at -1
         CUDA_TRY(cudaMemcpyAsync(c->h_start, c->sh, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
@@ -250,22 +308,60 @@ int stage_sph(mhpc_ctx* c, const mhpc_particles* p) {
                             c->cfg.max_sml_iterations, n, s));
     }
     record(c, EV_SML);
-    SphSorted S;
-    S.x = c->sx; S.y = c->sy; S.z = c->sz; S.m = c->sm; S.h = c->sh;
-    S.vx = c->svx; S.vy = c->svy; S.vz = c->svz; S.e = c->se;
-    S.mat = p->material_id ? c->smat : nullptr;
-    S.rho = c->srho; S.p = c->sp; S.cs = c->scs; S.bal = c->sbal;
-    S.f0 = c->sf0; S.f1 = c->sf1; S.f2 = c->sf2; S.f3 = c->sf3;
+    SphSorted S = sph_sorted(c, p);
     TRY(sph_frnn(c->T, P, S, c->nbr, c->noi, c->st, s));
+    record(c, EV_LISTS);
+    c->band_ran = false;
+    if (variable_h && c->cfg.sml_band_rounds > 0) {
+        // counts that drifted out of the band: repaired on the lists, then the
+        // final h goes back to the caller's order
+        BandBuffers B;
+        B.flags = c->vh_flags; B.off = c->vh_off; B.list = c->vh_list; B.dirty = c->vh_done; B.hnew = c->hold;
+        B.events = c->band_ev; B.cap_events = c->band_cap; B.ctr = c->band_ctr; B.scan_scratch = c->scan_scratch;
+        B.h0 = c->band_h0;
+        TRY(sph_band_fixup(c->T, P, c->sx, c->sy, c->sz, c->sh, c->nbr, c->noi, B, target, c->cfg.nb_tolerance,
+                           c->cfg.sml_band_rounds, c->st, s));
+        GatherList L;
+        std::memset(&L, 0, sizeof(L));
+        L.count = 1;
+        L.src[0] = c->sh;
+        L.dst[0] = p->sml;
+        TRY(launch_scatter(n, c->perm, L, s));
+        c->band_ran = true;
+    }
     record(c, EV_FRNN);
-    TRY(sph_density_eos(P, S, c->nbr, c->noi, c->perm, p->rho, p->p, p->cs, c->st, s));
-    if (c->cfg.balsara) TRY(sph_balsara(P, S, c->nbr, c->noi, c->st, s));
+    c->lists_n = n;
+    return MHPC_OK;
+}
+
+// SPH::Kernel::calculateDensity (src/sph/density.cu:8-72), calculateSoundSpeed
+// (src/sph/soundspeed.cu:38-97) and calculatePressure (src/sph/pressure.cu:5-87)
+// over the lists of stage_frnn, plus the Balsara factors when configured
+int stage_density_eos(mhpc_ctx* c, const mhpc_particles* p) {
+    SphParams P = sph_params(c, p->n);
+    SphSorted S = sph_sorted(c, p);
+    TRY(sph_density_eos(P, S, c->nbr, c->noi, c->perm, p->rho, p->p, p->cs, c->st, c->stream));
+    if (c->cfg.balsara) TRY(sph_balsara(P, S, c->nbr, c->noi, c->st, c->stream));
     record(c, EV_DENS);
+    return MHPC_OK;
+}
+
+// SPH::Kernel::internalForces (src/sph/internal_forces.cu:4-668) over the
+// lists of stage_frnn; the reference-layout lists and counts when the SoA
+// asks for them; the band statistic after a variable-h search; the learned
+// predictor's features and its prediction for the next right-hand side
+int stage_forces(mhpc_ctx* c, const mhpc_particles* p) {
+    const int n = p->n;
+    cudaStream_t s = c->stream;
+    SphParams P = sph_params(c, n);
+    SphSorted S = sph_sorted(c, p);
+    const int target = sph_target(c);
+    const bool learned = c->frnn_learned;
     TRY(sph_forces(P, S, c->nbr, c->noi, c->perm, p->ax, p->ay, p->az, p->drhodt, p->dedt, p->dsmldt, c->st, s));
     if (p->nnl || p->noi) TRY(sph_export_nnl(P, c->nbr, c->noi, c->perm, p->nnl, p->noi, s));
     if (c->cfg.variable_sml) TRY(sph_band_stats(P, c->noi, target, c->cfg.nb_tolerance, c->st, s));
     record(c, EV_FORCES);
-    if (learned && c->cfg.variable_sml) {
+    if (learned) {
         MlpFeatureInputs in;
         in.n = n; in.perm = c->perm; in.h = c->sh; in.h_start = c->h_start; in.rho = c->srho; in.cs = c->scs;
         in.vx = c->svx; in.vy = c->svy; in.vz = c->svz; in.noi = c->noi; in.nit = c->vh_nit;
@@ -277,6 +373,12 @@ int stage_sph(mhpc_ctx* c, const mhpc_particles* p) {
         TRY(mlp_features_predict(c->mlp, in, s));
     }
     return MHPC_OK;
+}
+
+int stage_sph(mhpc_ctx* c, const mhpc_particles* p) {
+    TRY(stage_frnn(c, p, c->cfg.variable_sml != 0, c->cfg.learned_h && c->mlp));
+    TRY(stage_density_eos(c, p));
+    return stage_forces(c, p);
 }
 
 int rhs_async(mhpc_ctx* c, const mhpc_particles* p, int self_gravity) {
@@ -422,7 +524,16 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
         A(c->noi, n);
         A(c->hold, n); A(c->vh_done, n); A(c->vh_nit, n); A(c->vh_count, n);
         A(c->vh_flags, n); A(c->vh_off, n + 1); A(c->vh_list, n); A(c->h_start, n);
+        // band repair events: a round changes a few pairs per out-of-band particle
+        // (room for 4 per particle: a round that needs more is skipped and counted)
+        c->band_cap = (int)std::min<size_t>(2147483000, std::max<size_t>(4096, 4 * n));
+        A(c->band_ev, c->band_cap);
+        A(c->band_ctr, 4);
+        A(c->band_h0, n);
     }
+    // mhpc_potential: the potential (when the caller passes no buffer) and the
+    // walk's own accelerations, so that the caller's g_a stay untouched
+    if (cfg->gravity) A(c->pot_scratch, 4 * n);
     A(c->diag_part, diagnostics_scratch_doubles());
     A(c->diag_out, 16);
     A(c->dt_dev, 1);
@@ -467,7 +578,6 @@ int mhpc_ctx_destroy(mhpc_ctx* c) {
         cudaStreamDestroy(c->copy_stream);
     }
     if (c->ev_drift) cudaEventDestroy(c->ev_drift);
-    if (c->pot_scratch) cudaFree(c->pot_scratch);
     if (c->mirror_ready) {
         double** ptrs[] = {&c->mirror.x, &c->mirror.y, &c->mirror.z, &c->mirror.mass, &c->mirror.vx, &c->mirror.vy,
                            &c->mirror.vz, &c->mirror.ax, &c->mirror.ay, &c->mirror.az, &c->mirror.g_ax,
@@ -489,8 +599,10 @@ int mhpc_ctx_set_stream(mhpc_ctx* c, void* stream) {
 
 int mhpc_ctx_set_config(mhpc_ctx* c, const mhpc_config* cfg) {
     if (!c || !cfg) return MHPC_ERR_ARG;
+    // max_num_interactions 0 means the default 180, as in mhpc_ctx_create
+    const int maxnb = cfg->max_num_interactions > 0 ? cfg->max_num_interactions : 180;
     if ((cfg->sph && !c->cfg.sph) || (cfg->gravity && !c->cfg.gravity) ||
-        (cfg->learned_h && !c->mlp) || cfg->max_num_interactions != c->maxnb)
+        (cfg->learned_h && !c->mlp) || maxnb != c->maxnb)
         return MHPC_ERR_ARG;  // would need buffers the context did not allocate
     c->cfg = *cfg;
     return MHPC_OK;
@@ -507,8 +619,9 @@ int mhpc_ctx_status(mhpc_ctx* c) {
     return read_status(c);
 }
 
-int mhpc_rhs(mhpc_ctx* c, const mhpc_particles* p, int step, int self_gravity, float* ms_out) {
+int mhpc_rhs(mhpc_ctx* c, const mhpc_particles* p, int step, int self_gravity, void* stream, float* ms_out) {
     if (!c) return MHPC_ERR_ARG;
+    c->stream = (cudaStream_t)stream;
     TRY(mhpc_rhs_async(c, p, step, self_gravity));
     int code = read_status(c);
     if (ms_out) {
@@ -533,6 +646,113 @@ int mhpc_stage_gravity(mhpc_ctx* c, const mhpc_particles* p) {
     TRY(check_particles(c, p));
     if (p->n == 0) return MHPC_OK;
     return stage_gravity(c, p);
+}
+
+int mhpc_tree_build(mhpc_ctx* c, const mhpc_particles* p) {
+    if (!c) return MHPC_ERR_ARG;
+    TRY(check_particles(c, p));
+    if (p->n == 0) return MHPC_OK;
+    CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevStatus), c->stream));
+    for (int e = 0; e < EV_COUNT; ++e) c->ev_recorded[e] = false;
+    c->last_n = p->n;
+    record(c, EV_START);
+    return stage_tree_build(c, p);
+}
+
+int mhpc_com(mhpc_ctx* c, const mhpc_particles* p) {
+    if (!c) return MHPC_ERR_ARG;
+    TRY(check_particles(c, p));
+    if (p->n == 0) return MHPC_OK;
+    if (c->tree_n != p->n) return MHPC_ERR_ARG;  // mhpc_tree_build first
+    return stage_com(c);
+}
+
+int mhpc_gravity(mhpc_ctx* c, const mhpc_particles* p, int precision) {
+    if (!c || !c->cfg.gravity || precision < -1 || precision > 2) return MHPC_ERR_ARG;
+    TRY(check_particles(c, p));
+    if (p->n == 0) return MHPC_OK;
+    if (c->tree_n != p->n || !c->com_ready) return MHPC_ERR_ARG;  // mhpc_tree_build + mhpc_com first
+    return stage_gravity(c, p, precision);
+}
+
+int mhpc_frnn(mhpc_ctx* c, const mhpc_particles* p, int variable_h, int predictor) {
+    if (!c || !c->cfg.sph || (predictor && !c->mlp)) return MHPC_ERR_ARG;
+    TRY(check_particles(c, p));
+    if (p->n == 0) return MHPC_OK;
+    if (c->tree_n != p->n || !c->com_ready) return MHPC_ERR_ARG;
+    return stage_frnn(c, p, variable_h != 0, predictor != 0);
+}
+
+int mhpc_density_eos(mhpc_ctx* c, const mhpc_particles* p) {
+    if (!c || !c->cfg.sph) return MHPC_ERR_ARG;
+    TRY(check_particles(c, p));
+    if (p->n == 0) return MHPC_OK;
+    if (c->lists_n != p->n) return MHPC_ERR_ARG;  // mhpc_frnn first
+    return stage_density_eos(c, p);
+}
+
+int mhpc_forces(mhpc_ctx* c, const mhpc_particles* p) {
+    if (!c || !c->cfg.sph) return MHPC_ERR_ARG;
+    TRY(check_particles(c, p));
+    if (p->n == 0) return MHPC_OK;
+    if (c->lists_n != p->n) return MHPC_ERR_ARG;
+    TRY(stage_forces(c, p));
+    record(c, EV_END);
+    return MHPC_OK;
+}
+
+int mhpc_integrate_leapfrog(mhpc_ctx* c, const mhpc_particles* p, double dt, int half) {
+    if (!c || !p || p->n < 0 || (half != 0 && half != 1)) return MHPC_ERR_ARG;
+    if (p->n == 0) return MHPC_OK;
+    if (!p->x || !p->y || !p->z || !p->vx || !p->vy || !p->vz || !p->g_ax || !p->g_ay || !p->g_az ||
+        !p->g_ax_old || !p->g_ay_old || !p->g_az_old)
+        return MHPC_ERR_ARG;
+    return half == 0 ? launch_leapfrog_x(*p, dt, c->stream) : launch_leapfrog_v(*p, dt, c->stream);
+}
+
+int mhpc_integrate_euler(mhpc_ctx* c, const mhpc_particles* p, double dt) {
+    if (!c || !p || p->n < 0) return MHPC_ERR_ARG;
+    if (p->n == 0) return MHPC_OK;
+    const mhpc_config& f = c->cfg;
+    if (!p->x || !p->y || !p->z || !p->vx || !p->vy || !p->vz) return MHPC_ERR_ARG;
+    if (f.gravity && (!p->g_ax || !p->g_ay || !p->g_az)) return MHPC_ERR_ARG;
+    if (f.sph && (!p->ax || !p->ay || !p->az)) return MHPC_ERR_ARG;
+    if (f.sph && ((f.integrate_density && (!p->rho || !p->drhodt)) || (f.integrate_energy && (!p->e || !p->dedt)) ||
+                  (f.integrate_sml && (!p->sml || !p->dsmldt))))
+        return MHPC_ERR_ARG;
+    return launch_euler(*p, dt, f.gravity, f.sph, f.sph && f.integrate_density, f.sph && f.integrate_energy,
+                        f.sph && f.integrate_sml, c->stream);
+}
+
+int mhpc_integrate_pc_step_size(mhpc_ctx* c, const mhpc_particles* p, double time_left, double* dt_dev) {
+    if (!c || !p || !dt_dev || p->n <= 0) return MHPC_ERR_ARG;
+    if (!p->sml || !p->vx || !p->vy || !p->vz) return MHPC_ERR_ARG;
+    if (c->cfg.gravity && (!p->g_ax || !p->g_ay || !p->g_az)) return MHPC_ERR_ARG;
+    if (c->cfg.sph && (!p->ax || !p->ay || !p->az || !p->cs || !p->rho || !p->drhodt)) return MHPC_ERR_ARG;
+    if (c->cfg.max_time_step <= 0) return MHPC_ERR_CONFIG;
+    return launch_set_time_step(*p, c->cfg.gravity, c->cfg.sph, c->mats[0].alpha, c->mats[0].beta,
+                                c->cfg.integrate_density, time_left, c->cfg.max_time_step, c->dt_part, dt_dev,
+                                c->stream);
+}
+
+int mhpc_integrate_pc_predictor(mhpc_ctx* c, const mhpc_particles* p, const mhpc_particles* q, const double* dt_dev) {
+    if (!c || !p || !q || !dt_dev || p->n < 0 || q->n < p->n) return MHPC_ERR_ARG;
+    if (p->n == 0) return MHPC_OK;
+    if (!p->g_ax || !p->g_ay || !p->g_az || !q->x || !q->y || !q->z || !q->vx || !q->vy || !q->vz || !q->mass)
+        return MHPC_ERR_ARG;
+    if (c->cfg.sph && (!q->sml || !q->cs || !q->rho || !q->p || !q->e || !p->ax)) return MHPC_ERR_ARG;
+    return launch_pc_predictor(*p, *q, dt_dev, c->cfg.sph, c->cfg.integrate_density, c->cfg.integrate_energy,
+                               c->stream);
+}
+
+int mhpc_integrate_pc_corrector(mhpc_ctx* c, const mhpc_particles* p, const mhpc_particles* q, const double* dt_dev) {
+    if (!c || !p || !q || !dt_dev || p->n < 0 || q->n < p->n) return MHPC_ERR_ARG;
+    if (p->n == 0) return MHPC_OK;
+    if (!p->g_ax || !p->g_ay || !p->g_az || !q->vx || !q->vy || !q->vz) return MHPC_ERR_ARG;
+    if (c->cfg.sph && (!q->ax || !q->sml || !q->drhodt || !q->dedt || !q->dsmldt || !p->ax || !p->sml))
+        return MHPC_ERR_ARG;
+    return launch_pc_corrector(*p, *q, dt_dev, c->cfg.sph, c->cfg.integrate_density, c->cfg.integrate_energy,
+                               c->cfg.integrate_sml, c->stream);
 }
 
 int mhpc_stage_sph(mhpc_ctx* c, const mhpc_particles* p) {
@@ -578,6 +798,9 @@ int mhpc_integrate(mhpc_ctx* c, const mhpc_particles* p, int step, double* dt_ou
         } break;
         case 1: {  // PredictorCorrectorEuler::integrate (src/integrator/predictor_corrector_euler.cpp:47-151)
             if (!c->pred.x) return MHPC_ERR_ARG;  // context created for another integrator
+            // the update kernels read g_a (zero without gravity, as in the reference) and the
+            // step size reads every h
+            if (!p->g_ax || !p->g_ay || !p->g_az || !p->sml) return MHPC_ERR_ARG;
             const int sph = c->cfg.sph;
             TRY(rhs_async(c, p, 1));
             const double alpha = c->mats[0].alpha, beta = c->mats[0].beta;
@@ -775,9 +998,11 @@ int mhpc_get_stats(mhpc_ctx* c, mhpc_stats* o) {
     o->sml_out_of_band = h.sml_out_of_band;
     o->predictor_used = h.predictor_used;
     o->predictor_fallback = h.predictor_fallback;
-    const int pairs[12][2] = {{EV_START, EV_KEYS}, {EV_KEYS, EV_SORT}, {EV_SORT, EV_TREE}, {EV_TREE, EV_COM},
-                              {EV_COM, EV_GRAV},   {EV_SML, EV_FRNN}, {EV_COM, EV_SML},   {EV_FRNN, EV_DENS},
-                              {EV_DENS, EV_FORCES}, {-1, -1},         {-1, -1},           {EV_START, EV_END}};
+    o->sml_band_before = c->band_ran ? h.sml_band_before : -1;
+    o->sml_band_skipped = h.sml_band_skipped;
+    const int pairs[12][2] = {{EV_START, EV_KEYS}, {EV_KEYS, EV_SORT}, {EV_SORT, EV_TREE},  {EV_TREE, EV_COM},
+                              {EV_COM, EV_GRAV},   {EV_SML, EV_LISTS}, {EV_COM, EV_SML},    {EV_FRNN, EV_DENS},
+                              {EV_DENS, EV_FORCES}, {EV_LISTS, EV_FRNN}, {-1, -1},          {EV_START, EV_END}};
     for (int k = 0; k < 12; ++k) {
         int a = pairs[k][0], b = pairs[k][1];
         if (a >= 0 && c->ev_recorded[a] && c->ev_recorded[b]) cudaEventElapsedTime(&o->ms_stage[k], c->ev[a], c->ev[b]);
@@ -851,7 +1076,7 @@ int mhpc_potential(mhpc_ctx* c, const mhpc_particles* p, double* pot_dev, double
         return MHPC_OK;
     }
     cudaStream_t s = c->stream;
-    if (!c->pot_scratch) CUDA_TRY(cudaMalloc(&c->pot_scratch, sizeof(double) * 4 * (size_t)c->cap));
+    if (!c->pot_scratch) return MHPC_ERR_ARG;
     double* pot = pot_dev ? pot_dev : c->pot_scratch;
     double* acc = c->pot_scratch + c->cap;  // accelerations of this walk (not the caller's g_a)
     CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevStatus), s));
@@ -863,7 +1088,7 @@ int mhpc_potential(mhpc_ctx* c, const mhpc_particles* p, double* pot_dev, double
     std::memset(&G, 0, sizeof(G));
     G.n = n;
     G.eps2 = c->cfg.smoothing;
-    G.h_factor = (c->cfg.softening_mode == 1) ? c->cfg.softening_h_factor : 0.0;
+    G.h_factor = h_softening(c->cfg) ? c->cfg.softening_h_factor : 0.0;
     G.G = c->cfg.si_units ? 6.67430e-11 : 1.0;
     G.ord = c->ord;
     G.theta = c->cfg.theta_mixed;  // geometric rule: the same opening rule at every call

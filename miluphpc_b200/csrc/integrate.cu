@@ -10,7 +10,14 @@ __global__ void __launch_bounds__(256) k_gather(int n, const int* __restrict__ p
         const int o = __ldg(perm + s);
 #pragma unroll 4
         for (int a = 0; a < L.count; ++a) L.dst[a][s] = __ldg(L.src[a] + o);
-        if (L.isrc) L.idst[s] = __ldg(L.isrc + o);
+        if (L.isrc) {
+            int v = __ldg(L.isrc + o);
+            if (L.imax > 0 && (v < 0 || v >= L.imax)) {
+                if (L.st) set_status(L.st, MHPC_ERR_ARG, o);
+                v = v < 0 ? 0 : L.imax - 1;
+            }
+            L.idst[s] = v;
+        }
     }
 }
 
@@ -22,45 +29,58 @@ __global__ void __launch_bounds__(256) k_scatter(int n, const int* __restrict__ 
     }
 }
 
-// LeapfrogNS::Kernel::updateX (src/integrator/device_leapfrog.cu:4-30)
+// The update kernels round every product and sum separately (__dmul_rn /
+// __dadd_rn), in the reference's order of operations, like its -fmad=false
+// build: the same inputs give bit-identical states.
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+// a + b * c without contraction
+__device__ __forceinline__ double axpy_rn(double a, double b, double c) { return __dadd_rn(a, __dmul_rn(b, c)); }
+
+// LeapfrogNS::Kernel::updateX (src/integrator/device_leapfrog.cu:4-30):
+// x += dt (v + 0.5 dt g), g_old = g
 __global__ void __launch_bounds__(256) k_leapfrog_x(mhpc_particles p, double dt) {
+    const double hdt = mul_rn(0.5, dt);
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < p.n; i += (long)gridDim.x * blockDim.x) {
         const double gx = p.g_ax[i], gy = p.g_ay[i], gz = p.g_az[i];
-        p.x[i] += dt * (p.vx[i] + 0.5 * dt * gx);
-        p.y[i] += dt * (p.vy[i] + 0.5 * dt * gy);
-        p.z[i] += dt * (p.vz[i] + 0.5 * dt * gz);
+        p.x[i] = axpy_rn(p.x[i], dt, axpy_rn(p.vx[i], hdt, gx));
+        p.y[i] = axpy_rn(p.y[i], dt, axpy_rn(p.vy[i], hdt, gy));
+        p.z[i] = axpy_rn(p.z[i], dt, axpy_rn(p.vz[i], hdt, gz));
         p.g_ax_old[i] = gx; p.g_ay_old[i] = gy; p.g_az_old[i] = gz;
     }
 }
 
-// LeapfrogNS::Kernel::updateV (device_leapfrog.cu:32-58)
+// LeapfrogNS::Kernel::updateV (device_leapfrog.cu:32-58): v += 0.5 dt (g + g_old)
 __global__ void __launch_bounds__(256) k_leapfrog_v(mhpc_particles p, double dt) {
+    const double hdt = mul_rn(0.5, dt);
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < p.n; i += (long)gridDim.x * blockDim.x) {
-        p.vx[i] += 0.5 * dt * (p.g_ax[i] + p.g_ax_old[i]);
-        p.vy[i] += 0.5 * dt * (p.g_ay[i] + p.g_ay_old[i]);
-        p.vz[i] += 0.5 * dt * (p.g_az[i] + p.g_az_old[i]);
+        p.vx[i] = axpy_rn(p.vx[i], hdt, add_rn(p.g_ax[i], p.g_ax_old[i]));
+        p.vy[i] = axpy_rn(p.vy[i], hdt, add_rn(p.g_ay[i], p.g_ay_old[i]));
+        p.vz[i] = axpy_rn(p.vz[i], hdt, add_rn(p.g_az[i], p.g_az_old[i]));
     }
 }
 
-// ExplicitEulerNS::Kernel::update (src/integrator/device_explicit_euler.cu:4-54)
+// ExplicitEulerNS::Kernel::update (src/integrator/device_explicit_euler.cu:4-54):
+// v += dt (a + g), x += dt v (the new v), rho, e (floored at 1e-50), h
 __global__ void __launch_bounds__(256) k_euler(mhpc_particles p, double dt, int gravity, int sph, int int_rho,
                                                int int_e, int int_sml) {
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < p.n; i += (long)gridDim.x * blockDim.x) {
+        // the reference adds a + g with a zero array for the absent part: 0 + g is exact
         double ax = 0, ay = 0, az = 0;
-        if (sph) { ax += p.ax[i]; ay += p.ay[i]; az += p.az[i]; }
-        if (gravity) { ax += p.g_ax[i]; ay += p.g_ay[i]; az += p.g_az[i]; }
-        p.vx[i] += dt * ax;
-        p.vy[i] += dt * ay;
-        p.vz[i] += dt * az;
-        p.x[i] += dt * p.vx[i];
-        p.y[i] += dt * p.vy[i];
-        p.z[i] += dt * p.vz[i];
-        if (int_rho) p.rho[i] = p.rho[i] + dt * p.drhodt[i];
+        if (sph) { ax = p.ax[i]; ay = p.ay[i]; az = p.az[i]; }
+        if (gravity) { ax = add_rn(ax, p.g_ax[i]); ay = add_rn(ay, p.g_ay[i]); az = add_rn(az, p.g_az[i]); }
+        p.vx[i] = axpy_rn(p.vx[i], dt, ax);
+        p.vy[i] = axpy_rn(p.vy[i], dt, ay);
+        p.vz[i] = axpy_rn(p.vz[i], dt, az);
+        p.x[i] = axpy_rn(p.x[i], dt, p.vx[i]);
+        p.y[i] = axpy_rn(p.y[i], dt, p.vy[i]);
+        p.z[i] = axpy_rn(p.z[i], dt, p.vz[i]);
+        if (int_rho) p.rho[i] = axpy_rn(p.rho[i], dt, p.drhodt[i]);
         if (int_e) {
-            p.e[i] += dt * p.dedt[i];
+            p.e[i] = axpy_rn(p.e[i], dt, p.dedt[i]);
             if (p.e[i] < 1e-50) p.e[i] = 1e-50;
         }
-        if (int_sml) p.sml[i] = p.sml[i] + dt * p.dsmldt[i];
+        if (int_sml) p.sml[i] = axpy_rn(p.sml[i], dt, p.dsmldt[i]);
     }
 }
 
@@ -71,19 +91,20 @@ __global__ void __launch_bounds__(256) k_pc_predictor(mhpc_particles p, mhpc_par
                                                       int sph, int int_rho, int int_e) {
     const double dt = *dtp;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < p.n; i += (long)gridDim.x * blockDim.x) {
-        double ax = p.g_ax[i], ay = p.g_ay[i], az = p.g_az[i];
-        if (sph) { ax += p.ax[i]; ay += p.ay[i]; az += p.az[i]; }
-        q.x[i] = p.x[i] + dt * p.vx[i];
-        q.vx[i] = p.vx[i] + dt * ax;
-        q.y[i] = p.y[i] + dt * p.vy[i];
-        q.vy[i] = p.vy[i] + dt * ay;
-        q.z[i] = p.z[i] + dt * p.vz[i];
-        q.vz[i] = p.vz[i] + dt * az;
+        double ax = 0, ay = 0, az = 0;
+        if (sph) { ax = p.ax[i]; ay = p.ay[i]; az = p.az[i]; }
+        ax = add_rn(ax, p.g_ax[i]); ay = add_rn(ay, p.g_ay[i]); az = add_rn(az, p.g_az[i]);
+        q.x[i] = axpy_rn(p.x[i], dt, p.vx[i]);
+        q.vx[i] = axpy_rn(p.vx[i], dt, ax);
+        q.y[i] = axpy_rn(p.y[i], dt, p.vy[i]);
+        q.vy[i] = axpy_rn(p.vy[i], dt, ay);
+        q.z[i] = axpy_rn(p.z[i], dt, p.vz[i]);
+        q.vz[i] = axpy_rn(p.vz[i], dt, az);
         q.mass[i] = p.mass[i];
         if (sph) {
-            if (int_rho) q.rho[i] = p.rho[i] + dt * p.drhodt[i];
+            if (int_rho) q.rho[i] = axpy_rn(p.rho[i], dt, p.drhodt[i]);
             if (int_e) {
-                q.e[i] = p.e[i] + dt * p.dedt[i];
+                q.e[i] = axpy_rn(p.e[i], dt, p.dedt[i]);
                 if (q.e[i] < 1e-6) q.e[i] = 1e-6;
             } else {
                 q.e[i] = p.e[i];
@@ -98,32 +119,33 @@ __global__ void __launch_bounds__(256) k_pc_predictor(mhpc_particles p, mhpc_par
 // PredictorCorrectorEulerNS::Kernel::corrector (device_predictor_corrector_euler.cu:130-205)
 __global__ void __launch_bounds__(256) k_pc_corrector(mhpc_particles p, mhpc_particles q, const double* dtp,
                                                       int sph, int int_rho, int int_e, int int_sml) {
-    const double h = 0.5 * *dtp;
+    const double h = mul_rn(0.5, *dtp);  // dt/2, exact
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < p.n; i += (long)gridDim.x * blockDim.x) {
         const double pax = sph ? q.ax[i] : 0.0, pay = sph ? q.ay[i] : 0.0, paz = sph ? q.az[i] : 0.0;
         const double cax = sph ? p.ax[i] : 0.0, cay = sph ? p.ay[i] : 0.0, caz = sph ? p.az[i] : 0.0;
-        p.x[i] = p.x[i] + h * (q.vx[i] + p.vx[i]);
-        p.vx[i] = p.vx[i] + h * (pax + cax + 2 * p.g_ax[i]);
-        p.y[i] = p.y[i] + h * (q.vy[i] + p.vy[i]);
-        p.vy[i] = p.vy[i] + h * (pay + cay + 2 * p.g_ay[i]);
-        p.z[i] = p.z[i] + h * (q.vz[i] + p.vz[i]);
-        p.vz[i] = p.vz[i] + h * (paz + caz + 2 * p.g_az[i]);
+        const double gx = p.g_ax[i], gy = p.g_ay[i], gz = p.g_az[i];
+        p.x[i] = axpy_rn(p.x[i], h, add_rn(q.vx[i], p.vx[i]));
+        p.vx[i] = axpy_rn(p.vx[i], h, add_rn(add_rn(pax, cax), mul_rn(2.0, gx)));
+        p.y[i] = axpy_rn(p.y[i], h, add_rn(q.vy[i], p.vy[i]));
+        p.vy[i] = axpy_rn(p.vy[i], h, add_rn(add_rn(pay, cay), mul_rn(2.0, gy)));
+        p.z[i] = axpy_rn(p.z[i], h, add_rn(q.vz[i], p.vz[i]));
+        p.vz[i] = axpy_rn(p.vz[i], h, add_rn(add_rn(paz, caz), mul_rn(2.0, gz)));
         if (sph) {
-            p.ax[i] = 0.5 * (pax + cax) + p.g_ax[i];
-            p.ay[i] = 0.5 * (pay + cay) + p.g_ay[i];
-            p.az[i] = 0.5 * (paz + caz) + p.g_az[i];
+            p.ax[i] = add_rn(mul_rn(0.5, add_rn(pax, cax)), gx);
+            p.ay[i] = add_rn(mul_rn(0.5, add_rn(pay, cay)), gy);
+            p.az[i] = add_rn(mul_rn(0.5, add_rn(paz, caz)), gz);
             if (int_rho) {
-                p.rho[i] = p.rho[i] + h * (q.drhodt[i] + p.drhodt[i]);
-                p.drhodt[i] = 0.5 * (q.drhodt[i] + p.drhodt[i]);
+                p.rho[i] = axpy_rn(p.rho[i], h, add_rn(q.drhodt[i], p.drhodt[i]));
+                p.drhodt[i] = mul_rn(0.5, add_rn(q.drhodt[i], p.drhodt[i]));
             }
             if (int_e) {
-                p.e[i] = p.e[i] + h * (q.dedt[i] + p.dedt[i]);
+                p.e[i] = axpy_rn(p.e[i], h, add_rn(q.dedt[i], p.dedt[i]));
                 if (p.e[i] < 1e-6) p.e[i] = 1e-6;
-                p.dedt[i] = 0.5 * (q.dedt[i] + p.dedt[i]);
+                p.dedt[i] = mul_rn(0.5, add_rn(q.dedt[i], p.dedt[i]));
             }
             if (int_sml) {
-                p.sml[i] = p.sml[i] + h * (q.dsmldt[i] + p.dsmldt[i]);
-                p.dsmldt[i] = 0.5 * (q.dsmldt[i] + p.dsmldt[i]);
+                p.sml[i] = axpy_rn(p.sml[i], h, add_rn(q.dsmldt[i], p.dsmldt[i]));
+                p.dsmldt[i] = mul_rn(0.5, add_rn(q.dsmldt[i], p.dsmldt[i]));
             } else {
                 p.sml[i] = q.sml[i];
             }
@@ -213,7 +235,9 @@ __global__ void k_max_sml(int n, const double* h, double* part) {
     }
 }
 
-constexpr int kDiag = 11;
+// 0 kinetic energy, 1 internal energy, 2-4 momentum, 5-7 angular momentum,
+// 8-10 mass-weighted position sums, 11 total mass
+constexpr int kDiag = 12;
 
 __global__ void __launch_bounds__(256) k_diag(mhpc_particles p, int sph, double* part) {
     double acc[kDiag];
@@ -229,6 +253,7 @@ __global__ void __launch_bounds__(256) k_diag(mhpc_particles p, int sph, double*
         acc[6] += m * (z * vx - x * vz);
         acc[7] += m * (x * vy - y * vx);
         acc[8] += m * x; acc[9] += m * y; acc[10] += m * z;
+        acc[11] += m;
     }
     __shared__ double sh[8][kDiag];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -246,11 +271,19 @@ __global__ void __launch_bounds__(256) k_diag(mhpc_particles p, int sph, double*
     }
 }
 
-__global__ void k_diag_final(int blocks, const double* part, double* out, const double* mass_total_part) {
+// block sums in block order (deterministic); the centre of mass is the
+// mass-weighted position sum over the total mass
+__global__ void k_diag_final(int blocks, const double* part, double* out) {
+    __shared__ double tot[kDiag];
     if (threadIdx.x < kDiag) {
         double v = 0;
         for (int b = 0; b < blocks; ++b) v += part[b * kDiag + threadIdx.x];
-        out[threadIdx.x] = v;
+        tot[threadIdx.x] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kDiag) {
+        const double v = tot[threadIdx.x];
+        out[threadIdx.x] = (threadIdx.x >= 8 && threadIdx.x < 11) ? (tot[11] > 0 ? v / tot[11] : 0.0) : v;
     }
 }
 
@@ -294,19 +327,22 @@ __global__ void __launch_bounds__(256) k_direct(const double* __restrict__ x, co
     }
 }
 
-// FP32 FMA throughput probe: 8 independent dependent chains per thread.
+// FP32 FMA throughput probe on the paired instruction the gravity walk
+// issues (FFMA2: two FP32 fused multiply-adds per lane): 8 independent
+// chains of float2 per thread, i.e. 16 FP32 FMAs per iteration.
 constexpr int kFmaIters = 2048;
 __global__ void __launch_bounds__(256) k_fma_peak(float* out, float b, float c) {
-    float a[8];
+    float2 a[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) a[k] = threadIdx.x * 1e-3f + k;
+    for (int k = 0; k < 8; ++k) a[k] = make_float2(threadIdx.x * 1e-3f + k, threadIdx.x * 2e-3f - k);
+    const float2 B = make_float2(b, b), C = make_float2(c, c);
     for (int i = 0; i < kFmaIters; ++i) {
 #pragma unroll
-        for (int k = 0; k < 8; ++k) a[k] = fmaf(a[k], b, c);
+        for (int k = 0; k < 8; ++k) a[k] = __ffma2_rn(a[k], B, C);
     }
     float s = 0.f;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) s += a[k];
+    for (int k = 0; k < 8; ++k) s += a[k].x + a[k].y;
     if (s == 1234.5f) out[blockIdx.x] = s;
 }
 
@@ -364,7 +400,7 @@ extern "C" int mhpc_fp32_peak(double* tflops) {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(out);
-    const double flops = 2.0 * 8 * kFmaIters * 256.0 * blocks * reps;
+    const double flops = 2.0 * 16 * kFmaIters * 256.0 * blocks * reps;
     *tflops = flops / (ms * 1e-3) / 1e12;
     return cudaGetLastError() == cudaSuccess ? MHPC_OK : MHPC_ERR_CUDA;
 }
@@ -430,7 +466,7 @@ int launch_set_time_step(const mhpc_particles& p, int gravity, int sph, double a
 int launch_diagnostics(const mhpc_particles& p, int sph, double* part, double* out, cudaStream_t s) {
     const int blocks = 148 * 4;
     k_diag<<<blocks, 256, 0, s>>>(p, sph, part);
-    k_diag_final<<<1, 32, 0, s>>>(blocks, part, out, nullptr);
+    k_diag_final<<<1, 32, 0, s>>>(blocks, part, out);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

@@ -10,6 +10,8 @@ struct GatherList {
     double* dst[MHPC_GATHER_MAX];
     const int* isrc;  // optional int array gathered alongside
     int* idst;
+    int imax;         // > 0: gathered ints must lie in [0, imax) (material ids); others are
+    DevStatus* st;    // reported as MHPC_ERR_ARG (detail: the original index) and clamped
 };
 
 int launch_gather(int n, const int* perm, const GatherList& L, cudaStream_t s);

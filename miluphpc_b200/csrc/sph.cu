@@ -126,13 +126,6 @@ __device__ __forceinline__ float3 rel_f(const float4& ah, const float4& al, cons
     return make_float3((ah.x - bh.x) + (al.x - bl.x), (ah.y - bh.y) + (al.y - bl.y), (ah.z - bh.z) + (al.z - bl.z));
 }
 
-__device__ __forceinline__ double d2_exact(double dx, double dy, double dz) {
-    return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-}
-
-__device__ __forceinline__ size_t nb_index(long s, int k, int maxnb) {
-    return ((size_t)(s >> 5) * maxnb + k) * 32 + (s & 31);
-}
 
 // ------------------------------------------------------------ FRNN walk
 // One warp per 32 consecutive (sorted or listed) particles, lane = particle,
@@ -668,6 +661,7 @@ __global__ void __launch_bounds__(kBlock) k_density_eos(SphParams P, SphSorted S
     double p = S.p[s], cs = S.cs[s];
     switch (M.eos_type) {
         case 0: cs = sqrt(M.K * pow(rho, M.gamma - 1.0)); break;
+        case 1: case 3: cs = M.cs_init; break;  // constant: initializeSoundSpeed (soundspeed.cu:4-36)
         case 9: cs = sqrt(M.gamma * p / rho); break;
         case 12: cs = 0.0; break;
         default: break;
@@ -805,6 +799,7 @@ __global__ void k_pack_pos(SphSorted S, int n) {
 __device__ __forceinline__ void eos(const MatDev& M, double rho, double e, double& p, double& cs) {
     switch (M.eos_type) {
         case 0: cs = sqrt(M.K * pow(rho, M.gamma - 1.0)); break;
+        case 1: case 3: cs = M.cs_init; break;  // constant: initializeSoundSpeed (soundspeed.cu:4-36)
         case 9: cs = sqrt(M.gamma * p / rho); break;
         case 12: cs = 0.0; break;
         default: break;

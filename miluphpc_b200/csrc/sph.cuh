@@ -40,6 +40,17 @@ struct SphSorted {
     float2* f3;
 };
 
+// Squared distance without FMA contraction, summed in the reference's order
+// (dx^2 + dy^2) + dz^2: the pair rule's d^2 of every neighbour kernel.
+__device__ __forceinline__ double d2_exact(double dx, double dy, double dz) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+}
+
+// Slot k of sorted particle s's neighbour list in the group-transposed layout.
+__device__ __forceinline__ size_t nb_index(long s, int k, int maxnb) {
+    return ((size_t)(s >> 5) * maxnb + k) * 32 + (s & 31);
+}
+
 // Neighbour lists in sorted index space, group-transposed:
 // nbr[((s >> 5) * maxnb + k) * 32 + (s & 31)], count noi[s].
 int sph_frnn(const TreeDev& T, const SphParams& P, const SphSorted& S, int* nbr, int* noi, DevStatus* st,
@@ -82,3 +93,31 @@ int sph_forces(const SphParams& P, const SphSorted& S, const int* nbr, const int
 int sph_band_stats(const SphParams& P, const int* noi, int target, int tol, DevStatus* st, cudaStream_t s);
 int sph_export_nnl(const SphParams& P, const int* nbr, const int* noi, const int* perm, int* nnl, int* noi_out,
                    cudaStream_t s);
+
+// Neighbour-band repair after the variable-h iteration and the list walk (an
+// addition of this library; the reference stops at its iteration limit and
+// leaves such particles where they are).  `rounds` times: every particle
+// whose count misses |n - target| < tol takes, with all other h frozen, the h
+// that gives it target + tol - 2 neighbours (from above) or target - tol + 2
+// (from below): the midpoint of the two candidate distances around that rank,
+// candidates being the j != i with d_ij < h_j within a search radius (h_i
+// from above; 1.5 h_i, or 2 h_i below half the wanted count, from below,
+// at most twice the h before the first round; the search radius itself when
+// it holds too few).  All such particles move
+// at once, and the neighbour lists and counts are edited in place pair by
+// pair, so they equal a fresh list walk on the new h.
+struct BandBuffers {
+    int* flags;          // [n] scratch (particles out of the band)
+    int* off;            // [n+1] scratch (scan); off[n] = particles out of the band
+    int* list;           // [n] particles out of the band
+    int* dirty;          // [n] lists with removed entries (zeroed here)
+    double* hnew;        // [n] new h (equal to h outside a round)
+    double* h0;          // [n] h before the first round
+    int2* events;        // [cap_events] pair changes (x >= 0: add (x, y); x < 0: remove (~x, y))
+    int cap_events;
+    int* ctr;            // [4] events, overflow flag
+    void* scan_scratch;
+};
+int sph_band_fixup(const TreeDev& T, const SphParams& P, const double* x, const double* y, const double* z,
+                   double* h, int* nbr, int* noi, const BandBuffers& B, int target, int tol, int rounds,
+                   DevStatus* st, cudaStream_t s);

@@ -58,6 +58,7 @@ class Miluphpc:
         self.capacity = int(capacity or n)
         self.num_nodes = int(num_nodes or n)
         mats = materials or [material()]
+        self.materials = list(mats)
         self._mats = (Material * max(1, len(mats)))(*mats)
         self.t = {}
         for f in DOUBLE_FIELDS:
@@ -104,7 +105,7 @@ class Miluphpc:
     def rhs(self, step=0, self_gravity=True):
         ms = ctypes.c_float(0)
         check(self.L.mhpc_rhs(self.ctx, ctypes.byref(self._soa), int(step), int(bool(self_gravity)),
-                              ctypes.byref(ms)), "rhs")
+                              ctypes.c_void_p(self.stream.cuda_stream), ctypes.byref(ms)), "rhs")
         return ms.value
 
     def rhs_async(self, step=0, self_gravity=True):

@@ -717,33 +717,71 @@ void orc_frnn(const double* x, const double* y, const double* z, const double* h
     }
 }
 
-// SmoothingKernel::cubicSpline, 3-D (kernel.cu:50-83): support radius = sml,
-// f = 8/(pi h^3), split at q = 1/2.  dWdx = dWdr/r * dx (NaN at r = 0, as in
-// the reference; only the self-density call hits r = 0 and it ignores dWdx).
-static inline void cubic(double* W, double dWdx[3], double* dWdr, const double dx[3], double sml) {
+// SmoothingKernel::{spiky, cubicSpline, wendlandc2, wendlandc4, wendlandc6},
+// 3-D forms (kernel.cu:14-183), support radius = sml; type 0 spiky, 1 cubic
+// spline (f = 8/(pi h^3), split at q = 1/2), 2/3/4 Wendland C2/C4/C6 (Dehnen &
+// Aly 2012; the C4 derivative as the reference writes it).  dWdx = dWdr/r * dx
+// (NaN at r = 0, as in the reference; only the self-density call hits r = 0
+// and it ignores dWdx).
+static inline void skern(int type, double* W, double dWdx[3], double* dWdr, const double dx[3], double sml) {
     double r = std::sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
     double q = r / sml;
-    double f = 8. / M_PI * 1. / (sml * sml * sml);
-    if (q > 1) { *W = 0; *dWdr = 0.0; }
-    else if (q > 0.5) { *W = 2. * f * (1. - q) * (1. - q) * (1 - q); *dWdr = -6. * f * 1. / sml * (1. - q) * (1. - q); }
-    else { *W = f * (6. * q * q * q - 6. * q * q + 1.); *dWdr = 6. * f / sml * (3 * q * q - 2 * q); }
+    *W = 0;
+    *dWdr = 0;
+    switch (type) {
+        case 0:
+            if (q > 1) { *W = 0; }
+            else if (q >= 0.0) {
+                *W = 15. / (M_PI * sml * sml * sml) * (1 - q) * (1 - q) * (1 - q);
+                *dWdr = -45 / (M_PI * sml * sml * sml * sml) * (1 - q) * (1 - q);
+            }
+            break;
+        case 1: {
+            double f = 8. / M_PI * 1. / (sml * sml * sml);
+            if (q > 1) { *W = 0; *dWdr = 0.0; }
+            else if (q > 0.5) { *W = 2. * f * (1. - q) * (1. - q) * (1 - q); *dWdr = -6. * f * 1. / sml * (1. - q) * (1. - q); }
+            else { *W = f * (6. * q * q * q - 6. * q * q + 1.); *dWdr = 6. * f / sml * (3 * q * q - 2 * q); }
+        } break;
+        case 2:
+            if (r <= sml) {
+                *W = 21. / (2 * M_PI * sml * sml * sml) * (1 - q) * (1 - q) * (1 - q) * (1 - q) * (1 + 4 * q) * (q < 1);
+                *dWdr = -210. / (M_PI * sml * sml * sml * sml) * q * (1 - q) * (1 - q) * (1 - q) * (q < 1);
+            }
+            break;
+        case 3:
+            if (r <= sml) {
+                *W = 495. / (32. * M_PI * sml * sml * sml) * (1 - q) * (1 - q) * (1 - q) * (1 - q) * (1 - q) *
+                     (1 - q) * (1. + 6. * q + 35. / 3. * q * q) * (q < 1);
+                *dWdr = -1485. / (16. * M_PI * sml * sml * sml * sml) * (1 - q) * (1 - q) * (1 - q) * (1 - q) *
+                        (1 - q) * (1. - 35. * q * q + 105. * q * q * q) * (q < 1);
+            }
+            break;
+        default:
+            if (r <= sml) {
+                *W = 1365. / (64. * M_PI * sml * sml * sml) * (1 - q) * (1 - q) * (1 - q) * (1 - q) * (1 - q) *
+                     (1 - q) * (1 - q) * (1 - q) * (1. + 8. * q + 25. * q * q + 32 * q * q * q) * (q < 1);
+                *dWdr = -15015. / (32. * M_PI * sml * sml * sml * sml) * q * (1 - q) * (1 - q) * (1 - q) *
+                        (1 - q) * (1 - q) * (1 - q) * (1 - q) * (1. + 7 * q + 16 * q * q) * (q < 1);
+            }
+            break;
+    }
     for (int d = 0; d < 3; ++d) dWdx[d] = *dWdr / r * dx[d];
 }
 
 // SPH::Kernel::calculateDensity (density.cu:8-72) over a CSR neighbour list;
 // avg_h selects h_bar = (h_i + h_j)/2 (VARIABLE_SML || INTEGRATE_SML).
 void orc_density(const double* x, const double* y, const double* z, const double* mass,
-                 const double* h, int n, const long* off, const int* nbr, int avg_h, double* rho) {
+                 const double* h, int n, const long* off, const int* nbr, int avg_h, int kernel, double* rho) {
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i) {
         double W, dWdx[3], dWdr, dx[3] = {0, 0, 0};
-        cubic(&W, dWdx, &dWdr, dx, h[i]);
+        skern(kernel, &W, dWdx, &dWdr, dx, h[i]);
         double r = mass[i] * W;
         for (long k = off[i]; k < off[i + 1]; ++k) {
             int j = nbr[k];
             double sml = avg_h ? 0.5 * (h[i] + h[j]) : h[i];
             dx[0] = x[i] - x[j]; dx[1] = y[i] - y[j]; dx[2] = z[i] - z[j];
-            cubic(&W, dWdx, &dWdr, dx, sml);
+            skern(kernel, &W, dWdx, &dWdr, dx, sml);
             r += mass[j] * W;
         }
         rho[i] = r;
@@ -754,13 +792,19 @@ void orc_density(const double* x, const double* y, const double* z, const double
 // SPH::Kernel::calculatePressure (pressure.cu:5-87), in the reference's order
 // (sound speed first, so the ideal-gas c_s uses the previous pressure).
 // eos: 0 polytropic, 1 Murnaghan, 3 isothermal H2, 9 ideal gas,
-// 12 locally isothermal.  par = {K, gamma, rho_0, bulk_modulus, n}.
+// 12 locally isothermal.  par = {K, gamma, rho_0, bulk_modulus, n, si_units}.
+// Murnaghan and isothermal keep the constant sound speed that
+// SPH::Kernel::initializeSoundSpeed (soundspeed.cu:4-36) sets once:
+// sqrt(bulk_modulus / rho_0), and 203 m/s (divided by c = 2.998e8 without SI
+// units).
 void orc_eos(int n, int eos, const double* par, const double* rho, const double* e, double* p,
              double* cs) {
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i) {
         switch (eos) {
             case 0: cs[i] = std::sqrt(par[0] * std::pow(rho[i], par[1] - 1.0)); break;
+            case 1: cs[i] = std::sqrt(par[3] / par[2]); break;
+            case 3: cs[i] = par[5] != 0.0 ? 203.0 : 203.0 / 2.998e8; break;
             case 9: cs[i] = std::sqrt(par[1] * p[i] / rho[i]); break;
             case 12: cs[i] = 0; break;
             default: break;
@@ -791,8 +835,8 @@ void orc_eos(int n, int eos, const double* par, const double* rho, const double*
 // (3 per particle) and f may be null.
 void orc_balsara(const double* x, const double* y, const double* z, const double* vx, const double* vy,
                  const double* vz, const double* mass, const double* h, const double* rho, const double* cs,
-                 int n, const long* off, const int* nbr, int avg_h, double* divv_out, double* curlv_out,
-                 double* f) {
+                 int n, const long* off, const int* nbr, int avg_h, int kernel, double* divv_out,
+                 double* curlv_out, double* f) {
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i) {
         double divv = 0, curl[3] = {0, 0, 0};
@@ -801,7 +845,7 @@ void orc_balsara(const double* x, const double* y, const double* z, const double
             const double sml = avg_h ? 0.5 * (h[i] + h[j]) : h[i];
             const double dr[3] = {x[i] - x[j], y[i] - y[j], z[i] - z[j]};
             double W, dW[3], dWdr;
-            cubic(&W, dW, &dWdr, dr, sml);
+            skern(kernel, &W, dW, &dWdr, dr, sml);
             const double vi[3] = {vx[i], vy[i], vz[i]}, vj[3] = {vx[j], vy[j], vz[j]};
             for (int d = 0; d < 3; ++d) divv += mass[j] / rho[j] * (vj[d] - vi[d]) * dW[d];
             curl[0] += mass[j] / rho[i] * ((vi[1] - vj[1]) * dW[2] - (vi[2] - vj[2]) * dW[1]);
@@ -821,7 +865,7 @@ void orc_forces(const double* x, const double* y, const double* z, const double*
                 const double* vy, const double* vz, const double* mass, const double* h,
                 const double* rho, const double* p, const double* cs, int n, const long* off,
                 const int* nbr, double alpha, double beta, int avg_h, int integrate_energy,
-                int integrate_sml, double* ax, double* ay, double* az, double* drhodt,
+                int integrate_sml, int kernel, double* ax, double* ay, double* az, double* drhodt,
                 double* dedt, double* dsmldt, const double* bal) {
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < n; ++i) {
@@ -831,7 +875,7 @@ void orc_forces(const double* x, const double* y, const double* z, const double*
             double sml = avg_h ? 0.5 * (h[i] + h[j]) : h[i];
             double dr[3] = {x[i] - x[j], y[i] - y[j], z[i] - z[j]};
             double W, dWdx[3], dWdr;
-            cubic(&W, dWdx, &dWdr, dr, sml);
+            skern(kernel, &W, dWdx, &dWdr, dr, sml);
             double dv[3] = {vx[i] - vx[j], vy[i] - vy[j], vz[i] - vz[j]};
             double vvnablaW = dv[0] * dWdx[0] + dv[1] * dWdx[1] + dv[2] * dWdx[2];
             double rr = 0, vr = 0;
@@ -925,6 +969,70 @@ int orc_variable_h(const double* x, const double* y, const double* z, double* h,
     return sweeps;
 }
 
+// Neighbour-band repair of this library (no counterpart in the reference,
+// whose variable-h iteration, src/sph/sph.cu:739-961, leaves particles whose
+// count drifted out of |n - target| < tol after they stopped, or that hit the
+// iteration limit, where they are).  Up to `rounds` times: counts with the
+// pair rule d^2 < h_i^2 && d^2 < h_j^2; every out-of-band particle i picks,
+// with all other h frozen, the h that gives it `want` neighbours (target +
+// tol - 2 from above, target - tol + 2 from below): candidates j != i with
+// d^2 < rad^2 and d^2 < h_j^2, rad = h_i from above, 1.5 h_i (2 h_i when the
+// count is below half of want) from below; more than 256 candidates shrink
+// rad by 0.8 (at most 5 tries, then h stays); more than want candidates give
+// the midpoint of the want-th and (want+1)-th smallest distances, fewer give
+// rad.  From below, rad is capped at twice the h the particle had before the
+// first round: a particle whose neighbours' h do not reach it (d >= h_j, at a
+// free surface) cannot gain pairs by its own h alone, and its h must not
+// grow without bound.  All picks of a round apply at once.  h is updated in
+// place; returns the out-of-band count before the first round.
+int orc_band_fixup(const double* x, const double* y, const double* z, double* h, int n, int target, int tol,
+                   int rounds) {
+    const int kCap = 256;
+    int before = -1;
+    std::vector<long> off(n + 1);
+    const std::vector<double> h0(h, h + n);
+    for (int r = 0; r < rounds; ++r) {
+        orc_frnn(x, y, z, h, n, off.data(), nullptr);
+        std::vector<int> out;
+        for (int i = 0; i < n; ++i)
+            if (std::abs((int)(off[i + 1] - off[i]) - target) >= tol) out.push_back(i);
+        if (r == 0) before = (int)out.size();
+        if (out.empty()) break;
+        std::vector<double> hn(h, h + n);
+#pragma omp parallel for schedule(dynamic, 16)
+        for (size_t q = 0; q < out.size(); ++q) {
+            const int i = out[q];
+            const int cnt = (int)(off[i + 1] - off[i]);
+            const bool above = cnt >= target + tol;
+            const int want = above ? target + tol - 2 : target - tol + 2;
+            double rad = above ? h[i] : std::min(2 * cnt >= want ? 1.5 * h[i] : 2.0 * h[i], 2.0 * h0[i]);
+            std::vector<double> c;
+            for (int attempt = 0; attempt < 5; ++attempt) {
+                c.clear();
+                const double rad2 = rad * rad;
+                for (int j = 0; j < n; ++j) {
+                    if (j == i) continue;
+                    const double dx = x[i] - x[j], dy = y[i] - y[j], dz = z[i] - z[j];
+                    const double d = dx * dx + dy * dy + dz * dz;
+                    if (d < rad2 && d < h[j] * h[j]) c.push_back(d);
+                }
+                if ((int)c.size() <= kCap) {
+                    if ((int)c.size() > want) {
+                        std::sort(c.begin(), c.end());
+                        hn[i] = 0.5 * (std::sqrt(c[want - 1]) + std::sqrt(c[want]));
+                    } else {
+                        hn[i] = rad;
+                    }
+                    break;
+                }
+                rad = 0.8 * rad;
+            }
+        }
+        for (int i = 0; i < n; ++i) h[i] = hn[i];
+    }
+    return before;
+}
+
 // ---------------------------------------------------------- integrators ---
 // LeapfrogNS::Kernel::updateX / updateV (device_leapfrog.cu:4-58).
 void orc_leapfrog_x(int n, double dt, double* x, double* y, double* z, const double* vx,
@@ -943,6 +1051,29 @@ void orc_leapfrog_v(int n, double dt, double* vx, double* vy, double* vz, const 
         vx[i] += 0.5 * dt * (gax[i] + gax_old[i]);
         vy[i] += 0.5 * dt * (gay[i] + gay_old[i]);
         vz[i] += 0.5 * dt * (gaz[i] + gaz_old[i]);
+    }
+}
+
+// ExplicitEulerNS::Kernel::update (device_explicit_euler.cu:4-54): v += dt
+// (a + g), then x += dt v with the new v; rho, e (floored at 1e-50) and h
+// from their rates when integrated.  a (SPH) and g (gravity) enter only when
+// their physics is on (the reference adds zero arrays otherwise).
+void orc_euler(int n, double dt, int gravity, int sph, int int_rho, int int_e, int int_sml, double* x,
+               double* y, double* z, double* vx, double* vy, double* vz, const double* ax, const double* ay,
+               const double* az, const double* gax, const double* gay, const double* gaz, double* rho,
+               const double* drhodt, double* e, const double* dedt, double* sml, const double* dsmldt) {
+    for (int i = 0; i < n; ++i) {
+        double a[3] = {0, 0, 0};
+        if (sph) { a[0] = ax[i]; a[1] = ay[i]; a[2] = az[i]; }
+        if (gravity) { a[0] += gax[i]; a[1] += gay[i]; a[2] += gaz[i]; }
+        vx[i] += dt * a[0]; vy[i] += dt * a[1]; vz[i] += dt * a[2];
+        x[i] += dt * vx[i]; y[i] += dt * vy[i]; z[i] += dt * vz[i];
+        if (sph && int_rho) rho[i] = rho[i] + dt * drhodt[i];
+        if (sph && int_e) {
+            e[i] += dt * dedt[i];
+            if (e[i] < 1e-50) e[i] = 1e-50;
+        }
+        if (sph && int_sml) sml[i] = sml[i] + dt * dsmldt[i];
     }
 }
 

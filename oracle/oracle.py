@@ -57,14 +57,18 @@ def lib():
         L.orc_direct.argtypes = [_d, _d, _d, _d, ctypes.c_int, _i, ctypes.c_int, ctypes.c_double,
                                  _d, _d, _d, _d]
         L.orc_frnn.argtypes = [_d, _d, _d, _d, ctypes.c_int, _l, _i]
-        L.orc_density.argtypes = [_d, _d, _d, _d, _d, ctypes.c_int, _l, _i, ctypes.c_int, _d]
+        L.orc_density.argtypes = [_d, _d, _d, _d, _d, ctypes.c_int, _l, _i, ctypes.c_int, ctypes.c_int, _d]
         L.orc_eos.argtypes = [ctypes.c_int, ctypes.c_int, _d, _d, _d, _d, _d]
         L.orc_forces.argtypes = [_d] * 11 + [ctypes.c_int, _l, _i, ctypes.c_double, ctypes.c_double,
-                                             ctypes.c_int, ctypes.c_int, ctypes.c_int] + [_d] * 7
-        L.orc_balsara.argtypes = [_d] * 10 + [ctypes.c_int, _l, _i, ctypes.c_int, _d, _d, _d]
+                                             ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [_d] * 7
+        L.orc_balsara.argtypes = [_d] * 10 + [ctypes.c_int, _l, _i, ctypes.c_int, ctypes.c_int, _d, _d, _d]
         L.orc_variable_h.argtypes = [_d, _d, _d, _d, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int, ctypes.c_int, _i]
         L.orc_variable_h.restype = ctypes.c_int
+        L.orc_band_fixup.argtypes = [_d, _d, _d, _d, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.orc_band_fixup.restype = ctypes.c_int
+        L.orc_euler.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                ctypes.c_int, ctypes.c_int] + [_d] * 18
         L.orc_leapfrog_x.argtypes = [ctypes.c_int, ctypes.c_double] + [_d] * 12
         L.orc_leapfrog_v.argtypes = [ctypes.c_int, ctypes.c_double] + [_d] * 9
         L.orc_num_threads.restype = ctypes.c_int
@@ -210,17 +214,20 @@ def frnn(x, y, z, h):
     return off, nbr
 
 
-def density(x, y, z, m, h, off, nbr, avg_h=False):
+def density(x, y, z, m, h, off, nbr, avg_h=False, kernel=1):
+    """kernel: 0 spiky, 1 cubic spline, 2/3/4 Wendland C2/C4/C6."""
     x, y, z, m, h = _f64(x), _f64(y), _f64(z), _f64(m), _f64(h)
     rho = np.zeros(len(x))
     lib().orc_density(_p(x), _p(y), _p(z), _p(m), _p(h), len(x), _p(off, _l), _p(nbr, _i),
-                      int(avg_h), _p(rho))
+                      int(avg_h), int(kernel), _p(rho))
     return rho
 
 
-def eos(eos_type, par, rho, e, p_prev):
+def eos(eos_type, par, rho, e, p_prev, si_units=False):
+    """par = (K, gamma, rho_0, bulk_modulus, n); the Murnaghan and isothermal
+    sound speeds are the constants of initializeSoundSpeed."""
     n = len(rho)
-    par = _f64(par)
+    par = np.concatenate([_f64(par)[:5], np.zeros(max(0, 5 - len(par))), [1.0 if si_units else 0.0]])
     rho, e = _f64(rho), _f64(e)
     p = np.array(p_prev, dtype=np.float64, copy=True)
     cs = np.zeros(n)
@@ -229,25 +236,40 @@ def eos(eos_type, par, rho, e, p_prev):
 
 
 def forces(x, y, z, vx, vy, vz, m, h, rho, p, cs, off, nbr, alpha, beta, avg_h=False,
-           integrate_energy=True, integrate_sml=False, bal=None):
+           integrate_energy=True, integrate_sml=False, bal=None, kernel=1):
     arrs = [_f64(a) for a in (x, y, z, vx, vy, vz, m, h, rho, p, cs)]
     n = len(x)
     outs = [np.zeros(n) for _ in range(6)]
     b = _f64(bal) if bal is not None else None
     lib().orc_forces(*[_p(a) for a in arrs], n, _p(off, _l), _p(nbr, _i), float(alpha),
-                     float(beta), int(avg_h), int(integrate_energy), int(integrate_sml),
+                     float(beta), int(avg_h), int(integrate_energy), int(integrate_sml), int(kernel),
                      *[_p(o) for o in outs], _p(b) if b is not None else None)
     return outs
 
 
-def balsara(x, y, z, vx, vy, vz, m, h, rho, cs, off, nbr, avg_h=False):
+def balsara(x, y, z, vx, vy, vz, m, h, rho, cs, off, nbr, avg_h=False, kernel=1):
     """Balsara switch: (div v, curl v [n x 3], f)."""
     arrs = [_f64(a) for a in (x, y, z, vx, vy, vz, m, h, rho, cs)]
     n = len(x)
     divv, curl, f = np.zeros(n), np.zeros((n, 3)), np.zeros(n)
-    lib().orc_balsara(*[_p(a) for a in arrs], n, _p(off, _l), _p(nbr, _i), int(avg_h), _p(divv), _p(curl),
-                      _p(f))
+    lib().orc_balsara(*[_p(a) for a in arrs], n, _p(off, _l), _p(nbr, _i), int(avg_h), int(kernel), _p(divv),
+                      _p(curl), _p(f))
     return divv, curl, f
+
+
+def euler(st, dt, gravity=True, sph=True, integrate_density=False, integrate_energy=False,
+          integrate_sml=False):
+    """ExplicitEulerNS::Kernel::update on a dict of float64 arrays (copied)."""
+    out = {k: np.array(v, dtype=np.float64, copy=True) for k, v in st.items()}
+    n = len(out["x"])
+    z = np.zeros(n)
+    names = ["x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "g_ax", "g_ay", "g_az", "rho", "drhodt", "e",
+             "dedt", "sml", "dsmldt"]
+    for k in names:
+        out.setdefault(k, z.copy())
+    lib().orc_euler(n, float(dt), int(gravity), int(sph), int(integrate_density), int(integrate_energy),
+                    int(integrate_sml), *[_p(out[k]) for k in names])
+    return out
 
 
 def variable_h(x, y, z, h, target, tol=5, max_nb=180, max_iter=5):
@@ -257,6 +279,15 @@ def variable_h(x, y, z, h, target, tol=5, max_nb=180, max_iter=5):
     sweeps = lib().orc_variable_h(_p(x), _p(y), _p(z), _p(h), len(x), int(target), int(tol),
                                   int(max_nb), int(max_iter), _p(cnt, _i))
     return h, cnt, sweeps
+
+
+def band_fixup(x, y, z, h, target, tol=5, rounds=8):
+    """Neighbour-band repair rounds on h (returns (h, out-of-band count before
+    the first round))."""
+    x, y, z = _f64(x), _f64(y), _f64(z)
+    h = np.array(h, dtype=np.float64, copy=True)
+    before = lib().orc_band_fixup(_p(x), _p(y), _p(z), _p(h), len(x), int(target), int(tol), int(rounds))
+    return h, before
 
 
 def quad(tree, max_level=21):

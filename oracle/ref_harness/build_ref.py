@@ -1,5 +1,6 @@
 """Build the reference harness: milupHPC's own CUDA sources, compiled
-unmodified where they lie under /root/reference, plus ref_driver.cu, into
+unmodified where they lie (the tree named by MHPC_REFERENCE, by default
+/root/reference), plus ref_driver.cu, into
 oracle/_ref/ref_gravity and oracle/_ref/ref_sph.
 
 TEST INFRASTRUCTURE ONLY.  The reference selects its physics with a
@@ -15,7 +16,8 @@ import os
 import subprocess
 import sys
 
-REF = "/root/reference"
+# the milupHPC source tree (read only): MHPC_REFERENCE, default /root/reference
+REF = os.environ.get("MHPC_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(os.path.dirname(HERE), "_ref")
 

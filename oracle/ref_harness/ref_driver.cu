@@ -14,6 +14,13 @@
 // pinned through the tree instead (every particle's path through the
 // reference tree is its key prefix).
 //
+// Timing (gravity build): with a third argument K > 0 the driver runs the
+// whole sequence above once more untimed, then K more times between CUDA
+// events (resetArrays, computeBoundingBox, buildTree, calculateCentersOfMass
+// 21..1, prepareSorting + sortArray, computeForces_v2; each reference launch
+// wrapper synchronises the device, as in the reference) and prints one line
+// `time_ms <stage> <mean ms>` per stage and for the total.
+//
 // Input (little-endian binary): int32 n, int32 flags, double theta, double eps2,
 // double params[8], then x, y, z, m (n doubles each), then (gravity) keys
 // (n uint64) or (SPH) vx, vy, vz, sml, e, p, cs (n doubles each).
@@ -74,7 +81,8 @@ static std::vector<T> dl(const T* d, size_t n) {
 }
 
 int main(int argc, char** argv) {
-    if (argc != 3) { std::fprintf(stderr, "usage: %s input output\n", argv[0]); return 1; }
+    if (argc != 3 && argc != 4) { std::fprintf(stderr, "usage: %s input output [repeats]\n", argv[0]); return 1; }
+    const int repeats = argc == 4 ? std::atoi(argv[3]) : 0;
     FILE* fi = std::fopen(argv[1], "rb");
     if (!fi) return 1;
     int n, flags;
@@ -83,14 +91,19 @@ int main(int argc, char** argv) {
     std::vector<double> x(n), y(n), z(n), m(n);
     rd(fi, x.data(), n); rd(fi, y.data(), n); rd(fi, z.data(), n); rd(fi, m.data(), n);
     // Input conditions the caller (tests/golden/make_golden.py) checks on the
-    // CPU before writing the file: n a multiple of 256 in [1024, 65536] (the
-    // reference kernels call __syncthreads inside their per-particle loops
-    // and read x[0..1023] in computeBoundingBox), pairwise distinct 21-level
+    // CPU before writing the file: n a multiple of 256 in [1024, 65536], or a
+    // multiple of 65536 (the reference kernels call __syncthreads inside their
+    // per-particle loops, so every thread of a block must run the same number
+    // of them: computeForces_v2 strides by its 256 x 256 threads; and
+    // computeBoundingBox reads x[0..1023]), pairwise distinct 21-level
     // keys and a shallow tree (buildTree subdivides until two particles
     // separate; computeForces_v2 keeps 128 stack entries per warp without a
     // bound check), fewer than MAX_NUM_INTERACTIONS neighbours per particle
     // (fixedRadiusNN v0 stores without a bound check).
-    if (n < 1024 || n > 65536 || n % 256 != 0) { std::fprintf(stderr, "unsupported n\n"); return 1; }
+    if (n < 1024 || n % 256 != 0 || (n > 65536 && n % 65536 != 0) || n > (1 << 20)) {
+        std::fprintf(stderr, "unsupported n\n");
+        return 1;
+    }
     const int numNodes = 2 * n + 20000;
     // Every particle array is sized numNodes: fixedRadiusNN v0 reads sml[] at
     // cell indices, which lie past the particle count.
@@ -153,6 +166,45 @@ int main(int argc, char** argv) {
     wr(fo, dl(ph.d_g_ax, n).data(), n);
     wr(fo, dl(ph.d_g_ay, n).data(), n);
     wr(fo, dl(ph.d_g_az, n).data(), n);
+    if (repeats > 0) {
+        // stages of one gravity right-hand side, the first pass untimed
+        const char* names[6] = {"reset_bbox", "build_tree", "centers_of_mass", "sort", "forces_v2", "total"};
+        double acc[6] = {0, 0, 0, 0, 0, 0};
+        cudaEvent_t ev[6];
+        for (int k = 0; k < 6; ++k) CK(cudaEventCreate(&ev[k]));
+        for (int rep = 0; rep <= repeats; ++rep) {
+            CK(cudaEventRecord(ev[0]));
+            Kernel::Launch::resetArrays(th.d_tree, ph.d_particles, th.d_mutex, n, numNodes, false);
+            TreeNS::Kernel::Launch::computeBoundingBox(th.d_tree, ph.d_particles, th.d_mutex, n, 256, false);
+            CK(cudaEventRecord(ev[1]));
+            TreeNS::Kernel::Launch::buildTree(th.d_tree, ph.d_particles, n, n, false);
+            CK(cudaEventRecord(ev[2]));
+            for (int level = MAX_LEVEL; level > 0; --level)
+                TreeNS::Kernel::Launch::calculateCentersOfMass(th.d_tree, ph.d_particles, n, level, false);
+            CK(cudaEventRecord(ev[3]));
+            CK(cudaMemcpy(d_keys, keys.data(), sizeof(keyType) * n, cudaMemcpyHostToDevice));
+            TreeNS::Kernel::Launch::prepareSorting(th.d_tree, ph.d_particles, n, n);
+            HelperNS::sortArray(th.d_start, th.d_sorted, d_keys, d_keys_out, n);
+            CK(cudaEventRecord(ev[4]));
+            Gravity::Kernel::Launch::computeForces_v2(th.d_tree, ph.d_particles, radius, n, n, 256, 32, 128, nullptr,
+                                                     theta, eps2, false);
+            CK(cudaEventRecord(ev[5]));
+            CK(cudaEventSynchronize(ev[5]));
+            int idx2 = 0;
+            CK(cudaMemcpy(&idx2, th.d_index, sizeof(int), cudaMemcpyDeviceToHost));
+            if (idx2 != index) { std::fprintf(stderr, "tree changed between runs\n"); return 5; }
+            if (rep == 0) continue;
+            for (int k = 0; k < 5; ++k) {
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+                acc[k] += ms;
+            }
+            float tot = 0.f;
+            CK(cudaEventElapsedTime(&tot, ev[0], ev[5]));
+            acc[5] += tot;
+        }
+        for (int k = 0; k < 6; ++k) std::printf("time_ms %s %.6f\n", names[k], acc[k] / repeats);
+    }
     cudaFree(d_keys);
     cudaFree(d_keys_out);
 #endif

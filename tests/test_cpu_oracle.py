@@ -7,7 +7,7 @@ is pinned here by (a) closed-form known answers of the key construction
 reference's own tree invariant `test_localTree` (tree.cu:1983-2080: node mass
 = sum of children, COM consistent), (c) the limit theta -> 0 of the tree walk
 equalling direct summation, and (d) the golden fixtures produced by running
-the reference's own kernels (tests/test_cpu_golden.py).
+the reference's own kernels (tests/test_ref_golden.py).
 """
 import ctypes
 import os
