@@ -510,9 +510,14 @@ __device__ __forceinline__ void eval_leaves_sel(const ListSmem& S, int count, co
 }
 
 constexpr int kListBlock = 128;
+// resident blocks per SM the list walk is compiled for (register budget)
+#ifndef MHPC_LISTS_MIN_BLOCKS
+#define MHPC_LISTS_MIN_BLOCKS 1
+#endif
 
 template <bool kGuard, bool kRel, bool kPot>
-__global__ void __launch_bounds__(kListBlock) k_grav_lists(TreeDev T, GravParams P, const double* __restrict__ sx,
+__global__ void __launch_bounds__(kListBlock, MHPC_LISTS_MIN_BLOCKS) k_grav_lists(TreeDev T, GravParams P,
+                                                                                 const double* __restrict__ sx,
                                                            const double* __restrict__ sy,
                                                            const double* __restrict__ sz,
                                                            const double* __restrict__ sh,

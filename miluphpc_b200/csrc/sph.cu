@@ -11,6 +11,7 @@
 // (j != i), d^2 formed without FMA contraction like the reference build.  All
 // pruning is conservative, so the neighbour set equals the brute-force set.
 #include "sph.cuh"
+#include "walk.cuh"
 
 namespace {
 
@@ -420,147 +421,45 @@ __global__ void __launch_bounds__(kBlock, 6) k_frnn(TreeDev T, int n, int maxnb,
 }
 
 // Count walk for sparse lists (later variable-h sweeps, where the particles
-// still iterating are scattered, so a shared group box would be large): 8
-// lanes per particle, 4 particles per warp.  Each particle has its own stack
-// in shared memory; every step its 8 lanes pop up to 8 nodes, prune those
-// whose box does not come within h_i of the particle or whose largest h_j
-// cannot reach it, push the children of the others, and test the particles
-// of overlapping leaves, small cells and shared-key buckets 8 at a time.
-// Same stack bound as the group walk (a pop of k nodes pushes at most 8k).
-constexpr int kSubStack = 256;
-constexpr int kSubReserve = 7 * 22 + 8;
+// still iterating are scattered, so a shared group box would be large): one
+// warp per particle (warp_walk), its lanes testing 32 candidates at a time
+// with the reference's pair rule.  The longest walks (particles with a large
+// h) set a sweep's time, so each particle gets a whole warp.
+struct CountVisit {
+    const double *sx, *sy, *sz, *sh;
+    double px, py, pz, hi2;
+    long s;
+    int* k;
+    __device__ void operator()(int j) const {
+        if (j == s) return;
+        const double d = d2_exact(px - __ldg(sx + j), py - __ldg(sy + j), pz - __ldg(sz + j));
+        const double hj = __ldg(sh + j);
+        *k += (d < hi2 && d < hj * hj);
+    }
+};
 
-__global__ void __launch_bounds__(kBlock) k_count_sub(TreeDev T, const double* __restrict__ sx,
-                                                      const double* __restrict__ sy, const double* __restrict__ sz,
-                                                      const double* __restrict__ sh, const int* __restrict__ list,
-                                                      const int* __restrict__ list_count,
-                                                      const float* __restrict__ node_hmax, int* __restrict__ count,
-                                                      DevStatus* st) {
-    __shared__ int stk[kWarps][4][kSubStack];
-    __shared__ int rfs[kWarps][4][8], rends[kWarps][4][8];
+__global__ void __launch_bounds__(kBlock) k_count_warp(TreeDev T, const double* __restrict__ sx,
+                                                       const double* __restrict__ sy, const double* __restrict__ sz,
+                                                       const double* __restrict__ sh, const int* __restrict__ list,
+                                                       const int* __restrict__ list_count,
+                                                       const float* __restrict__ node_hmax, int* __restrict__ count,
+                                                       DevStatus* st) {
+    __shared__ int stk[kWarps][kWalkStack];
+    __shared__ int rfs[kWarps][32], rends[kWarps][32];
     if (st->code) return;
     const int M = *T.nodes;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, sg = lane >> 3, r = lane & 7;
-    const unsigned seg = 0xffu << (8 * sg);
-    const unsigned lt = (1u << lane) - 1u;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const long cnt = *list_count;
     const long nwarps = (long)gridDim.x * kWarps;
-    // warp-stride loop over groups of 4 list entries (the grid does not
-    // depend on the list length, which only the device knows)
-    for (long gw = ((long)blockIdx.x * kBlock + threadIdx.x) >> 5; gw * 4 < cnt; gw += nwarps) {
-        const long q = gw * 4 + sg;
-        const bool valid = q < cnt;
-        const int s = valid ? list[q] : 0;
-        const double px = sx[s], py = sy[s], pz = sz[s], hi = sh[s], hi2 = hi * hi;
-        const float lx = __double2float_rd(px - hi), ly = __double2float_rd(py - hi), lz = __double2float_rd(pz - hi);
-        const float ux = __double2float_ru(px + hi), uy = __double2float_ru(py + hi), uz = __double2float_ru(pz + hi);
-        const float fx0 = __double2float_rd(px), fy0 = __double2float_rd(py), fz0 = __double2float_rd(pz);
-        const float fx1 = __double2float_ru(px), fy1 = __double2float_ru(py), fz1 = __double2float_ru(pz);
-        int* S = stk[w][sg];
-        int* RF = rfs[w][sg];
-        int* RE = rends[w][sg];
-        // the root's children: node 0 and its skip chain
-        int top = 0;
-        if (valid && r == 0) {
-            int c = 0;
-            while (c < M && top < 8) { S[top++] = c; c = __ldg(&T.link[c].x); }
-            if (c < M) set_status(st, MHPC_ERR_DEPTH, 5);
-        }
-        top = __shfl_sync(MHPC_FULL, top, lane & ~7);
-        __syncwarp();
+    for (long q = ((long)blockIdx.x * kBlock + threadIdx.x) >> 5; q < cnt; q += nwarps) {
+        const int s = list[q];
+        const double px = sx[s], py = sy[s], pz = sz[s], hi = sh[s];
         int k = 0;
-        while (__any_sync(MHPC_FULL, top > 0)) {
-            const int room = (kSubStack - kSubReserve - top) / 7;
-            int kk = top < 8 ? top : 8;
-            if (kk > room) kk = room > 1 ? room : 1;
-            if (top == 0) kk = 0;
-            const bool act = r < kk;
-            const int nd = act ? S[top - 1 - r] : 0;
-            __syncwarp();
-            top -= kk;
-            int rf = 0, rlen = 0, kmask = 0;
-            if (act) {
-                const int2 lk = __ldg(T.link + nd);
-                const float4 bl = __ldg(T.bmin + nd), bh = __ldg(T.bmax + nd);
-                const float hn = __ldg(node_hmax + nd);
-                const bool overlap =
-                    !(bh.x < lx || bl.x > ux || bh.y < ly || bl.y > uy || bh.z < lz || bl.z > uz) &&
-                    !(__fadd_ru(bh.x, hn) < fx0 || __fadd_rd(bl.x, -hn) > fx1 || __fadd_ru(bh.y, hn) < fy0 ||
-                      __fadd_rd(bl.y, -hn) > fy1 || __fadd_ru(bh.z, hn) < fz0 || __fadd_rd(bl.z, -hn) > fz1);
-                if (overlap) {
-                    rf = __ldg(T.first + nd);
-                    if (lk.y & ND_LEAF) {
-                        rlen = 1;
-                    } else {
-                        const int l = __ldg(T.last + nd);
-                        const int km = __ldg(T.kmask + nd);
-                        if (l - rf + 1 <= kSmall || (km & 0x100)) rlen = l - rf + 1;
-                        else kmask = km & 0xff;
-                    }
-                }
-            }
-            // push children (scan within the 8-lane segment)
-            const int nkid = __popc(kmask);
-            int incl = nkid;
-    #pragma unroll
-            for (int o = 1; o < 8; o <<= 1) {
-                const int v = __shfl_up_sync(MHPC_FULL, incl, o, 8);
-                if (r >= o) incl += v;
-            }
-            const int total = __shfl_sync(MHPC_FULL, incl, 7, 8);
-            const bool over = top + total > kSubStack;  // unreachable by the bound on kk
-            if (over && r == 0 && valid) set_status(st, MHPC_ERR_DEPTH, 6);
-            if (nkid && !over) {
-                const int4 k0 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)nd));
-                const int4 k1 = __ldg(reinterpret_cast<const int4*>(T.kids + 8 * (size_t)nd) + 1);
-                const int all[8] = {k0.x, k0.y, k0.z, k0.w, k1.x, k1.y, k1.z, k1.w};
-                int wpos = top + incl - nkid;
-    #pragma unroll
-                for (int d = 0; d < 8; ++d)
-                    if ((kmask >> d) & 1) S[wpos++] = all[d];
-            }
-            top = over ? 0 : top + total;
-            // staged ranges of this particle, with running ends
-            int rincl = rlen;
-    #pragma unroll
-            for (int o = 1; o < 8; o <<= 1) {
-                const int v = __shfl_up_sync(MHPC_FULL, rincl, o, 8);
-                if (r >= o) rincl += v;
-            }
-            const int ncand = __shfl_sync(MHPC_FULL, rincl, 7, 8);
-            const unsigned br = __ballot_sync(MHPC_FULL, rlen > 0) & seg;
-            const int nr = __popc(br);
-            if (rlen > 0) {
-                const int slot = __popc(br & lt);
-                RF[slot] = rf;
-                RE[slot] = rincl;
-            }
-            __syncwarp();
-            int maxc = ncand;
-            maxc = max(maxc, __shfl_xor_sync(MHPC_FULL, maxc, 8));
-            maxc = max(maxc, __shfl_xor_sync(MHPC_FULL, maxc, 16));
-            for (int c0 = 0; c0 < maxc; c0 += 8) {
-                const int c = c0 + r;
-                if (c < ncand) {
-                    int lo = 0, hr = nr - 1;
-                    while (lo < hr) {
-                        const int mid = (lo + hr) >> 1;
-                        if (RE[mid] > c) hr = mid;
-                        else lo = mid + 1;
-                    }
-                    const int j = RF[lo] + c - (lo ? RE[lo - 1] : 0);
-                    const double dx = px - __ldg(sx + j), dy = py - __ldg(sy + j), dz = pz - __ldg(sz + j);
-                    const double d = d2_exact(dx, dy, dz);
-                    const double hj = __ldg(sh + j);
-                    k += (j != s && d < hi2 && d < hj * hj);
-                }
-            }
-            __syncwarp();
-        }
-        k += __shfl_xor_sync(MHPC_FULL, k, 1);
-        k += __shfl_xor_sync(MHPC_FULL, k, 2);
-        k += __shfl_xor_sync(MHPC_FULL, k, 4);
-        if (valid && r == 0) count[s] = k;
+        CountVisit v{sx, sy, sz, sh, px, py, pz, hi * hi, (long)s, &k};
+        warp_walk(T, M, true, px, py, pz, hi, node_hmax, stk[w], rfs[w], rends[w], st, v);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) k += __shfl_xor_sync(MHPC_FULL, k, o);
+        if (lane == 0) count[s] = k;
         __syncwarp();
     }
 }
@@ -969,8 +868,8 @@ int sph_variable_h(const TreeDev& T, const SphParams& P, const double* x, const 
             k_frnn<1><<<(int)blocks, kBlock, 0, s>>>(T, P.n, P.maxnb, x, y, z, B.hold, B.list, list_count, T.hmax,
                                                       nullptr, B.count, st);
         } else {
-            // later sweeps: the few particles still iterating, 8 lanes each
-            k_count_sub<<<148 * 16, kBlock, 0, s>>>(T, x, y, z, B.hold, B.list, list_count, T.hmax, B.count, st);
+            // later sweeps: the few particles still iterating, a warp each
+            k_count_warp<<<148 * 8, kBlock, 0, s>>>(T, x, y, z, B.hold, B.list, list_count, T.hmax, B.count, st);
         }
         k_vh_update<<<g, 256, 0, s>>>(B.list, list_count, B.count, h, B.hold, B.done, B.nit, target, tol, max_iter,
                                       P.maxnb, T.hmax, T.leaf_node, T.parent);

@@ -1006,6 +1006,7 @@ int orc_band_fixup(const double* x, const double* y, const double* z, double* h,
             const bool above = cnt >= target + tol;
             const int want = above ? target + tol - 2 : target - tol + 2;
             double rad = above ? h[i] : std::min(2 * cnt >= want ? 1.5 * h[i] : 2.0 * h[i], 2.0 * h0[i]);
+            if (!above && rad <= h[i]) continue;  // at the cap: no pair to gain, h stays
             std::vector<double> c;
             for (int attempt = 0; attempt < 5; ++attempt) {
                 c.clear();

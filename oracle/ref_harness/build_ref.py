@@ -1,7 +1,8 @@
 """Build the reference harness: milupHPC's own CUDA sources, compiled
 unmodified where they lie (the tree named by MHPC_REFERENCE, by default
 /root/reference), plus ref_driver.cu, into
-oracle/_ref/ref_gravity and oracle/_ref/ref_sph.
+oracle/_ref/ref_gravity, oracle/_ref/ref_sph, oracle/_ref/ref_sph_bal and
+oracle/_ref/ref_integrators (the integrator update kernels, ref_integrators.cu).
 
 TEST INFRASTRUCTURE ONLY.  The reference selects its physics with a
 parameter.h per test case (testcases/*/parameter.h, copied over
@@ -30,18 +31,21 @@ SPH_SRCS = COMMON + ["src/materials/material_handler.cpp", "src/sph/sph.cu", "sr
                      "src/sph/soundspeed.cu", "src/sph/pressure.cu", "src/sph/internal_forces.cu",
                      "src/sph/kernel.cu", "src/sph/kernel_handler.cu", "src/sph/stress.cu",
                      "src/sph/artificial_stress.cu", "src/sph/viscosity.cu"]
-# name: (test-case parameter.h, extra pre-included header of this directory or None, sources)
+INTEG_SRCS = SPH_SRCS + ["src/integrator/device_leapfrog.cu", "src/integrator/device_explicit_euler.cu",
+                         "src/integrator/device_predictor_corrector_euler.cu"]
+# name: (test-case parameter.h, extra pre-included header of this directory or None, sources, driver)
 BUILDS = {
-    "gravity": ("testcases/plummer/parameter.h", None, COMMON + ["src/gravity/gravity.cu"]),
-    "sph": ("testcases/sedov/parameter.h", None, SPH_SRCS),
-    "sph_bal": ("testcases/sedov/parameter.h", "balsara_on.h", SPH_SRCS),
+    "gravity": ("testcases/plummer/parameter.h", None, COMMON + ["src/gravity/gravity.cu"], "ref_driver.cu"),
+    "sph": ("testcases/sedov/parameter.h", None, SPH_SRCS, "ref_driver.cu"),
+    "sph_bal": ("testcases/sedov/parameter.h", "balsara_on.h", SPH_SRCS, "ref_driver.cu"),
+    "integrators": ("testcases/sedov/parameter.h", None, INTEG_SRCS, "ref_integrators.cu"),
 }
 
 
 def build(verbose=False):
     if not os.path.isdir(REF):
         return False
-    for name, (param, extra, srcs) in BUILDS.items():
+    for name, (param, extra, srcs, driver) in BUILDS.items():
         objdir = os.path.join(OUT, "obj_" + name)
         os.makedirs(objdir, exist_ok=True)
         exe = os.path.join(OUT, "ref_" + name)
@@ -51,7 +55,7 @@ def build(verbose=False):
             flags += ["-include", os.path.join(HERE, extra)]
         flags += ["-I" + os.path.join(HERE, "shim"), "-I" + os.path.join(REF, "include")]
         objs = []
-        for s in srcs + [os.path.join(HERE, "ref_driver.cu")]:
+        for s in srcs + [os.path.join(HERE, driver)]:
             src = s if os.path.isabs(s) else os.path.join(REF, s)
             obj = os.path.join(objdir, os.path.basename(s).replace(".", "_") + ".o")
             objs.append(obj)

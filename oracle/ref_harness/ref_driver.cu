@@ -80,7 +80,30 @@ static std::vector<T> dl(const T* d, size_t n) {
     return h;
 }
 
+// Host only, no GPU: `--hilbert in out` converts 21-level Lebesgue keys
+// (int32 n, then n uint64) to Hilbert keys with the reference's
+// host-callable KeyNS::lebesgue2hilbert(key, MAX_LEVEL, MAX_LEVEL), the
+// conversion Tree::getParticleKey applies (tree.cu:233), and writes n uint64.
+static int hilbert_keys(const char* in, const char* out) {
+    FILE* fi = std::fopen(in, "rb");
+    if (!fi) return 1;
+    int n = 0;
+    rd(fi, &n, 1);
+    if (n < 0 || n > (1 << 26)) return 1;
+    std::vector<unsigned long long> k(n), h(n);
+    rd(fi, k.data(), n);
+    std::fclose(fi);
+    for (int i = 0; i < n; ++i) h[i] = KeyNS::lebesgue2hilbert((keyType)k[i], MAX_LEVEL, MAX_LEVEL);
+    FILE* fo = std::fopen(out, "wb");
+    if (!fo) return 1;
+    wr(fo, h.data(), n);
+    std::fclose(fo);
+    std::printf("ok hilbert n=%d\n", n);
+    return 0;
+}
+
 int main(int argc, char** argv) {
+    if (argc == 4 && std::strcmp(argv[1], "--hilbert") == 0) return hilbert_keys(argv[2], argv[3]);
     if (argc != 3 && argc != 4) { std::fprintf(stderr, "usage: %s input output [repeats]\n", argv[0]); return 1; }
     const int repeats = argc == 4 ? std::atoi(argv[3]) : 0;
     FILE* fi = std::fopen(argv[1], "rb");

@@ -1,4 +1,5 @@
-"""Generate the reference fixtures ref_gravity_*.npz and ref_sph.npz.
+"""Generate the reference fixtures ref_gravity_*.npz, ref_sph*.npz,
+ref_hilbert.npz (CPU only) and ref_integrators.npz.
 
 The fixtures hold seeded inputs together with the outputs of milupHPC's own
 kernels, run by the reference harness (oracle/_ref/ref_gravity and
@@ -218,6 +219,71 @@ def sph_case(out, run, balsara=False):
     os.remove(fout)
 
 
+def hilbert_case(out, seed=31):
+    """Lebesgue -> Hilbert keys by the reference's own host-callable
+    KeyNS::lebesgue2hilbert (run on the CPU, no GPU): seeded random 63-bit
+    keys, the Lebesgue keys of a seeded Plummer sphere (whose positions are
+    stored, so that the GPU keys can be checked too) and edge keys."""
+    rng = np.random.default_rng(seed)
+    rand = rng.integers(0, 1 << 63, 4096, dtype=np.uint64)
+    P = ics.plummer(4096, seed=seed)
+    bb = O.bbox(P["x"], P["y"], P["z"])
+    pk = O.keys(P["x"], P["y"], P["z"], bb, 0)
+    edge = np.array([0, 1, 7, 8, (1 << 63) - 1, (1 << 60), (1 << 62) + 5, 0o1234567012345670123456],
+                    dtype=np.uint64)
+    leb = np.concatenate([rand, pk, edge])
+    fin = os.path.join(out, "ref_hilbert.in")
+    fout = os.path.join(out, "ref_hilbert.out")
+    with open(fin, "wb") as f:
+        f.write(struct.pack("<i", len(leb)))
+        f.write(np.ascontiguousarray(leb, dtype="<u8").tobytes())
+    subprocess.check_call([os.path.join(REF, "ref_gravity"), "--hilbert", fin, fout])
+    hil = np.frombuffer(open(fout, "rb").read(), dtype="<u8").copy()
+    np.savez_compressed(os.path.join(out, "ref_hilbert.npz"), lebesgue=leb, hilbert=hil, x=P["x"], y=P["y"],
+                        z=P["z"], n_random=len(rand), n_plummer=len(pk))
+    os.remove(fin)
+    os.remove(fout)
+
+
+INTEG_FIELDS = ["x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "g_ax", "g_ay", "g_az", "rho", "drhodt", "e",
+                "dedt", "sml", "dsmldt", "p", "cs", "gx2", "gy2", "gz2", "pax", "pay", "paz"]
+INTEG_OUT = [("euler", ["x", "y", "z", "vx", "vy", "vz", "e", "sml"]),
+             ("leapfrog", ["x", "y", "z", "g_ax_old", "g_ay_old", "g_az_old", "vx", "vy", "vz"]),
+             ("predictor", ["x", "y", "z", "vx", "vy", "vz", "e", "sml", "cs", "p"]),
+             ("corrector", ["x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "e", "dedt", "sml", "dsmldt"])]
+
+
+def integrators_case(out, n=4096, seed=41, dt=3.7e-3):
+    """The reference's integrator update kernels (ref_integrators, Sedov
+    parameter.h: INTEGRATE_ENERGY, INTEGRATE_SML) on a seeded random state:
+    positive e, sml, rho, p, c_s; some dedt negative enough to hit the
+    energy floors (1e-50 in Euler, 1e-6 in the predictor-corrector)."""
+    rng = np.random.default_rng(seed)
+    st = {k: rng.normal(0.0, 1.0, n) for k in INTEG_FIELDS}
+    for k in ("rho", "e", "sml", "p", "cs"):
+        st[k] = np.abs(st[k]) + 0.1
+    st["dedt"][:64] = -1e6
+    if not all(np.isfinite(v).all() for v in st.values()):
+        raise RuntimeError("non-finite input")
+    fin = os.path.join(out, "ref_integrators.in")
+    fout = os.path.join(out, "ref_integrators.out")
+    with open(fin, "wb") as f:
+        f.write(struct.pack("<id", n, dt))
+        for k in INTEG_FIELDS:
+            f.write(np.ascontiguousarray(st[k], dtype="<f8").tobytes())
+    subprocess.check_call([os.path.join(REF, "ref_integrators"), fin, fout])
+    raw = np.frombuffer(open(fout, "rb").read(), dtype="<f8")
+    res, pos = {}, 0
+    for stage, names in INTEG_OUT:
+        for k in names:
+            res[stage + "_" + k] = raw[pos:pos + n].copy()
+            pos += n
+    np.savez_compressed(os.path.join(out, "ref_integrators.npz"), dt=dt, **{"in_" + k: v for k, v in st.items()},
+                        **res)
+    os.remove(fin)
+    os.remove(fout)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=HERE)
@@ -234,6 +300,10 @@ def main():
         sph_case(a.out, run=not a.check_only)
     if only is None or "ref_sph_balsara" in only:
         sph_case(a.out, run=not a.check_only, balsara=True)
+    if (only is None or "ref_hilbert" in only) and not a.check_only:
+        hilbert_case(a.out)
+    if (only is None or "ref_integrators" in only) and not a.check_only:
+        integrators_case(a.out)
 
 
 if __name__ == "__main__":

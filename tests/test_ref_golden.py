@@ -201,3 +201,138 @@ def test_cuda_balsara_matches_reference(cuda):
     for k in ("ax", "ay", "az", "drhodt", "dedt", "dsmldt"):
         close_rates(sim.numpy(k), F[k])
     sim.close()
+
+
+# ------------------------------------------------------------ Hilbert keys --
+# ref_hilbert.npz: Lebesgue keys (seeded random 63-bit keys, a seeded Plummer
+# sphere's keys, edge keys) and their Hilbert keys from the reference's own
+# KeyNS::lebesgue2hilbert(key, 21, 21) (src/subdomain_key_tree/tree.cu:40-53,
+# the conversion of Tree::getParticleKey, tree.cu:233), run on the CPU.
+def test_oracle_hilbert_matches_reference():
+    F = fixture("ref_hilbert")
+    got = np.array([O.lebesgue2hilbert(int(k)) for k in F["lebesgue"]], dtype=np.uint64)
+    assert np.array_equal(got, F["hilbert"])
+
+
+@pytest.mark.gpu
+def test_gpu_hilbert_keys_match_reference(cuda):
+    """The CUDA key kernel (curve 1) on the Plummer positions of the fixture
+    equals the reference's conversion of the same positions' Lebesgue keys."""
+    from tests.test_gpu_parity import gpu_keys
+    F = fixture("ref_hilbert")
+    a, b = int(F["n_random"]), int(F["n_random"] + F["n_plummer"])
+    _, leb = gpu_keys(F["x"], F["y"], F["z"], 0)
+    assert np.array_equal(leb, F["lebesgue"][a:b])
+    _, hil = gpu_keys(F["x"], F["y"], F["z"], 1)
+    assert np.array_equal(hil, F["hilbert"][a:b])
+
+
+# ------------------------------------------------------------- integrators --
+# ref_integrators.npz: a seeded random state and what milupHPC's own update
+# kernels made of it (Sedov parameter.h build: INTEGRATE_ENERGY, INTEGRATE_SML,
+# no INTEGRATE_DENSITY): ExplicitEulerNS::Kernel::update, LeapfrogNS::Kernel::
+# updateX / updateV and PredictorCorrectorEulerNS::Kernel::predictor /
+# corrector (src/integrator/device_explicit_euler.cu:4-54,
+# device_leapfrog.cu:4-58, device_predictor_corrector_euler.cu:130-300).
+# The reference build rounds every product and sum (-fmad=false), so the bar
+# is bit-identical.
+def _integ():
+    F = fixture("ref_integrators")
+    st = {k[3:]: F[k] for k in F if k.startswith("in_")}
+    return F, st, float(F["dt"])
+
+
+def _pc_numpy(st, dt):
+    """The predictor and corrector formulas in elementwise IEEE double."""
+    q = {}
+    for c, v, a, g in (("x", "vx", "ax", "g_ax"), ("y", "vy", "ay", "g_ay"), ("z", "vz", "az", "g_az")):
+        q[c] = st[c] + dt * st[v]
+        q[v] = st[v] + dt * (st[a] + st[g])
+    q["e"] = np.maximum(st["e"] + dt * st["dedt"], 1e-6)
+    q["sml"], q["cs"], q["p"] = st["sml"], st["cs"], st["p"]
+    return q
+
+
+def test_oracle_integrators_match_reference():
+    F, st, dt = _integ()
+    e = O.euler(st, dt, gravity=True, sph=True, integrate_energy=True, integrate_sml=True)
+    for k in ("x", "y", "z", "vx", "vy", "vz", "e", "sml"):
+        assert np.array_equal(e[k], F["euler_" + k]), k
+    ref = {k: np.array(v, copy=True) for k, v in st.items()}
+    for k in ("g_ax_old", "g_ay_old", "g_az_old"):
+        ref[k] = np.zeros_like(ref["x"])
+    p = O._p
+    O.lib().orc_leapfrog_x(len(ref["x"]), dt, *[p(ref[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "g_ax", "g_ay",
+                                                                     "g_az", "g_ax_old", "g_ay_old", "g_az_old")])
+    for k in ("x", "y", "z", "g_ax_old", "g_ay_old", "g_az_old"):
+        assert np.array_equal(ref[k], F["leapfrog_" + k]), k
+    ref["g_ax"], ref["g_ay"], ref["g_az"] = st["gx2"], st["gy2"], st["gz2"]
+    O.lib().orc_leapfrog_v(len(ref["x"]), dt, *[p(np.ascontiguousarray(ref[k])) for k in (
+        "vx", "vy", "vz", "g_ax", "g_ay", "g_az", "g_ax_old", "g_ay_old", "g_az_old")])
+    # orc_leapfrog_v updated ref's own velocity arrays in place
+    for k in ("vx", "vy", "vz"):
+        assert np.array_equal(ref[k], F["leapfrog_" + k]), k
+    q = _pc_numpy(st, dt)
+    for k in ("x", "y", "z", "vx", "vy", "vz", "e", "sml", "cs", "p"):
+        assert np.array_equal(q[k], F["predictor_" + k]), k
+    h = 0.5 * dt
+    pde, pdh = 0.5 * st["dedt"], 0.5 * st["dsmldt"]
+    for c, v, a, g, pa in (("x", "vx", "ax", "g_ax", "pax"), ("y", "vy", "ay", "g_ay", "pay"),
+                           ("z", "vz", "az", "g_az", "paz")):
+        assert np.array_equal(st[c] + h * (q[v] + st[v]), F["corrector_" + c]), c
+        assert np.array_equal(st[v] + h * ((st[pa] + st[a]) + 2 * st[g]), F["corrector_" + v]), v
+        assert np.array_equal(0.5 * (st[pa] + st[a]) + st[g], F["corrector_" + a]), a
+    assert np.array_equal(np.maximum(st["e"] + h * (pde + st["dedt"]), 1e-6), F["corrector_e"])
+    assert np.array_equal(0.5 * (pde + st["dedt"]), F["corrector_dedt"])
+    assert np.array_equal(st["sml"] + h * (pdh + st["dsmldt"]), F["corrector_sml"])
+    assert np.array_equal(0.5 * (pdh + st["dsmldt"]), F["corrector_dsmldt"])
+
+
+@pytest.mark.gpu
+def test_gpu_integrators_match_reference(cuda):
+    """The library's update kernels through mhpc_integrate_euler /
+    _leapfrog / _pc_predictor / _pc_corrector, bit for bit."""
+    import ctypes
+    import torch
+    from miluphpc_b200 import _lib
+    from miluphpc_b200.miluphpc import Miluphpc, material
+    from tests.helpers import sph_cfg
+    F, st, dt = _integ()
+    L = _lib.load()
+    n = len(st["x"])
+    cfg = sph_cfg(gravity=1, integrator=1, integrate_energy=1, integrate_sml=1, integrate_density=0,
+                  max_time_step=1.0)
+    mat = [material(eos_type=9)]
+    sim = Miluphpc(cfg, st, materials=mat)
+    _lib.check(L.mhpc_integrate_euler(sim.ctx, ctypes.byref(sim.soa), dt), "euler")
+    torch.cuda.synchronize()
+    for k in ("x", "y", "z", "vx", "vy", "vz", "e", "sml"):
+        assert np.array_equal(sim.numpy(k), F["euler_" + k]), k
+    sim.close()
+    sim = Miluphpc(cfg, st, materials=mat)
+    _lib.check(L.mhpc_integrate_leapfrog(sim.ctx, ctypes.byref(sim.soa), dt, 0), "leapfrog x")
+    for k, g in (("g_ax", "gx2"), ("g_ay", "gy2"), ("g_az", "gz2")):
+        sim.t[k][:n] = torch.as_tensor(st[g], device=cuda)
+    _lib.check(L.mhpc_integrate_leapfrog(sim.ctx, ctypes.byref(sim.soa), dt, 1), "leapfrog v")
+    torch.cuda.synchronize()
+    for k in ("x", "y", "z", "g_ax_old", "g_ay_old", "g_az_old", "vx", "vy", "vz"):
+        assert np.array_equal(sim.numpy(k), F["leapfrog_" + k]), k
+    sim.close()
+    sim = Miluphpc(cfg, st, materials=mat)
+    q = Miluphpc(cfg, {k: np.zeros(n) for k in ("x",)}, materials=mat)
+    dt_dev = torch.full((1,), dt, dtype=torch.float64, device=cuda)
+    _lib.check(L.mhpc_integrate_pc_predictor(sim.ctx, ctypes.byref(sim.soa), ctypes.byref(q.soa),
+                                             ctypes.c_void_p(dt_dev.data_ptr())), "predictor")
+    torch.cuda.synchronize()
+    for k in ("x", "y", "z", "vx", "vy", "vz", "e", "sml", "cs", "p"):
+        assert np.array_equal(q.numpy(k), F["predictor_" + k]), k
+    for k, v in (("ax", st["pax"]), ("ay", st["pay"]), ("az", st["paz"]), ("dedt", 0.5 * st["dedt"]),
+                 ("dsmldt", 0.5 * st["dsmldt"]), ("drhodt", st["drhodt"])):
+        q.t[k][:n] = torch.as_tensor(v, device=cuda)
+    _lib.check(L.mhpc_integrate_pc_corrector(sim.ctx, ctypes.byref(sim.soa), ctypes.byref(q.soa),
+                                             ctypes.c_void_p(dt_dev.data_ptr())), "corrector")
+    torch.cuda.synchronize()
+    for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "e", "dedt", "sml", "dsmldt"):
+        assert np.array_equal(sim.numpy(k), F["corrector_" + k]), k
+    sim.close()
+    q.close()
