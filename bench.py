@@ -500,7 +500,7 @@ def run_ours(args, wl):
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": args.steps * launches_per_step(args.variant, wl["kind"]),
+            "gpu_launches": args.steps * launches_per_step(args.variant, wl["kind"], args.band_rounds),
             "clocks": clk,
         }
     if world > 1:
@@ -562,12 +562,12 @@ def hbm_peak_gbs():
         return {"value": 6650.0, "source": "fallback 6.65 TB/s"}
 
 
-def launches_per_step(variant, kind="gravity"):
+def launches_per_step(variant, kind="gravity", band_rounds=8):
     """This library's kernel launches in one timed step (counted from the
     launch sequence; the ncu launch lists in profiles/ show the same)."""
     # every RHS: bbox, bbox_finish, keys, hist, hist_scan, 8 onesweep (13), gather (1),
     # tree: lcp, count, 4 scan, copy_total, zero_cells, nodes, 3 level-list kernels (12),
-    # upward: leaves + 21 levels (22)
+    # upward pass: leaves + 21 levels (22)
     tree = 13 + 1 + 12 + 22
     mixed = variant == "mixed"
     if kind == "sph":
@@ -579,11 +579,14 @@ def launches_per_step(variant, kind="gravity"):
     if kind == "cloud":
         # variable h: snapshot copy, largest-h bounds (leaves + 21 levels), 7 sweeps x
         # (flags, 4 scan, compact, count walk, update), record, final flags + 4 scan +
-        # record, scatter of h; list walk with its own bounds (22 + 1); (mixed:
-        # position pack) density, forces, noi export, band statistics; learned h:
-        # apply, collect, features; explicit Euler update
+        # record, scatter of h; list walk with its own bounds (22 + 1); band repair: 2
+        # copies, rounds x
+        # (flags, 4 scan, compact, select, events, remove, compact, add, commit),
+        # scatter of h; (mixed: position pack) density, forces, noi export, band
+        # statistics; learned h: apply, collect, features; explicit Euler update
         vh = 1 + 22 + 7 * 8 + 1 + 6 + 1
-        sphk = 23 + (1 if mixed else 0) + 4
+        band = (2 + 12 * band_rounds + 1) if band_rounds > 0 else 0
+        sphk = 23 + band + (1 if mixed else 0) + 4
         learned = 3 if mixed else 0
         return grav + vh + sphk + learned + 1
     return grav + 2  # leapfrog updateX, updateV
