@@ -43,7 +43,7 @@ WORKLOADS = {
     # direct sum softened with the h the walk used: mixed relative rule alpha = 1.0e-3
     # -> 8.1e-4 at 1M, 1.5e-3 at 8.4M (1.2e-3 -> 8.2e-4, 1.8e-3 -> 9.7e-4); plain
     # FP64 v2 theta = 0.05 -> 9.7e-4 at 1M, theta = 0.07 -> 2.9e-3 at 8.4M)
-    "cloud1m": dict(kind="cloud", n=1 << 20, sfc=1, dt=0.004, theta=0.5, theta_mixed=0.25, mac_alpha=1.0e-3,
+    "cloud1m": dict(kind="cloud", n=1 << 20, sfc=1, dt=0.002, theta=0.5, theta_mixed=0.25, mac_alpha=1.0e-3,
                     theta_plain_matched=0.05, train_steps=20, train_iters=1500, seed=3),
     "cloud8m": dict(kind="cloud", n=1 << 23, sfc=1, dt=0.002, theta=0.6, theta_mixed=0.25, mac_alpha=1.5e-3,
                     theta_plain_matched=0.05, train_steps=20, train_iters=1500, seed=3),
@@ -256,11 +256,13 @@ def timed_steps(sim, step, steps, torch, per_step_stats=False):
     return e0.elapsed_time(e1), step, stats
 
 
-def cloud_run(args, wl, variant, learned, torch):
+def cloud_run(args, wl, variant, learned, torch, steps=None):
     """One cloud variant: the same seeded cloud, train_steps warm-up steps (the
     learned variant trains its predictor on them), one more step, then
-    `cloud_steps` timed steps with per-step statistics; drift of E and L over
-    the timed steps; force error of an extra untimed right-hand side."""
+    `steps` (default --cloud-steps) timed steps with per-step statistics; drift
+    of E and L over the timed steps; force error of an extra untimed
+    right-hand side."""
+    steps = steps or args.cloud_steps
     import ctypes
     from miluphpc_b200 import _lib
     state = plummer_state(wl, 0)
@@ -282,7 +284,7 @@ def cloud_run(args, wl, variant, learned, torch):
     sim.integrate(step)
     step += 1
     c0 = cloud_energy(sim, torch)
-    ms, step, st = timed_steps(sim, step, args.cloud_steps, torch, per_step_stats=True)
+    ms, step, st = timed_steps(sim, step, steps, torch, per_step_stats=True)
     c1 = cloud_energy(sim, torch)
     n = sim.n
     h_walk = sim.t["sml"][:n].clone()
@@ -292,8 +294,8 @@ def cloud_run(args, wl, variant, learned, torch):
     ob = [s["sml_out_of_band"] for s in st]
     obb = [s["sml_band_before"] for s in st]
     l0n = float(np.linalg.norm(c0["L"]))
-    out = {"ms_per_step": ms / args.cloud_steps, "value": n * args.cloud_steps / (ms / 1e3),
-           "steps": args.cloud_steps, "force_error": ferr,
+    out = {"ms_per_step": ms / steps, "value": n * steps / (ms / 1e3),
+           "steps": steps, "force_error": ferr,
            "gravity_theta": wl["theta_mixed"] if variant == "mixed" else wl["theta_plain_matched"],
            "opening_rule": ("relative, alpha %g (geometric theta %.2f on the first RHS)" % (wl["mac_alpha"],
                                                                                         wl["theta_mixed"]))
@@ -418,20 +420,18 @@ def run_ours(args, wl):
     compare = rank == 0 and world == 1 and not args.no_compare
     vs_plain = None
     if compare and wl["kind"] == "gravity":
-        vs_plain = {wl_name(args): plain_compare(args, wl, state, value, ferr, torch)}
+        vs_plain = {wl_name(args): guarded(plain_compare, args, wl, state, value, ferr, torch)}
     del state
     if compare and args.workload == "plummer16m" and args.cloud_steps > 0:
         vs_plain = vs_plain or {}
-        cw = dict(WORKLOADS["cloud8m"])
-        runs = {"mixed_learned": cloud_run(args, cw, "mixed", 1, torch),
-                "mixed_no_learned": cloud_run(args, cw, "mixed", 0, torch),
-                "plain": cloud_run(args, cw, "plain_matched", 0, torch)}
-        runs["speedup_vs_plain"] = runs["mixed_learned"]["value"] / runs["plain"]["value"]
-        runs["learned_h_gain"] = runs["mixed_learned"]["value"] / runs["mixed_no_learned"]["value"]
-        runs["workload"] = "cloud8m: rotating isothermal cloud N = 2^23, gravity (eps_i = h_i / 2) + SPH, " \
-                           "variable h 60 +- 5, explicit Euler dt %g, %d warm-up steps" % (cw["dt"],
-                                                                                         cw["train_steps"] + 1)
-        vs_plain["cloud8m"] = runs
+        vs_plain["cloud8m"] = guarded(cloud_compare, args, "cloud8m", args.cloud_steps, torch)
+    if compare and args.workload == "plummer16m" and args.all_configs:
+        vs_plain = vs_plain or {}
+        # the learned-h configuration at 1M: 20 plain steps train the predictor,
+        # then cloud1m_steps steps with predictor + plain fallback
+        vs_plain["cloud1m"] = guarded(cloud_compare, args, "cloud1m", args.cloud1m_steps, torch)
+        vs_plain["sedov2m"] = guarded(sph_compare, args, torch)
+        vs_plain["plummer131k"] = guarded(small_plummer, args, torch)
     if rank == 0:
         traffic = load_traffic(args.workload, args.variant)
         if sph:
@@ -533,6 +533,89 @@ def workload_config(args, wl, world):
         base.update({"sfc": "hilbert" if wl["sfc"] else "lebesgue", "integrator": "leapfrog", "dt": wl["dt"],
                      "eps2": wl["eps2"], "l2": "inputs larger than L2 (positions alone %.0f MB)" % (n * 24 / 1e6)})
     return base
+
+
+def guarded(fn, *a, **k):
+    """A comparison block: its failure is reported in the JSON line (the
+    headline measurement stands on its own)."""
+    try:
+        return fn(*a, **k)
+    except Exception as e:  # noqa: BLE001 - reported, not hidden
+        return {"error": "%s: %s" % (type(e).__name__, e)}
+
+
+def cloud_compare(args, name, steps, torch):
+    """The cloud with the mixed walk and the learned predictor, the same
+    without the predictor, and the plain FP64 path, `steps` timed steps each."""
+    cw = dict(WORKLOADS[name])
+    runs = {"mixed_learned": cloud_run(args, cw, "mixed", 1, torch, steps=steps),
+            "mixed_no_learned": cloud_run(args, cw, "mixed", 0, torch, steps=steps),
+            "plain": cloud_run(args, cw, "plain_matched", 0, torch, steps=steps)}
+    runs["speedup_vs_plain"] = runs["mixed_learned"]["value"] / runs["plain"]["value"]
+    runs["learned_h_gain"] = runs["mixed_learned"]["value"] / runs["mixed_no_learned"]["value"]
+    runs["workload"] = "%s: rotating isothermal cloud N = %d, gravity (eps_i = h_i / 2) + SPH, variable h " \
+                       "60 +- 5, explicit Euler dt %g, %d warm-up steps" % (name, cw["n"], cw["dt"],
+                                                                          cw["train_steps"] + 1)
+    return runs
+
+
+def sph_compare(args, torch, steps=20):
+    """Sedov blast (2.1M particles, SPH only, predictor-corrector): the FP32
+    pair sums against the FP64 path on the same state (one right-hand side
+    each: density and acceleration differences), then `steps` timed steps of
+    each after one warm-up step."""
+    wl = dict(WORKLOADS["sedov2m"])
+    state = plummer_state(wl, 0)
+    n = wl["n"]
+    out = {"workload": "sedov2m: 128^3 jittered lattice, fixed h = 2.5 dx, ideal gas, predictor-corrector, "
+                       "dt_max %g" % wl["dt_max"]}
+    first = {}
+    for variant in ("mixed", "plain"):
+        sim = make_sim(wl, state, variant)
+        sim.rhs(0)
+        first[variant] = {k: sim.t[k][:n].clone() for k in ("rho", "ax", "ay", "az")}
+        sim.close()
+        sim = make_sim(wl, state, variant)
+        sim.integrate(0)
+        ms, _, _ = timed_steps(sim, 1, steps, torch)
+        out[variant] = {"ms_per_step": ms / steps, "value": n * steps / (ms / 1e3), "steps": steps,
+                        "sph_pair_sums": "FP32 on hi/lo splits, FP64 accumulation" if variant == "mixed"
+                        else "FP64"}
+        sim.close()
+    a, b = first["mixed"], first["plain"]
+    amax = float(torch.sqrt(b["ax"] ** 2 + b["ay"] ** 2 + b["az"] ** 2).max().item())
+    out["mixed_vs_plain_first_rhs"] = {
+        "density_max_rel_diff": float((a["rho"] / b["rho"] - 1).abs().max().item()),
+        "acceleration_max_diff_over_max": float(max((a[k] - b[k]).abs().max().item() for k in ("ax", "ay", "az"))
+                                                / amax)}
+    out["speedup_vs_plain"] = out["mixed"]["value"] / out["plain"]["value"]
+    return out
+
+
+def small_plummer(args, torch, steps=10):
+    """The reference's own single-rank case (131,072 Plummer particles,
+    Lebesgue keys, theta 0.5, eps 0.01, leapfrog dt 0.025) on the plain FP64
+    path with the reference's v2 semantics: time per step, force error against
+    FP64 direct summation and energy drift over the steps."""
+    wl = dict(WORKLOADS["plummer131k"])
+    state = plummer_state(wl, 0)
+    sim = make_sim(wl, state, "plain")
+    e0 = sim.diagnostics()["kinetic"] + sim.potential()
+    sim.integrate(0)
+    sim.integrate(1)
+    ms, step, _ = timed_steps(sim, 2, steps, torch)
+    e1 = sim.diagnostics()["kinetic"] + sim.potential()
+    ferr = force_error(sim, torch, wl["eps2"])
+    st = sim.stats()
+    sim.close()
+    n = wl["n"]
+    return {"workload": "plummer131k: N = 131072 Plummer, Lebesgue, theta 0.5 (v2 semantics), eps2 1e-4, "
+                        "leapfrog dt 0.025", "plain": {"ms_per_step": ms / steps, "value": n * steps / (ms / 1e3),
+                                                       "steps": steps, "force_error": ferr,
+                                                       "energy_rel_drift": (e1 - e0) / abs(e0),
+                                                       "energy_steps": step,
+                                                       "stages_ms_last_step": {k: round(v, 3) for k, v in
+                                                                               st["ms_stage"].items()}}}
 
 
 def plain_compare(args, wl, state, mixed_value, mixed_ferr, torch):
@@ -746,6 +829,9 @@ def main():
     ap.add_argument("--plain-warmup", type=int, default=1)
     ap.add_argument("--cloud-steps", type=int, default=100,
                     help="timed steps of each cloud8m comparison run (0: no cloud comparison)")
+    ap.add_argument("--cloud1m-steps", type=int, default=200, help="timed steps of each cloud1m comparison run")
+    ap.add_argument("--no-all-configs", dest="all_configs", action="store_false",
+                    help="skip the cloud1m, sedov2m and plummer131k comparison blocks")
     ap.add_argument("--theta-mixed", type=float, default=None, help="override the mixed walk's opening parameter")
     ap.add_argument("--theta-plain", type=float, default=None,
                     help="override the accuracy-matched opening parameter of the plain FP64 walk")

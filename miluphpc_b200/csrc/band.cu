@@ -99,7 +99,8 @@ __global__ void __launch_bounds__(kBandBlock) k_band_select(TreeDev T, const dou
                                                             const int* __restrict__ nbr, int maxnb,
                                                             const int* __restrict__ list,
                                                             const int* __restrict__ list_count, BandRule R,
-                                                            double* hnew, float* node_hmax, DevStatus* st) {
+                                                            const long long* __restrict__ ord, double* hnew,
+                                                            float* node_hmax, DevStatus* st) {
     __shared__ SelectSmem smem[kBandWarps];
     if (st->code) return;
     const long cnt = *list_count;
@@ -115,8 +116,10 @@ __global__ void __launch_bounds__(kBandBlock) k_band_select(TreeDev T, const dou
         const int want = R.want(ni);
         const bool above = ni >= R.target + R.tol;
         // from below at most twice the h before the first round (at a free
-        // surface the neighbours' h may not reach the particle at all)
-        double rad = above ? R.radius(ni, hi) : fmin(R.radius(ni, hi), 2.0 * h0[s]);
+        // surface the neighbours' h may not reach the particle at all), and
+        // never past the edge of the bounding box
+        const double hcap = ord_to_dbl(ord[1]) - ord_to_dbl(ord[0]);
+        double rad = above ? R.radius(ni, hi) : fmin(fmin(R.radius(ni, hi), 2.0 * h0[s]), hcap);
         // the list holds the candidates of a particle above the band
         const bool from_list = above && ni <= min(maxnb, kBandCap);
         bool done = !above && rad <= hi;  // capped: nothing to gain
@@ -364,7 +367,7 @@ int sph_band_fixup(const TreeDev& T, const SphParams& P, const double* x, const 
         if (rc) return rc;
         k_band_compact_list<<<g, 256, 0, s>>>(n, B.flags, B.off, B.list, B.ctr, st, r);
         k_band_select<<<148 * 8, kBandBlock, 0, s>>>(T, x, y, z, h, B.h0, noi, nbr, P.maxnb, B.list, list_count, R,
-                                                     B.hnew, T.hmax, st);
+                                                     P.ord, B.hnew, T.hmax, st);
         k_band_events<<<148 * 8, kBandBlock, 0, s>>>(T, x, y, z, h, B.hnew, noi, nbr, P.maxnb, B.list, list_count,
                                                      T.hmax, B.events, B.cap_events, B.ctr, st);
         k_band_remove<<<148 * 4, 256, 0, s>>>(B.events, B.ctr, B.cap_events, nbr, noi, P.maxnb, B.dirty, st);

@@ -146,6 +146,7 @@ SphParams sph_params(const mhpc_ctx* c, int n) {
     P.mixed = c->cfg.precision >= 1;
     P.balsara = c->cfg.balsara ? 1 : 0;
     P.variable_sml = c->cfg.variable_sml ? 1 : 0;
+    P.ord = c->ord;
     for (int i = 0; i < c->nmat && i < MHPC_MAX_MATERIALS; ++i) P.mat[i] = to_dev(c->mats[i], c->cfg.si_units);
     return P;
 }

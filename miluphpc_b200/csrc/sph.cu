@@ -127,7 +127,6 @@ __device__ __forceinline__ float3 rel_f(const float4& ah, const float4& al, cons
     return make_float3((ah.x - bh.x) + (al.x - bl.x), (ah.y - bh.y) + (al.y - bl.y), (ah.z - bh.z) + (al.z - bl.z));
 }
 
-
 // ------------------------------------------------------------ FRNN walk
 // One warp per 32 consecutive (sorted or listed) particles, lane = particle,
 // four sub-groups of 8 lanes.
@@ -476,8 +475,14 @@ __global__ void __launch_bounds__(kBlock) k_count_warp(TreeDev T, const double* 
 __global__ void k_vh_update(const int* __restrict__ list, const int* __restrict__ list_count,
                             const int* __restrict__ count, double* h, double* hold, int* done, int* nit, int target,
                             int tol, int max_iter, int maxnb, float* node_hmax, const int* __restrict__ leaf_node,
-                            const int* __restrict__ parent) {
+                            const int* __restrict__ parent, const long long* __restrict__ ord) {
     const int m = *list_count;
+    // h never grows past the edge of the (cubic) bounding box: a particle whose
+    // neighbours' h do not reach it (an isolated or ejected particle) would
+    // otherwise multiply its h by up to 2.46 per sweep, without bound across
+    // steps (the reference has no such bound); at the box edge its search
+    // already covers every particle.
+    const double hcap = ord_to_dbl(ord[1]) - ord_to_dbl(ord[0]);
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x) {
         const int i = list[q];
         const int it = ++nit[i];
@@ -487,7 +492,7 @@ __global__ void k_vh_update(const int* __restrict__ list, const int* __restrict_
         } else {
             const int cc = c < 1 ? 1 : c;
             const double h0 = h[i];
-            const double hn = h0 * (0.5 * (1.0 + pow((double)target / (double)cc, 1. / 3.)));
+            const double hn = fmin(h0 * (0.5 * (1.0 + pow((double)target / (double)cc, 1. / 3.))), fmax(hcap, h0));
             h[i] = hn;
             hold[i] = hn;
             if (hn > h0) {
@@ -872,7 +877,7 @@ int sph_variable_h(const TreeDev& T, const SphParams& P, const double* x, const 
             k_count_warp<<<148 * 8, kBlock, 0, s>>>(T, x, y, z, B.hold, B.list, list_count, T.hmax, B.count, st);
         }
         k_vh_update<<<g, 256, 0, s>>>(B.list, list_count, B.count, h, B.hold, B.done, B.nit, target, tol, max_iter,
-                                      P.maxnb, T.hmax, T.leaf_node, T.parent);
+                                      P.maxnb, T.hmax, T.leaf_node, T.parent, P.ord);
     }
     k_flags<<<g, 256, 0, s>>>(P.n, B.done, B.flags);
     int rc = scan_exclusive_i32(B.flags, B.off, P.n, B.scan_scratch, s);

@@ -23,6 +23,7 @@ struct SphParams {
     int mixed;             // FP32 pair sums on group-relative coordinates
     int balsara;           // Balsara switch on the viscosity (S.bal holds the factors)
     int variable_sml;      // the Balsara gradients use h_bar only under VARIABLE_SML
+    const long long* ord;  // device bounding box (ordered-integer min, max): its edge caps h
     MatDev mat[MHPC_MAX_MATERIALS];
 };
 

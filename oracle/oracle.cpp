@@ -917,7 +917,7 @@ void orc_forces(const double* x, const double* y, const double* z, const double*
 // htmp *= 0.5 (1 + (target/n)^{1/3}).  Returns the number of sweeps; h is
 // updated in place, counts[] receives the last count.
 int orc_variable_h(const double* x, const double* y, const double* z, double* h, int n, int target,
-                   int tol, int max_nb, int max_iter, int* counts) {
+                   int tol, int max_nb, int max_iter, int* counts, double hcap) {
     std::vector<double> hold(h, h + n), hnew(h, h + n);
     std::vector<int> done(n, 0), nit(n, -1);
     std::vector<long> off(n + 1);
@@ -959,7 +959,10 @@ int orc_variable_h(const double* x, const double* y, const double* z, double* h,
                 done[i] = 1;
             } else {
                 int kk = k < 1 ? 1 : k;
-                hnew[i] *= 0.5 * (1.0 + std::pow((double)target / (double)kk, 1. / 3.));
+                // never past hcap (the edge of the cubic bounding box) when growing
+                const double h0 = hnew[i];
+                hnew[i] = std::min(h0 * (0.5 * (1.0 + std::pow((double)target / (double)kk, 1. / 3.))),
+                                   std::max(hcap, h0));
             }
         }
         hold = hnew;
@@ -983,10 +986,11 @@ int orc_variable_h(const double* x, const double* y, const double* z, double* h,
 // rad.  From below, rad is capped at twice the h the particle had before the
 // first round: a particle whose neighbours' h do not reach it (d >= h_j, at a
 // free surface) cannot gain pairs by its own h alone, and its h must not
-// grow without bound.  All picks of a round apply at once.  h is updated in
-// place; returns the out-of-band count before the first round.
+// grow without bound; nor past hcap (the edge of the cubic bounding box).
+// All picks of a round apply at once.  h is updated in place; returns the
+// out-of-band count before the first round.
 int orc_band_fixup(const double* x, const double* y, const double* z, double* h, int n, int target, int tol,
-                   int rounds) {
+                   int rounds, double hcap) {
     const int kCap = 256;
     int before = -1;
     std::vector<long> off(n + 1);
@@ -1005,7 +1009,8 @@ int orc_band_fixup(const double* x, const double* y, const double* z, double* h,
             const int cnt = (int)(off[i + 1] - off[i]);
             const bool above = cnt >= target + tol;
             const int want = above ? target + tol - 2 : target - tol + 2;
-            double rad = above ? h[i] : std::min(2 * cnt >= want ? 1.5 * h[i] : 2.0 * h[i], 2.0 * h0[i]);
+            double rad = above ? h[i] : std::min(std::min(2 * cnt >= want ? 1.5 * h[i] : 2.0 * h[i], 2.0 * h0[i]),
+                                                 hcap);
             if (!above && rad <= h[i]) continue;  // at the cap: no pair to gain, h stays
             std::vector<double> c;
             for (int attempt = 0; attempt < 5; ++attempt) {

@@ -63,9 +63,10 @@ def lib():
                                              ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [_d] * 7
         L.orc_balsara.argtypes = [_d] * 10 + [ctypes.c_int, _l, _i, ctypes.c_int, ctypes.c_int, _d, _d, _d]
         L.orc_variable_h.argtypes = [_d, _d, _d, _d, ctypes.c_int, ctypes.c_int, ctypes.c_int,
-                                     ctypes.c_int, ctypes.c_int, _i]
+                                     ctypes.c_int, ctypes.c_int, _i, ctypes.c_double]
         L.orc_variable_h.restype = ctypes.c_int
-        L.orc_band_fixup.argtypes = [_d, _d, _d, _d, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.orc_band_fixup.argtypes = [_d, _d, _d, _d, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_double]
         L.orc_band_fixup.restype = ctypes.c_int
         L.orc_euler.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                 ctypes.c_int, ctypes.c_int] + [_d] * 18
@@ -277,7 +278,7 @@ def variable_h(x, y, z, h, target, tol=5, max_nb=180, max_iter=5):
     h = np.array(h, dtype=np.float64, copy=True)
     cnt = np.zeros(len(x), dtype=np.int32)
     sweeps = lib().orc_variable_h(_p(x), _p(y), _p(z), _p(h), len(x), int(target), int(tol),
-                                  int(max_nb), int(max_iter), _p(cnt, _i))
+                                  int(max_nb), int(max_iter), _p(cnt, _i), _box_edge(x, y, z))
     return h, cnt, sweeps
 
 
@@ -286,8 +287,14 @@ def band_fixup(x, y, z, h, target, tol=5, rounds=8):
     the first round))."""
     x, y, z = _f64(x), _f64(y), _f64(z)
     h = np.array(h, dtype=np.float64, copy=True)
-    before = lib().orc_band_fixup(_p(x), _p(y), _p(z), _p(h), len(x), int(target), int(tol), int(rounds))
+    before = lib().orc_band_fixup(_p(x), _p(y), _p(z), _p(h), len(x), int(target), int(tol), int(rounds),
+                                  _box_edge(x, y, z))
     return h, before
+
+
+def _box_edge(x, y, z):
+    bb = bbox(x, y, z)
+    return float(bb[1] - bb[0])
 
 
 def quad(tree, max_level=21):
