@@ -604,9 +604,9 @@ def small_plummer(args, torch, steps=10):
     sim.integrate(0)
     sim.integrate(1)
     ms, step, _ = timed_steps(sim, 2, steps, torch)
+    st = sim.stats()
     e1 = sim.diagnostics()["kinetic"] + sim.potential()
     ferr = force_error(sim, torch, wl["eps2"])
-    st = sim.stats()
     sim.close()
     n = wl["n"]
     return {"workload": "plummer131k: N = 131072 Plummer, Lebesgue, theta 0.5 (v2 semantics), eps2 1e-4, "

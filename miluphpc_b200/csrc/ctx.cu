@@ -152,6 +152,7 @@ SphParams sph_params(const mhpc_ctx* c, int n) {
 }
 
 void record(mhpc_ctx* c, int e) {
+    if (c->force_wrec) return;  // mhpc_potential's tree build: the last RHS keeps its stage times
     cudaEventRecord(c->ev[e], c->stream);
     c->ev_recorded[e] = true;
 }
