@@ -237,31 +237,28 @@ def cloud_energy(sim, torch):
     return {"E": d["kinetic"] + w + u, "L": d["angular_momentum"]}
 
 
-def timed_steps(sim, step, steps, torch, per_step_stats=False):
+def timed_steps(sim, step, steps, torch):
     """`steps` integration steps bracketed by CUDA events on the library's
-    stream (the current torch stream).  Returns (ms, next step, per-step
-    statistics or None); with per_step_stats every step's status counters are
-    read (one stream synchronisation per step)."""
+    stream (the current torch stream), with no host synchronisation between
+    them.  Returns (ms, next step)."""
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    stats = [] if per_step_stats else None
     torch.cuda.synchronize()
     e0.record()
     for _ in range(steps):
         sim.integrate(step)
         step += 1
-        if per_step_stats:
-            stats.append(sim.stats())
     e1.record()
     torch.cuda.synchronize()
-    return e0.elapsed_time(e1), step, stats
+    return e0.elapsed_time(e1), step
 
 
 def cloud_run(args, wl, variant, learned, torch, steps=None):
     """One cloud variant: the same seeded cloud, train_steps warm-up steps (the
     learned variant trains its predictor on them), one more step, then
-    `steps` (default --cloud-steps) timed steps with per-step statistics; drift
-    of E and L over the timed steps; force error of an extra untimed
-    right-hand side."""
+    `steps` (default --cloud-steps) timed steps; the band and predictor
+    statistics of the timed steps come from the library's device-side run
+    totals, read once after them; drift of E and L over the timed steps; force
+    error of an extra untimed right-hand side."""
     steps = steps or args.cloud_steps
     import ctypes
     from miluphpc_b200 import _lib
@@ -284,15 +281,15 @@ def cloud_run(args, wl, variant, learned, torch, steps=None):
     sim.integrate(step)
     step += 1
     c0 = cloud_energy(sim, torch)
-    ms, step, st = timed_steps(sim, step, steps, torch, per_step_stats=True)
+    sim.reset_run_stats()
+    ms, step = timed_steps(sim, step, steps, torch)
+    st = sim.stats()
+    assert st["run_rhs"] == steps, (st["run_rhs"], steps)
     c1 = cloud_energy(sim, torch)
     n = sim.n
     h_walk = sim.t["sml"][:n].clone()
     sim.rhs(step)
     ferr = force_error(sim, torch, 0.0, h_factor=0.5, h=h_walk)
-    fb = [s["predictor_fallback"] for s in st]
-    ob = [s["sml_out_of_band"] for s in st]
-    obb = [s["sml_band_before"] for s in st]
     l0n = float(np.linalg.norm(c0["L"]))
     out = {"ms_per_step": ms / steps, "value": n * steps / (ms / 1e3),
            "steps": steps, "force_error": ferr,
@@ -303,15 +300,17 @@ def cloud_run(args, wl, variant, learned, torch, steps=None):
            "sph_pair_sums": "FP32 on hi/lo splits, FP64 accumulation" if variant == "mixed" else "FP64",
            "learned_h": bool(variant == "mixed" and learned),
            "band_rule": "reference iteration (max 5 updates, |n - 60| < 5) + %d repair rounds" % w["band_rounds"],
-           "out_of_band_before_repair_rate": float(np.mean(obb)) / n if min(obb) >= 0 else None,
-           "final_out_of_band_rate": float(np.mean(ob)) / n, "final_out_of_band_max": int(max(ob)),
-           "final_out_of_band_last_step": int(ob[-1]),
+           "out_of_band_before_repair_rate": st["run_band_before_sum"] / st["run_band_rhs"] / n
+           if st["run_band_rhs"] > 0 else None,
+           "final_out_of_band_rate": st["run_out_of_band_sum"] / st["run_rhs"] / n,
+           "final_out_of_band_max": int(st["run_out_of_band_max"]),
+           "final_out_of_band_last_step": int(st["sml_out_of_band"]),
            "energy_rel_drift": (c1["E"] - c0["E"]) / abs(c0["E"]),
            "angular_momentum_rel_drift": float(np.linalg.norm(np.subtract(c1["L"], c0["L"]))) / l0n
            if l0n > 0 else None,
-           "stages_ms_last_step": {k: round(v, 3) for k, v in st[-1]["ms_stage"].items()}}
+           "stages_ms_last_step": {k: round(v, 3) for k, v in st["ms_stage"].items()}}
     if variant == "mixed" and learned:
-        out["first_sweep_fallback_rate"] = float(np.mean(fb)) / n
+        out["first_sweep_fallback_rate"] = st["run_predictor_fallback_sum"] / st["run_rhs"] / n
         out["training"] = train
     sim.close()
     return out
@@ -369,10 +368,12 @@ def run_ours(args, wl):
     sph = wl["kind"] == "sph"
     # NVTX range "timed": profilers can select the timed steps' launches
     # (ncu --nvtx --nvtx-include "timed/"); the timed loop reads no statistics
-    # (no host synchronisation between steps), the last timed step's counters
-    # and stage events are read after it
+    # (no host synchronisation between steps): the last timed step's counters
+    # and stage events, and the library's device-side totals over the timed
+    # steps, are read after it
+    sim.reset_run_stats()
     torch.cuda.nvtx.range_push("timed")
-    ms, step, per_step = timed_steps(sim, step, args.steps, torch, per_step_stats=wl["kind"] == "cloud")
+    ms, step = timed_steps(sim, step, args.steps, torch)
     torch.cuda.nvtx.range_pop()
     clk = clocks.stop()
     value, ms_max = job_rate(ms, n, args.steps, world, dev)
@@ -403,15 +404,14 @@ def run_ours(args, wl):
         ferr = force_error(sim, torch, 0.0, h_factor=0.5, h=h_walk)
     learned = None
     if wl["kind"] == "cloud":
-        fallback = [s["predictor_fallback"] for s in per_step]
-        out_band = [s["sml_out_of_band"] for s in per_step]
+        rr = max(last["run_rhs"], 1)
         learned = {"training": train_info, "target_band": "60 +- 5 (|n - 60| < 5)",
-                   "band_repair_rounds": wl.get("band_rounds", 8),
-                   "out_of_band_before_repair_per_step": [s["sml_band_before"] for s in per_step],
-                   "first_sweep_fallback_per_step": fallback,
-                   "fallback_rate": float(np.mean(fallback)) / n,
-                   "final_out_of_band_per_step": out_band,
-                   "out_of_band_rate": float(np.mean(out_band)) / n}
+                   "band_repair_rounds": wl.get("band_rounds", 8), "timed_rhs": last["run_rhs"],
+                   "out_of_band_before_repair_rate": last["run_band_before_sum"] / max(last["run_band_rhs"], 1) / n,
+                   "fallback_rate": last["run_predictor_fallback_sum"] / rr / n,
+                   "out_of_band_rate": last["run_out_of_band_sum"] / rr / n,
+                   "out_of_band_max": last["run_out_of_band_max"],
+                   "out_of_band_last_step": last["sml_out_of_band"]}
     # end to end through the public C ABI with host buffers (pinned)
     e2e = run_e2e(args, wl, sim, state, torch, step)
     sim.close()
@@ -577,7 +577,7 @@ def sph_compare(args, torch, steps=20):
         sim.close()
         sim = make_sim(wl, state, variant)
         sim.integrate(0)
-        ms, _, _ = timed_steps(sim, 1, steps, torch)
+        ms, _ = timed_steps(sim, 1, steps, torch)
         out[variant] = {"ms_per_step": ms / steps, "value": n * steps / (ms / 1e3), "steps": steps,
                         "sph_pair_sums": "FP32 on hi/lo splits, FP64 accumulation" if variant == "mixed"
                         else "FP64"}
@@ -603,7 +603,7 @@ def small_plummer(args, torch, steps=10):
     e0 = sim.diagnostics()["kinetic"] + sim.potential()
     sim.integrate(0)
     sim.integrate(1)
-    ms, step, _ = timed_steps(sim, 2, steps, torch)
+    ms, step = timed_steps(sim, 2, steps, torch)
     st = sim.stats()
     e1 = sim.diagnostics()["kinetic"] + sim.potential()
     ferr = force_error(sim, torch, wl["eps2"])
@@ -626,7 +626,7 @@ def plain_compare(args, wl, state, mixed_value, mixed_ferr, torch):
     for _ in range(max(1, args.plain_warmup)):
         sim.integrate(step)
         step += 1
-    ms, step, _ = timed_steps(sim, step, args.plain_steps, torch)
+    ms, step = timed_steps(sim, step, args.plain_steps, torch)
     ferr = force_error(sim, torch, wl["eps2"])
     sim.close()
     value = wl["n"] * args.plain_steps / (ms / 1e3)
@@ -656,7 +656,8 @@ def launches_per_step(variant, kind="gravity", band_rounds=8):
     if kind == "sph":
         # frnn, (mixed: position pack), density+EOS, forces; noi export on the
         # first RHS only; predictor-corrector: 3 step-size kernels, predictor, corrector
-        rhs = tree + 1 + (1 if mixed else 0) + 2
+        # (+1: the status fold at the start of every SPH right-hand side)
+        rhs = 1 + tree + 1 + (1 if mixed else 0) + 2
         return (rhs + 1) + rhs + 3 + 2
     grav = tree + 1  # + the walk
     if kind == "cloud":
@@ -671,7 +672,7 @@ def launches_per_step(variant, kind="gravity", band_rounds=8):
         band = (2 + 12 * band_rounds + 1) if band_rounds > 0 else 0
         sphk = 23 + band + (1 if mixed else 0) + 4
         learned = 3 if mixed else 0
-        return grav + vh + sphk + learned + 1
+        return 1 + grav + vh + sphk + learned + 1  # status fold, ..., explicit Euler
     return grav + 2  # leapfrog updateX, updateV
 
 

@@ -328,8 +328,23 @@ typedef struct mhpc_stats {
     int sml_band_before;       /* particles out of the band before the band repair (-1: no repair ran) */
     int sml_band_skipped;      /* band repair rounds skipped because their pair changes overflowed the
                                   event buffer (4 per particle) */
+    /* Totals over the right-hand sides of mhpc_rhs / mhpc_integrate since the
+     * context was created or mhpc_stats_reset_run was called (SPH
+     * configurations; the per-stage exports are not counted).  They are
+     * accumulated on the device, so a caller reads them once after a run
+     * instead of synchronising after every step. */
+    int run_rhs;                       /* right-hand sides counted */
+    int run_out_of_band_max;           /* largest sml_out_of_band of one RHS */
+    double run_out_of_band_sum;        /* sum of sml_out_of_band */
+    double run_band_before_sum;        /* sum of sml_band_before over the RHS that ran the repair */
+    int run_band_rhs;                  /* RHS that ran the band repair */
+    int run_pad;
+    double run_predictor_used_sum;     /* sum of predictor_used */
+    double run_predictor_fallback_sum; /* sum of predictor_fallback */
 } mhpc_stats;
 int mhpc_get_stats(mhpc_ctx* ctx, mhpc_stats* out);
+/* Restart the run totals (run_* fields of mhpc_stats); stream-ordered. */
+int mhpc_stats_reset_run(mhpc_ctx* ctx);
 
 /* FP64 diagnostics (src/miluphpc.cpp:577-677, Physics::Kernel
  * src/subdomain_key_tree/subdomain.cu:2423-2644): out[0] kinetic energy,

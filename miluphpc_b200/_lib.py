@@ -75,6 +75,9 @@ class Stats(ctypes.Structure):
         ("sml_sweeps", c_int), ("sml_out_of_band", c_int), ("predictor_used", c_int),
         ("predictor_fallback", c_int), ("ms_stage", c_float * 12), ("sml_band_before", c_int),
         ("sml_band_skipped", c_int),
+        ("run_rhs", c_int), ("run_out_of_band_max", c_int), ("run_out_of_band_sum", c_double),
+        ("run_band_before_sum", c_double), ("run_band_rhs", c_int), ("run_pad", c_int),
+        ("run_predictor_used_sum", c_double), ("run_predictor_fallback_sum", c_double),
     ]
 
 
@@ -133,6 +136,7 @@ def load():
     L.mhpc_export_sorted.argtypes = [c_void_p, c_void_p, c_void_p]
     L.mhpc_export_tree.argtypes = [c_void_p, c_int, P_i, P_i, P_d, P_d, P_d, P_d, P_i]
     L.mhpc_get_stats.argtypes = [c_void_p, ctypes.POINTER(Stats)]
+    L.mhpc_stats_reset_run.argtypes = [c_void_p]
     L.mhpc_diagnostics.argtypes = [c_void_p, ctypes.POINTER(Particles), P_d]
     L.mhpc_potential.argtypes = [c_void_p, ctypes.POINTER(Particles), c_void_p, P_d]
     L.mhpc_remove_particles.argtypes = [c_void_p, ctypes.POINTER(Particles), P_i]
@@ -179,5 +183,5 @@ EXPORTS = [
     "mhpc_remove_particles", "mhpc_direct_gravity_soft",
     "mhpc_tree_build", "mhpc_com", "mhpc_gravity", "mhpc_frnn", "mhpc_density_eos", "mhpc_forces",
     "mhpc_integrate_leapfrog", "mhpc_integrate_euler", "mhpc_integrate_pc_step_size",
-    "mhpc_integrate_pc_predictor", "mhpc_integrate_pc_corrector",
+    "mhpc_integrate_pc_predictor", "mhpc_integrate_pc_corrector", "mhpc_stats_reset_run",
 ]

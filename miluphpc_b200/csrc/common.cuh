@@ -32,6 +32,11 @@ struct DevStatus {
     int pad[2];
 };
 
+// Device-side totals of the per-RHS counters over a run (mhpc_stats run_*).
+struct RunTotals {
+    unsigned long long rhs, oob_sum, oob_max, before_sum, band_rhs, used_sum, fallback_sum, pad;
+};
+
 __device__ __forceinline__ void set_status(DevStatus* st, int code, int detail) {
     if (atomicCAS(&st->code, 0, code) == 0) st->detail = detail;
 }

@@ -70,6 +70,10 @@ struct mhpc_ctx {
     int* band_ctr = nullptr;
     double* band_h0 = nullptr;
     bool band_ran = false;
+    // run totals of the per-RHS counters (SPH configurations); st_pending: *st
+    // holds a finished RHS whose counters are not yet in *run
+    RunTotals* run = nullptr;
+    bool st_pending = false;
     // particle count of the last gravity walk, -1 before the first: the
     // relative opening rule reads that walk's accelerations from g_ax/g_ay/g_az
     int grav_prev_n = -1;
@@ -383,18 +387,31 @@ int stage_sph(mhpc_ctx* c, const mhpc_particles* p) {
     return stage_forces(c, p);
 }
 
+// Zero the status word on the stream; with SPH the counters of a finished
+// right-hand side are first added to the run totals (one small kernel).
+int reset_status(mhpc_ctx* c, cudaStream_t s) {
+    if (c->cfg.sph) {
+        TRY(launch_status_fold(c->st, c->run, c->st_pending ? 1 : 0, c->band_ran ? 1 : 0, s));
+    } else {
+        CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevStatus), s));
+    }
+    c->st_pending = false;
+    return MHPC_OK;
+}
+
 int rhs_async(mhpc_ctx* c, const mhpc_particles* p, int self_gravity) {
     TRY(check_particles(c, p));
     for (int e = 0; e < EV_COUNT; ++e) c->ev_recorded[e] = false;
     c->last_n = p->n;
     if (p->n == 0) return MHPC_OK;
-    CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevStatus), c->stream));
+    TRY(reset_status(c, c->stream));
     record(c, EV_START);
     TRY(stage_tree(c, p));
     if (c->cfg.gravity && self_gravity) TRY(stage_gravity(c, p));
     if (c->cfg.sph) TRY(stage_sph(c, p));
     record(c, EV_END);
     c->first_rhs_done = true;
+    c->st_pending = c->cfg.sph != 0;
     return MHPC_OK;
 }
 
@@ -489,6 +506,7 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
 #define A(p, cnt) \
     if (!rc) rc = dalloc(c, &(p), (cnt))
     A(c->st, 1);
+    A(c->run, 1);
     A(c->ord, 2);
     A(c->bbox, 6);
     A(c->keys, n);
@@ -562,6 +580,7 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
         return rc;
     }
     CUDA_TRY(cudaMemset(c->st, 0, sizeof(DevStatus)));
+    CUDA_TRY(cudaMemset(c->run, 0, sizeof(RunTotals)));
     *out = c;
     return MHPC_OK;
 }
@@ -638,7 +657,7 @@ int mhpc_stage_tree(mhpc_ctx* c, const mhpc_particles* p) {
     if (!c) return MHPC_ERR_ARG;
     TRY(check_particles(c, p));
     if (p->n == 0) return MHPC_OK;
-    CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevStatus), c->stream));
+    TRY(reset_status(c, c->stream));
     c->last_n = p->n;
     return stage_tree(c, p);
 }
@@ -654,7 +673,7 @@ int mhpc_tree_build(mhpc_ctx* c, const mhpc_particles* p) {
     if (!c) return MHPC_ERR_ARG;
     TRY(check_particles(c, p));
     if (p->n == 0) return MHPC_OK;
-    CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevStatus), c->stream));
+    TRY(reset_status(c, c->stream));
     for (int e = 0; e < EV_COUNT; ++e) c->ev_recorded[e] = false;
     c->last_n = p->n;
     record(c, EV_START);
@@ -1002,6 +1021,27 @@ int mhpc_get_stats(mhpc_ctx* c, mhpc_stats* o) {
     o->predictor_fallback = h.predictor_fallback;
     o->sml_band_before = c->band_ran ? h.sml_band_before : -1;
     o->sml_band_skipped = h.sml_band_skipped;
+    RunTotals R;
+    CUDA_TRY(cudaMemcpy(&R, c->run, sizeof(R), cudaMemcpyDeviceToHost));
+    if (c->st_pending) {  // the last RHS, not yet folded on the device
+        const unsigned long long oob = (unsigned long long)(h.sml_out_of_band > 0 ? h.sml_out_of_band : 0);
+        R.rhs += 1;
+        R.oob_sum += oob;
+        R.oob_max = oob > R.oob_max ? oob : R.oob_max;
+        if (c->band_ran && h.sml_band_before >= 0) {
+            R.before_sum += (unsigned long long)h.sml_band_before;
+            R.band_rhs += 1;
+        }
+        R.used_sum += (unsigned long long)(h.predictor_used > 0 ? h.predictor_used : 0);
+        R.fallback_sum += (unsigned long long)(h.predictor_fallback > 0 ? h.predictor_fallback : 0);
+    }
+    o->run_rhs = (int)R.rhs;
+    o->run_out_of_band_max = (int)R.oob_max;
+    o->run_out_of_band_sum = (double)R.oob_sum;
+    o->run_band_before_sum = (double)R.before_sum;
+    o->run_band_rhs = (int)R.band_rhs;
+    o->run_predictor_used_sum = (double)R.used_sum;
+    o->run_predictor_fallback_sum = (double)R.fallback_sum;
     const int pairs[12][2] = {{EV_START, EV_KEYS}, {EV_KEYS, EV_SORT}, {EV_SORT, EV_TREE},  {EV_TREE, EV_COM},
                               {EV_COM, EV_GRAV},   {EV_SML, EV_LISTS}, {EV_COM, EV_SML},    {EV_FRNN, EV_DENS},
                               {EV_DENS, EV_FORCES}, {EV_LISTS, EV_FRNN}, {-1, -1},          {EV_START, EV_END}};
@@ -1014,6 +1054,13 @@ int mhpc_get_stats(mhpc_ctx* c, mhpc_stats* o) {
         cudaEventElapsedTime(&o->ms_stage[6], c->ev[EV_GRAV], c->ev[EV_SML]);
     }
     return code;
+}
+
+int mhpc_stats_reset_run(mhpc_ctx* c) {
+    if (!c) return MHPC_ERR_ARG;
+    CUDA_TRY(cudaMemsetAsync(c->run, 0, sizeof(RunTotals), c->stream));
+    c->st_pending = false;
+    return MHPC_OK;
 }
 
 int mhpc_remove_particles(mhpc_ctx* c, mhpc_particles* p, int* n_removed) {
@@ -1081,7 +1128,7 @@ int mhpc_potential(mhpc_ctx* c, const mhpc_particles* p, double* pot_dev, double
     if (!c->pot_scratch) return MHPC_ERR_ARG;
     double* pot = pot_dev ? pot_dev : c->pot_scratch;
     double* acc = c->pot_scratch + c->cap;  // accelerations of this walk (not the caller's g_a)
-    CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevStatus), s));
+    TRY(reset_status(c, s));
     c->force_wrec = true;
     const int rc = stage_tree(c, p);
     c->force_wrec = false;

@@ -405,6 +405,30 @@ extern "C" int mhpc_fp32_peak(double* tflops) {
     return cudaGetLastError() == cudaSuccess ? MHPC_OK : MHPC_ERR_CUDA;
 }
 
+__global__ void k_status_fold(DevStatus* st, RunTotals* run, int fold, int band) {
+    if (fold && threadIdx.x == 0) {
+        const unsigned long long oob = (unsigned long long)max(st->sml_out_of_band, 0);
+        run->rhs += 1;
+        run->oob_sum += oob;
+        run->oob_max = oob > run->oob_max ? oob : run->oob_max;
+        if (band && st->sml_band_before >= 0) {
+            run->before_sum += (unsigned long long)st->sml_band_before;
+            run->band_rhs += 1;
+        }
+        run->used_sum += (unsigned long long)max(st->predictor_used, 0);
+        run->fallback_sum += (unsigned long long)max(st->predictor_fallback, 0);
+    }
+    __syncthreads();
+    int* w = reinterpret_cast<int*>(st);
+    for (int i = threadIdx.x; i < (int)(sizeof(DevStatus) / sizeof(int)); i += blockDim.x) w[i] = 0;
+}
+
+int launch_status_fold(DevStatus* st, RunTotals* run, int fold, int band, cudaStream_t s) {
+    k_status_fold<<<1, 32, 0, s>>>(st, run, fold, band);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
 int launch_gather(int n, const int* perm, const GatherList& L, cudaStream_t s) {
     if (n <= 0 || (L.count == 0 && !L.isrc)) return MHPC_OK;
     k_gather<<<grid_for(n, 256, 148 * 16), 256, 0, s>>>(n, perm, L);

@@ -139,6 +139,10 @@ class Miluphpc:
         d["ms_stage"] = dict(zip(_lib.STAGES, list(s.ms_stage)))
         return d
 
+    def reset_run_stats(self):
+        """Restart the run totals (run_* fields of stats())."""
+        check(self.L.mhpc_stats_reset_run(self.ctx), "stats_reset_run")
+
     def diagnostics(self):
         out = (ctypes.c_double * 11)()
         check(self.L.mhpc_diagnostics(self.ctx, ctypes.byref(self._soa), out), "diagnostics")

@@ -402,6 +402,35 @@ def test_band_repair_matches_oracle(cuda):
     sim.close()
 
 
+def test_run_totals_equal_per_step_counters(cuda):
+    """The device-side run totals (run_* of mhpc_stats) equal the sums and the
+    maximum of the per-RHS counters read after every step, and restart at
+    mhpc_stats_reset_run."""
+    S, C = _cloud_state(20_000)
+    mat = material(interactions=60, eos_type=0, K=C["cs2"], gamma=1.0)
+    sim = Miluphpc(sph_cfg(variable_sml=1, integrate_energy=0, sml_band_rounds=2, time_step=1e-3), S,
+                   materials=[mat])
+    sim.integrate(0)
+    sim.reset_run_stats()
+    assert sim.stats()["run_rhs"] == 0
+    per = []
+    for k in range(1, 5):
+        sim.integrate(k)
+        per.append(sim.stats())
+    tot = sim.stats()
+    assert tot["run_rhs"] == 4 and tot["run_band_rhs"] == 4
+    assert tot["run_out_of_band_sum"] == sum(s["sml_out_of_band"] for s in per)
+    assert tot["run_out_of_band_max"] == max(s["sml_out_of_band"] for s in per)
+    assert tot["run_band_before_sum"] == sum(s["sml_band_before"] for s in per)
+    assert sum(s["sml_band_before"] for s in per) > 0
+    assert tot["run_predictor_fallback_sum"] == sum(s["predictor_fallback"] for s in per)
+    sim.reset_run_stats()
+    sim.integrate(5)
+    sim.integrate(6)
+    assert sim.stats()["run_rhs"] == 2
+    sim.close()
+
+
 # ------------------------------------------------------ boundary checks
 def test_boundary_argument_checks(cuda):
     P = ics.plummer(4096, seed=3)
