@@ -335,6 +335,7 @@ def run_ours(args, wl):
     e_start = None
     if wl["kind"] == "gravity":
         e_start = sim.diagnostics()["kinetic"] + sim.potential()
+    sim_cfg_refresh = (sim.cfg.learned_refresh_every, sim.cfg.learned_refresh_iters)
     learned_on = wl["kind"] == "cloud" and args.variant == "mixed" and wl.get("learned", 1)
     if wl["kind"] == "cloud":
         # the same start for every variant: train_steps plain steps (the
@@ -372,6 +373,7 @@ def run_ours(args, wl):
     # and stage events, and the library's device-side totals over the timed
     # steps, are read after it
     sim.reset_run_stats()
+    step_t0 = step
     torch.cuda.nvtx.range_push("timed")
     ms, step = timed_steps(sim, step, args.steps, torch)
     torch.cuda.nvtx.range_pop()
@@ -500,7 +502,8 @@ def run_ours(args, wl):
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
-            "gpu_launches": args.steps * launches_per_step(args.variant, wl["kind"], args.band_rounds),
+            "gpu_launches": args.steps * launches_per_step(args.variant, wl["kind"], args.band_rounds)
+            + (refresh_launches(sim_cfg_refresh, step_t0, args.steps) if learned_on else 0),
             "clocks": clk,
         }
     if world > 1:
@@ -674,6 +677,17 @@ def launches_per_step(variant, kind="gravity", band_rounds=8):
         learned = 3 if mixed else 0
         return 1 + grav + vh + sphk + learned + 1  # status fold, ..., explicit Euler
     return grav + 2  # leapfrog updateX, updateV
+
+
+def refresh_launches(every_iters, step0, steps):
+    """Launches of the learned predictor's refreshes inside the timed steps:
+    k_train, Adam and the BF16 mirror per Adam step, at every right-hand side
+    whose count since the context's creation is a multiple of `every` (one RHS
+    per explicit Euler step, counted from 1)."""
+    every, iters = every_iters
+    if every <= 0:
+        return 0
+    return 3 * iters * sum(1 for r in range(step0 + 1, step0 + steps + 1) if r % every == 0)
 
 
 def run_e2e(args, wl, sim, state, torch, step0):

@@ -101,6 +101,13 @@ typedef struct mhpc_config {
                                   other h frozen, the h giving it target + tol - 2 (from above) or
                                   target - tol + 2 (from below) neighbours; lists and counts are updated
                                   pair by pair.  Not in the reference. */
+    int learned_refresh_every; /* learned h, once trained: every this many right-hand sides the
+                                  predictor takes learned_refresh_iters Adam steps on the (features,
+                                  converged h) pairs collected so far, on the library's stream with
+                                  no host synchronisation, so that it follows the flow as it evolves
+                                  (0: never; default 10) */
+    int learned_refresh_iters; /* Adam steps (mini-batches of 8192 pairs, rate 1e-3) per refresh
+                                  (default 32) */
 } mhpc_config;
 
 /* Material (include/materials/material.cuh:123-150), one entry of the

@@ -42,7 +42,7 @@ class Config(ctypes.Structure):
         ("precision", c_int), ("theta_mixed", c_double), ("learned_h", c_int), ("softening_mode", c_int),
         ("softening_h_factor", c_double), ("node_pool_factor", c_double),
         ("gravity_mac", c_int), ("mac_alpha", c_double), ("balsara", c_int), ("mac_quad_alpha", c_double),
-        ("sml_band_rounds", c_int),
+        ("sml_band_rounds", c_int), ("learned_refresh_every", c_int), ("learned_refresh_iters", c_int),
     ]
 
 

@@ -214,6 +214,8 @@ void mhpc_config_default(mhpc_config* c) {
     c->balsara = 0;
     c->mac_quad_alpha = 0.0;
     c->sml_band_rounds = 0;
+    c->learned_refresh_every = 10;
+    c->learned_refresh_iters = 32;
 }
 
 int mhpc_config_from_info(const char* path, mhpc_config* c) {
@@ -261,7 +263,10 @@ int mhpc_config_from_info(const char* path, mhpc_config* c) {
     b("balsaraSwitch", &c->balsara);
     f("macQuadAlpha", &c->mac_quad_alpha);
     i("smlBandRounds", &c->sml_band_rounds);
-    if (c->sml_band_rounds < 0) return MHPC_ERR_CONFIG;
+    i("learnedRefreshEvery", &c->learned_refresh_every);
+    i("learnedRefreshIters", &c->learned_refresh_iters);
+    if (c->sml_band_rounds < 0 || c->learned_refresh_every < 0 || c->learned_refresh_iters < 0)
+        return MHPC_ERR_CONFIG;
     if (c->gravity_mac < 0 || c->gravity_mac > 1 || (c->gravity_mac == 1 && c->mac_alpha <= 0))
         return MHPC_ERR_CONFIG;
     if (c->integrator < 0 || c->integrator > 2 || c->sfc < 0 || c->sfc > 1 || c->theta <= 0 ||

@@ -74,6 +74,7 @@ struct mhpc_ctx {
     // holds a finished RHS whose counters are not yet in *run
     RunTotals* run = nullptr;
     bool st_pending = false;
+    long long learned_rhs = 0;  // right-hand sides that ran the learned feature pass
     // particle count of the last gravity walk, -1 before the first: the
     // relative opening rule reads that walk's accelerations from g_ax/g_ay/g_az
     int grav_prev_n = -1;
@@ -376,6 +377,11 @@ int stage_forces(mhpc_ctx* c, const mhpc_particles* p) {
         in.drhodt = p->drhodt; in.m = c->sm;
         in.dt = c->last_dt > 0 ? c->last_dt : (c->cfg.time_step > 0 ? c->cfg.time_step : 1.0);
         in.target = target;
+        // the predictor follows the flow: a few Adam steps on the recent pairs
+        // every learned_refresh_every right-hand sides (queued, no sync)
+        ++c->learned_rhs;
+        if (c->cfg.learned_refresh_every > 0 && c->learned_rhs % c->cfg.learned_refresh_every == 0)
+            TRY(mlp_refresh(c->mlp, c->cfg.learned_refresh_iters, 1e-3f, 8192, s));
         TRY(mlp_features_predict(c->mlp, in, s));
     }
     return MHPC_OK;

@@ -753,6 +753,24 @@ int mlp_train(MlpState* m, int iters, float lr, int batch, float* loss_out, cuda
     return MHPC_OK;
 }
 
+int mlp_refresh(MlpState* m, int iters, float lr, int batch, cudaStream_t s) {
+    if (!m->trained || iters <= 0) return MHPC_OK;
+    const int blocks = (batch + kTrainRows - 1) / kTrainRows;
+    for (int it = 0; it < iters; ++it) {
+        CUDA_TRY(cudaMemsetAsync(m->loss, 0, sizeof(float), s));
+        k_train<<<blocks, kTrainRows, train_smem(), s>>>(m->tx, m->ty, batch, m->tcount, m->tcap,
+                                                         0x5eed0000ULL + (unsigned long long)m->adam_t * 7919ULL,
+                                                         m->w, m->w1t, m->w2t, m->w2k, m->norm, 1, m->grad,
+                                                         m->loss, nullptr);
+        ++m->adam_t;
+        const float b1c = 1.f - powf(0.9f, (float)m->adam_t), b2c = 1.f - powf(0.999f, (float)m->adam_t);
+        k_adam<<<(MLP_NPARAM + 255) / 256, 256, 0, s>>>(m->w, m->adam_m, m->adam_v, m->grad, lr, b1c, b2c);
+        k_mirror<<<16, 256, 0, s>>>(m->w, m->w1t, m->w2t, m->w2k);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
 int mlp_forward_backward(MlpState* m, const float* feats, int rows, const float* target, float* out, float* grad,
                          float* loss_out, cudaStream_t s) {
     CUDA_TRY(cudaMemsetAsync(m->grad, 0, sizeof(float) * MLP_NPARAM, s));

@@ -49,6 +49,10 @@ int mlp_create(MlpState** out, int capacity);
 void mlp_destroy(MlpState* m);
 int mlp_reset(MlpState* m, unsigned long long seed, cudaStream_t s);
 int mlp_train(MlpState* m, int iters, float lr, int batch, float* loss_out, cudaStream_t s);
+// Once trained: `iters` more Adam steps on the pairs collected so far, queued
+// on `s` without a host synchronisation (the normalisation stays that of the
+// first training).  No-op before the first mlp_train.
+int mlp_refresh(MlpState* m, int iters, float lr, int batch, cudaStream_t s);
 int mlp_forward_backward(MlpState* m, const float* feats, int rows, const float* target, float* out, float* grad,
                          float* loss_out, cudaStream_t s);
 int mlp_get_params(MlpState* m, float* host, cudaStream_t s);

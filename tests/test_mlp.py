@@ -84,13 +84,13 @@ def test_mlp_forward_backward_matches_oracle(cuda):
     sim.close()
 
 
-def _cloud_sim(n, learned, seed=3):
+def _cloud_sim(n, learned, seed=3, **kw):
     from miluphpc_b200.miluphpc import Miluphpc, material
     C = ics.rotating_cloud(n, seed=seed)
     C["p"] = np.zeros(n); C["cs"] = np.zeros(n)
     cfg = _lib.default_config(gravity=1, sph=1, variable_sml=1, learned_h=int(learned), integrator=0,
                               time_step=0.004, smoothing=0.0, softening_mode=1, softening_h_factor=0.5,
-                              precision=1, theta_mixed=0.25, sfc=1)
+                              precision=1, theta_mixed=0.25, sfc=1, **kw)
     return Miluphpc(cfg, C, materials=[material(interactions=60, eos_type=0, K=C["cs2"], gamma=1.0)])
 
 
@@ -124,3 +124,38 @@ def test_training_lowers_loss_and_predictor_saves_sweeps(cuda):
     assert np.mean(band_l[1:]) <= 1.2 * np.mean(band_p[1:]) + 0.001 * n, (band_l, band_p)
     sim.close()
     plain.close()
+
+
+def _params(sim):
+    L = _lib.load()
+    k = L.mhpc_mlp_num_params()
+    buf = (ctypes.c_float * k)()
+    _lib.check(L.mhpc_mlp_get_params(sim.ctx, buf), "get_params")
+    return np.frombuffer(buf, dtype=np.float32).copy()
+
+
+@pytest.mark.gpu
+def test_predictor_refresh_between_steps(cuda):
+    """Once trained, the predictor takes learned_refresh_iters Adam steps every
+    learned_refresh_every right-hand sides (queued on the stream, no host
+    synchronisation): its weights change at exactly those right-hand sides,
+    and stay fixed when the refresh is off."""
+    n = 32768
+    L = _lib.load()
+    runs = {}
+    for every in (0, 3):
+        sim = _cloud_sim(n, learned=True, learned_refresh_every=every, learned_refresh_iters=4)
+        for step in range(12):
+            sim.integrate(step)
+        _lib.check(L.mhpc_mlp_train(sim.ctx, 50, 1e-3, None), "train")
+        w = [_params(sim)]
+        for step in range(12, 18):  # right-hand sides 13..18: refreshes at 15 and 18 when every = 3
+            sim.integrate(step)
+            w.append(_params(sim))
+        runs[every] = w
+        sim.close()
+    fixed = runs[0]
+    assert all(np.array_equal(fixed[0], x) for x in fixed[1:])
+    moved = runs[3]
+    changed = [not np.array_equal(moved[k], moved[k + 1]) for k in range(6)]
+    assert changed == [False, False, True, False, False, True], changed
