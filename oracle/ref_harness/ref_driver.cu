@@ -14,12 +14,14 @@
 // pinned through the tree instead (every particle's path through the
 // reference tree is its key prefix).
 //
-// Timing (gravity build): with a third argument K > 0 the driver runs the
-// whole sequence above once more untimed, then K more times between CUDA
-// events (resetArrays, computeBoundingBox, buildTree, calculateCentersOfMass
-// 21..1, prepareSorting + sortArray, computeForces_v2; each reference launch
-// wrapper synchronises the device, as in the reference) and prints one line
-// `time_ms <stage> <mean ms>` per stage and for the total.
+// Timing: with a third argument K > 0 the driver runs the whole sequence
+// above once more untimed, then K more times between CUDA events (gravity
+// build: resetArrays, computeBoundingBox, buildTree, calculateCentersOfMass
+// 21..1, prepareSorting + sortArray, computeForces_v2; SPH build: resetArrays
+// with the noi/nnl memsets, computeBoundingBox, buildTree, fixedRadiusNN,
+// calculateDensity, calculateSoundSpeed + calculatePressure, internalForces;
+// each reference launch wrapper synchronises the device, as in the reference)
+// and prints one line `time_ms <stage> <mean ms>` per stage and for the total.
 //
 // Input (little-endian binary): int32 n, int32 flags, double theta, double eps2,
 // double params[8], then x, y, z, m (n doubles each), then (gravity) keys
@@ -281,6 +283,52 @@ int main(int argc, char** argv) {
     wr(fo, dl(ph.d_divv, n).data(), n);
     wr(fo, dl(ph.d_curlv, (size_t)3 * n).data(), (size_t)3 * n);
 #endif
+    if (repeats > 0) {
+        // stages of one fixed-h SPH right-hand side (Miluphpc::rhs single rank:
+        // reset with the neighbour-list memsets, bounding box, tree,
+        // parallel_sph), the first pass untimed
+        const char* names[7] = {"reset_bbox", "build_tree", "fixed_radius_nn", "density",
+                                "sound_speed_pressure", "internal_forces", "total"};
+        double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+        cudaEvent_t ev[7];
+        for (int k = 0; k < 7; ++k) CK(cudaEventCreate(&ev[k]));
+        for (int rep = 0; rep <= repeats; ++rep) {
+            CK(cudaEventRecord(ev[0]));
+            Kernel::Launch::resetArrays(th.d_tree, ph.d_particles, th.d_mutex, n, numNodes, false);
+            CK(cudaMemset(ph.d_noi, 0, sizeof(integer) * n));
+            CK(cudaMemset(ph.d_nnl, 0xff, sizeof(integer) * (size_t)MAX_NUM_INTERACTIONS * n));
+            TreeNS::Kernel::Launch::computeBoundingBox(th.d_tree, ph.d_particles, th.d_mutex, n, 256, false);
+            CK(cudaEventRecord(ev[1]));
+            TreeNS::Kernel::Launch::buildTree(th.d_tree, ph.d_particles, n, n, false);
+            CK(cudaEventRecord(ev[2]));
+            SPH::Kernel::Launch::fixedRadiusNN(th.d_tree, ph.d_particles, ph.d_nnl, diam, n, n, numNodes);
+            CK(cudaEventRecord(ev[3]));
+            SPH::Kernel::Launch::calculateDensity(kh.kernel, th.d_tree, ph.d_particles, ph.d_nnl, n);
+            CK(cudaEventRecord(ev[4]));
+            SPH::Kernel::Launch::calculateSoundSpeed(ph.d_particles, mh.d_materials, n);
+#if BALSARA_SWITCH
+            SPH::Kernel::Launch::CalcDivvandCurlv(kh.kernel, ph.d_particles, ph.d_nnl, n);
+#endif
+            SPH::Kernel::Launch::calculatePressure(mh.d_materials, ph.d_particles, n);
+            CK(cudaEventRecord(ev[5]));
+            SPH::Kernel::Launch::internalForces(kh.kernel, mh.d_materials, th.d_tree, ph.d_particles, ph.d_nnl, n);
+            CK(cudaEventRecord(ev[6]));
+            CK(cudaEventSynchronize(ev[6]));
+            int idx2 = 0;
+            CK(cudaMemcpy(&idx2, th.d_index, sizeof(int), cudaMemcpyDeviceToHost));
+            if (idx2 != index) { std::fprintf(stderr, "tree changed between runs\n"); return 5; }
+            if (rep == 0) continue;
+            for (int k = 0; k < 6; ++k) {
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+                acc[k] += ms;
+            }
+            float tot = 0.f;
+            CK(cudaEventElapsedTime(&tot, ev[0], ev[6]));
+            acc[6] += tot;
+        }
+        for (int k = 0; k < 7; ++k) std::printf("time_ms %s %.6f\n", names[k], acc[k] / repeats);
+    }
 #endif
     std::fclose(fo);
     std::fclose(fi);
