@@ -664,16 +664,18 @@ def launches_per_step(variant, kind="gravity", band_rounds=8):
         return (rhs + 1) + rhs + 3 + 2
     grav = tree + 1  # + the walk
     if kind == "cloud":
-        # variable h: snapshot copy, largest-h bounds (leaves + 21 levels), 7 sweeps x
-        # (flags, 4 scan, compact, count walk, update), record, final flags + 4 scan +
-        # record, scatter of h; list walk with its own bounds (22 + 1); band repair: 2
-        # copies, rounds x
-        # (flags, 4 scan, compact, select, events, remove, compact, add, commit),
-        # scatter of h; (mixed: position pack) density, forces, noi export, band
-        # statistics; learned h: apply, collect, features; explicit Euler update
-        vh = 1 + 22 + 7 * 8 + 1 + 6 + 1
-        band = (2 + 12 * band_rounds + 1) if band_rounds > 0 else 0
-        sphk = 23 + band + (1 if mixed else 0) + 4
+        # variable h on lists: copy of h, largest-h bounds (leaves + 21 levels), the
+        # list walk of the starting h, 7 sweeps x (flags, 4 scan, compact, update,
+        # event reset, events, removals, compaction, appends, commit, gated re-walk),
+        # record after the first sweep, final flags + 4 scan + record, sort of the
+        # appended lists, list statistics, scatter of h; band repair: 2 copies,
+        # rounds x (flags, 4 scan, compact, select, events, remove, compact, add,
+        # commit), sort of the appended lists, scatter of h; (mixed: position pack)
+        # density, forces, noi export, band statistics; learned h: apply, collect,
+        # features; explicit Euler update
+        vh = 1 + 22 + 1 + 7 * 14 + 1 + 5 + 1 + 1 + 1 + 1
+        band = (2 + 12 * band_rounds + 1 + 1) if band_rounds > 0 else 0
+        sphk = band + (1 if mixed else 0) + 4
         learned = 3 if mixed else 0
         return 1 + grav + vh + sphk + learned + 1  # status fold, ..., explicit Euler
     return grav + 2  # leapfrog updateX, updateV

@@ -234,9 +234,10 @@ __global__ void __launch_bounds__(kBandBlock) k_band_events(TreeDev T, const dou
                                                             const int* __restrict__ list,
                                                             const int* __restrict__ list_count,
                                                             const float* __restrict__ node_hmax, int2* ev, int cap,
-                                                            int* ctr, DevStatus* st) {
+                                                            int* ctr, DevStatus* st, const int* skip = nullptr) {
     __shared__ EventSmem smem[kBandWarps];
     if (st->code) return;
+    if (skip && *skip) return;  // lists truncated: the caller re-walks them instead
     const long cnt = *list_count;
     if (cnt == 0) return;
     const int M = *T.nodes;
@@ -282,8 +283,9 @@ __device__ __forceinline__ bool tombstone(int* nbr, const int* noi, int maxnb, i
 }
 
 __global__ void k_band_remove(const int2* __restrict__ ev, const int* __restrict__ ctr, int cap, int* nbr,
-                              const int* __restrict__ noi, int maxnb, int* dirty, DevStatus* st) {
-    if (ctr[1]) return;
+                              const int* __restrict__ noi, int maxnb, int* dirty, DevStatus* st,
+                              const int* skip = nullptr) {
+    if (ctr[1] || (skip && *skip)) return;
     const int m = min(ctr[0], cap);
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
         const int2 v = ev[e];
@@ -297,8 +299,9 @@ __global__ void k_band_remove(const int2* __restrict__ ev, const int* __restrict
     }
 }
 
-__global__ void k_band_compact(int n, const int* __restrict__ ctr, int* nbr, int* noi, int maxnb, int* dirty) {
-    if (ctr[1]) return;
+__global__ void k_band_compact(int n, const int* __restrict__ ctr, int* nbr, int* noi, int maxnb, int* dirty,
+                               const int* skip = nullptr) {
+    if (ctr[1] || (skip && *skip)) return;
     for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
         if (!dirty[a]) continue;
         dirty[a] = 0;
@@ -312,21 +315,80 @@ __global__ void k_band_compact(int n, const int* __restrict__ ctr, int* nbr, int
     }
 }
 
-__device__ __forceinline__ void append(int* nbr, int* noi, int maxnb, int a, int b, DevStatus* st) {
+// A list already holding maxnb entries: an error for the band repair (its
+// targets stay far below maxnb); the variable-h iteration (trunc given) marks
+// the lists truncated and re-walks them instead.
+__device__ __forceinline__ void append(int* nbr, int* noi, int maxnb, int a, int b, DevStatus* st, int* trunc) {
     const int k = atomicAdd(noi + a, 1);
     if (k < maxnb) nbr[nb_index(a, k, maxnb)] = b;
+    else if (trunc) *trunc = 1;
     else set_status(st, MHPC_ERR_NEIGHBOURS, a);
 }
 
+// Appends land in atomic order: both ends are marked in `appended` and their
+// lists sorted afterwards (k_sort_appended), so that the lists, and the sums
+// over them, do not depend on the order in which the events ran.
 __global__ void k_band_add(const int2* __restrict__ ev, const int* __restrict__ ctr, int cap, int* nbr, int* noi,
-                           int maxnb, DevStatus* st) {
-    if (ctr[1]) return;
+                           int maxnb, DevStatus* st, int* appended, int* trunc = nullptr) {
+    if (ctr[1] || (trunc && *trunc)) return;
     const int m = min(ctr[0], cap);
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
         const int2 v = ev[e];
         if (v.x < 0) continue;
-        append(nbr, noi, maxnb, v.x, v.y, st);
-        append(nbr, noi, maxnb, v.y, v.x, st);
+        append(nbr, noi, maxnb, v.x, v.y, st, trunc);
+        append(nbr, noi, maxnb, v.y, v.x, st, trunc);
+        appended[v.x] = 1;
+        appended[v.y] = 1;
+    }
+}
+
+// Every list marked in `appended` sorted by neighbour index (one warp per
+// list: ranks by counting, the entries are distinct), and the mark cleared.
+constexpr int kSortPerLane = 8;  // lists up to 256 entries in registers; longer ones by lane 0
+__global__ void k_sort_appended(int n, int* appended, int* nbr, const int* __restrict__ noi, int maxnb) {
+    const int lane = threadIdx.x & 31;
+    const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long base = warp * 32; base < n; base += nwarps * 32) {
+        const long me = base + lane;
+        const bool mark = me < n && appended[me];
+        unsigned todo = __ballot_sync(MHPC_FULL, mark);
+        if (mark) appended[me] = 0;
+        while (todo) {
+            const int b = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const long a = base + b;
+            const int k = min(noi[a], maxnb);
+            if (k <= 32 * kSortPerLane) {
+                int val[kSortPerLane], rank[kSortPerLane];
+#pragma unroll
+                for (int r = 0; r < kSortPerLane; ++r) {
+                    const int q = lane + 32 * r;
+                    val[r] = q < k ? nbr[nb_index(a, q, maxnb)] : 0;
+                    rank[r] = 0;
+                }
+                for (int q = 0; q < k; ++q) {
+                    const int v = nbr[nb_index(a, q, maxnb)];
+#pragma unroll
+                    for (int r = 0; r < kSortPerLane; ++r) rank[r] += v < val[r];
+                }
+                __syncwarp();
+#pragma unroll
+                for (int r = 0; r < kSortPerLane; ++r)
+                    if (lane + 32 * r < k) nbr[nb_index(a, rank[r], maxnb)] = val[r];
+            } else if (lane == 0) {
+                for (int q = 1; q < k; ++q) {  // insertion sort in place
+                    const int v = nbr[nb_index(a, q, maxnb)];
+                    int w = q;
+                    while (w > 0 && nbr[nb_index(a, w - 1, maxnb)] > v) {
+                        nbr[nb_index(a, w, maxnb)] = nbr[nb_index(a, w - 1, maxnb)];
+                        --w;
+                    }
+                    nbr[nb_index(a, w, maxnb)] = v;
+                }
+            }
+            __syncwarp();
+        }
     }
 }
 
@@ -348,7 +410,34 @@ __global__ void k_copy_h(int n, const double* __restrict__ a, double* b) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
 }
 
+__global__ void k_reset_events(int* ctr) {
+    ctr[0] = 0;
+    ctr[1] = 0;
+}
+
 }  // namespace
+
+int sph_sort_appended(const SphParams& P, int* nbr, const int* noi, int* appended, cudaStream_t s) {
+    if (P.n <= 0) return MHPC_OK;
+    k_sort_appended<<<148 * 4, 256, 0, s>>>(P.n, appended, nbr, noi, P.maxnb);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int sph_apply_h_changes(const TreeDev& T, const SphParams& P, const double* x, const double* y, const double* z,
+                        const double* h, const double* hnew, int* nbr, int* noi, const int* list,
+                        const int* list_count, const BandBuffers& B, int* trunc, DevStatus* st, cudaStream_t s) {
+    if (P.n <= 0) return MHPC_OK;
+    const int g = grid_for(P.n, 256, 148 * 16);
+    k_reset_events<<<1, 1, 0, s>>>(B.ctr);
+    k_band_events<<<148 * 8, kBandBlock, 0, s>>>(T, x, y, z, h, hnew, noi, nbr, P.maxnb, list, list_count, T.hmax,
+                                                 B.events, B.cap_events, B.ctr, st, trunc);
+    k_band_remove<<<148 * 4, 256, 0, s>>>(B.events, B.ctr, B.cap_events, nbr, noi, P.maxnb, B.dirty, st, trunc);
+    k_band_compact<<<g, 256, 0, s>>>(P.n, B.ctr, nbr, noi, P.maxnb, B.dirty, trunc);
+    k_band_add<<<148 * 4, 256, 0, s>>>(B.events, B.ctr, B.cap_events, nbr, noi, P.maxnb, st, B.appended, trunc);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
 
 int sph_band_fixup(const TreeDev& T, const SphParams& P, const double* x, const double* y, const double* z,
                    double* h, int* nbr, int* noi, const BandBuffers& B, int target, int tol, int rounds,
@@ -372,9 +461,10 @@ int sph_band_fixup(const TreeDev& T, const SphParams& P, const double* x, const 
                                                      T.hmax, B.events, B.cap_events, B.ctr, st);
         k_band_remove<<<148 * 4, 256, 0, s>>>(B.events, B.ctr, B.cap_events, nbr, noi, P.maxnb, B.dirty, st);
         k_band_compact<<<g, 256, 0, s>>>(n, B.ctr, nbr, noi, P.maxnb, B.dirty);
-        k_band_add<<<148 * 4, 256, 0, s>>>(B.events, B.ctr, B.cap_events, nbr, noi, P.maxnb, st);
+        k_band_add<<<148 * 4, 256, 0, s>>>(B.events, B.ctr, B.cap_events, nbr, noi, P.maxnb, st, B.appended);
         k_band_commit<<<148 * 4, 256, 0, s>>>(B.list, list_count, B.ctr, h, B.hnew, st);
     }
+    k_sort_appended<<<148 * 4, 256, 0, s>>>(n, B.appended, nbr, noi, P.maxnb);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

@@ -69,6 +69,7 @@ struct mhpc_ctx {
     int band_cap = 0;
     int* band_ctr = nullptr;
     double* band_h0 = nullptr;
+    int* nb_appended = nullptr;  // [n] lists with appended entries (zero between calls)
     bool band_ran = false;
     // run totals of the per-RHS counters (SPH configurations); st_pending: *st
     // holds a finished RHS whose counters are not yet in *run
@@ -286,6 +287,11 @@ SphSorted sph_sorted(mhpc_ctx* c, const mhpc_particles* p) {
 // SPH::fixedRadiusNN_variableSML (src/sph/sph.cu:739-961, Jacobi form) when
 // variable_h, starting from the learned prediction when `predictor`, then
 // SPH::fixedRadiusNN (src/sph/sph.cu:93-281): the neighbour lists
+// The variable-h iteration runs on neighbour lists (sph_variable_h_lists; 0:
+// count walks, then one list walk with the final h).
+#ifndef MHPC_VH_LISTS
+#define MHPC_VH_LISTS 1
+#endif
 int stage_frnn(mhpc_ctx* c, const mhpc_particles* p, bool variable_h, bool learned) {
     const int n = p->n;
     cudaStream_t s = c->stream;
@@ -302,8 +308,19 @@ int stage_frnn(mhpc_ctx* c, const mhpc_particles* p, bool variable_h, bool learn
         VhBuffers B;
         B.hold = c->hold; B.done = c->vh_done; B.nit = c->vh_nit; B.count = c->vh_count;
         B.flags = c->vh_flags; B.off = c->vh_off; B.list = c->vh_list; B.scan_scratch = c->scan_scratch;
-        TRY(sph_variable_h(c->T, P, c->sx, c->sy, c->sz, c->sh, B, target, c->cfg.nb_tolerance,
-                           c->cfg.max_sml_iterations, c->cfg.max_sml_iterations + 2, c->st, s));
+        if (MHPC_VH_LISTS) {
+            // the iteration on lists: its lists are the right-hand side's
+            BandBuffers E;
+            std::memset(&E, 0, sizeof(E));
+            E.dirty = c->vh_count; E.hnew = c->hold; E.events = c->band_ev; E.cap_events = c->band_cap;
+            E.ctr = c->band_ctr; E.scan_scratch = c->scan_scratch; E.appended = c->nb_appended;
+            TRY(sph_variable_h_lists(c->T, P, c->sx, c->sy, c->sz, c->sh, c->nbr, c->noi, B, E, target,
+                                     c->cfg.nb_tolerance, c->cfg.max_sml_iterations,
+                                     c->cfg.max_sml_iterations + 2, c->st, s));
+        } else {
+            TRY(sph_variable_h(c->T, P, c->sx, c->sy, c->sz, c->sh, B, target, c->cfg.nb_tolerance,
+                               c->cfg.max_sml_iterations, c->cfg.max_sml_iterations + 2, c->st, s));
+        }
         GatherList L;
         std::memset(&L, 0, sizeof(L));
         L.count = 1;
@@ -311,12 +328,12 @@ int stage_frnn(mhpc_ctx* c, const mhpc_particles* p, bool variable_h, bool learn
         L.dst[0] = p->sml;
         TRY(launch_scatter(n, c->perm, L, s));
         if (learned)
-            TRY(mlp_collect(c->mlp, c->perm, c->h_start, c->sh, c->vh_count, c->vh_nit, target, c->cfg.nb_tolerance,
-                            c->cfg.max_sml_iterations, n, s));
+            TRY(mlp_collect(c->mlp, c->perm, c->h_start, c->sh, MHPC_VH_LISTS ? c->noi : c->vh_count, c->vh_nit,
+                            target, c->cfg.nb_tolerance, c->cfg.max_sml_iterations, n, s));
     }
     record(c, EV_SML);
     SphSorted S = sph_sorted(c, p);
-    TRY(sph_frnn(c->T, P, S, c->nbr, c->noi, c->st, s));
+    if (!(variable_h && MHPC_VH_LISTS)) TRY(sph_frnn(c->T, P, S, c->nbr, c->noi, c->st, s));
     record(c, EV_LISTS);
     c->band_ran = false;
     if (variable_h && c->cfg.sml_band_rounds > 0) {
@@ -326,6 +343,7 @@ int stage_frnn(mhpc_ctx* c, const mhpc_particles* p, bool variable_h, bool learn
         B.flags = c->vh_flags; B.off = c->vh_off; B.list = c->vh_list; B.dirty = c->vh_done; B.hnew = c->hold;
         B.events = c->band_ev; B.cap_events = c->band_cap; B.ctr = c->band_ctr; B.scan_scratch = c->scan_scratch;
         B.h0 = c->band_h0;
+        B.appended = c->nb_appended;
         TRY(sph_band_fixup(c->T, P, c->sx, c->sy, c->sz, c->sh, c->nbr, c->noi, B, target, c->cfg.nb_tolerance,
                            c->cfg.sml_band_rounds, c->st, s));
         GatherList L;
@@ -556,6 +574,7 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
         A(c->band_ev, c->band_cap);
         A(c->band_ctr, 4);
         A(c->band_h0, n);
+        A(c->nb_appended, n);
     }
     // mhpc_potential: the potential (when the caller passes no buffer) and the
     // walk's own accelerations, so that the caller's g_a stay untouched
@@ -587,6 +606,7 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
     }
     CUDA_TRY(cudaMemset(c->st, 0, sizeof(DevStatus)));
     CUDA_TRY(cudaMemset(c->run, 0, sizeof(RunTotals)));
+    if (c->nb_appended) CUDA_TRY(cudaMemset(c->nb_appended, 0, sizeof(int) * n));
     *out = c;
     return MHPC_OK;
 }

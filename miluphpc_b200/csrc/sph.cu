@@ -157,7 +157,10 @@ __device__ __forceinline__ float3 rel_f(const float4& ah, const float4& al, cons
 // mode 0: write lists (h_i = h[i], h_j = h[j]) for all particles; mode 1:
 // count only, with h_i = h[i], h_j = h[j] (the variable-h sweep passes the
 // sweep's snapshot as h), for the particles of `list` (list_count entries, in
-// sorted order, so 32 consecutive entries are still spatially close).
+// sorted order, so 32 consecutive entries are still spatially close); mode 2:
+// mode 0 for the variable-h iteration on lists: runs only when *gate is
+// nonzero, and a count above maxnb (the list keeps its first maxnb entries,
+// noi the full count) sets *trunc instead of an error; no statistics.
 constexpr int kStack = 512;
 constexpr int kReserve = 7 * 22 + 8;
 constexpr int kPool = 128;
@@ -180,9 +183,11 @@ __global__ void __launch_bounds__(kBlock, 6) k_frnn(TreeDev T, int n, int maxnb,
                                                  const double* __restrict__ sh, const int* __restrict__ list,
                                                  const int* __restrict__ list_count,
                                                  const float* __restrict__ node_hmax, int* __restrict__ nbr,
-                                                 int* __restrict__ noi, DevStatus* st) {
+                                                 int* __restrict__ noi, DevStatus* st,
+                                                 const int* __restrict__ gate = nullptr, int* trunc = nullptr) {
     __shared__ FrnnSmem smem[kWarps];
     if (st->code) return;
+    if (MODE == 2 && *gate == 0) return;
     const int M = *T.nodes;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
@@ -261,7 +266,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_frnn(TreeDev T, int n, int maxnb,
                     hit = j != is && d < ih2 && d < S.ch2[slot];
                 }
                 const unsigned b = __ballot_sync(MHPC_FULL, hit) & pmask;
-                if (MODE == 0 && hit) {
+                if (MODE != 1 && hit) {
                     const int pos = kb + __popc(b & lt);
                     if (pos < maxnb) nbr[nb_index(is, pos, maxnb)] = j;
                 }
@@ -409,6 +414,7 @@ __global__ void __launch_bounds__(kBlock, 6) k_frnn(TreeDev T, int n, int maxnb,
     if (active) {
         noi[s] = k;
         if (MODE == 0 && k > maxnb) set_status(st, MHPC_ERR_NEIGHBOURS, (int)s);
+        if (MODE == 2 && k > maxnb) *trunc = 1;
         if (MODE == 0) atomicMax(&st->max_noi, k);
     }
     if (MODE == 0) {
@@ -527,6 +533,41 @@ __global__ void k_record_unconverged(const int* __restrict__ list_count, DevStat
 
 __global__ void k_copy(int n, const double* __restrict__ a, double* b) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
+}
+
+// End of a sweep on lists: every iterating particle takes its new h; the
+// lists are re-walked when they are truncated (a count above maxnb) or when
+// the sweep's pair changes overflowed the event buffer (nothing was edited).
+__global__ void k_vh_commit(const int* __restrict__ list, const int* __restrict__ list_count,
+                            const double* __restrict__ hnew, double* h, const int* __restrict__ ctr, int* rewalk) {
+    const int m = *list_count;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *rewalk = (ctr[1] || ctr[2]) ? 1 : 0;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x) {
+        const int i = list[q];
+        h[i] = hnew[i];
+    }
+}
+
+// Statistics and the capacity check of the list walk, for lists that the
+// variable-h iteration kept current instead of a final walk.
+__global__ void k_noi_stats(int n, int maxnb, const int* __restrict__ noi, DevStatus* st) {
+    int mx = 0;
+    unsigned long long tot = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int k = noi[i];
+        if (k > maxnb) set_status(st, MHPC_ERR_NEIGHBOURS, i);
+        mx = max(mx, k);
+        tot += (unsigned long long)k;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = max(mx, __shfl_xor_sync(MHPC_FULL, mx, o));
+        tot += __shfl_xor_sync(MHPC_FULL, tot, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&st->max_noi, mx);
+        atomicAdd(&st->noi_sum, tot);
+    }
 }
 
 // --------------------------------------------------- density + EOS (fused)
@@ -883,6 +924,52 @@ int sph_variable_h(const TreeDev& T, const SphParams& P, const double* x, const 
     int rc = scan_exclusive_i32(B.flags, B.off, P.n, B.scan_scratch, s);
     if (rc) return rc;
     k_record_unconverged<<<1, 1, 0, s>>>(list_count, st);
+    CUDA_TRY(cudaGetLastError());
+    return MHPC_OK;
+}
+
+int sph_variable_h_lists(const TreeDev& T, const SphParams& P, const double* x, const double* y, const double* z,
+                         double* h, int* nbr, int* noi, const VhBuffers& V, const BandBuffers& B, int target,
+                         int tol, int max_iter, int sweeps, DevStatus* st, cudaStream_t s) {
+    if (P.n <= 0) return MHPC_OK;
+    const long blocks = (((long)P.n + 31) / 32 * 32 + kBlock - 1) / kBlock;
+    const int g = grid_for(P.n, 256, 148 * 16);
+    const int* list_count = V.off + P.n;
+    int* trunc = B.ctr + 2;   // some list holds fewer entries than its count
+    int* rewalk = B.ctr + 3;  // the lists are re-walked after this sweep
+    double* hnew = B.hnew;
+    CUDA_TRY(cudaMemsetAsync(B.ctr, 0, sizeof(int) * 4, s));
+    CUDA_TRY(cudaMemsetAsync(rewalk, 1, sizeof(int), s));  // nonzero: the first walk runs
+    CUDA_TRY(cudaMemsetAsync(B.dirty, 0, sizeof(int) * P.n, s));
+    k_copy<<<g, 256, 0, s>>>(P.n, h, hnew);
+    int rc = tree_node_hmax(T, h, st, s);
+    if (rc) return rc;
+    // the lists and counts of the starting h: the counts of the first sweep
+    k_frnn<2><<<(int)blocks, kBlock, 0, s>>>(T, P.n, P.maxnb, x, y, z, h, nullptr, nullptr, T.hmax, nbr, noi, st,
+                                              rewalk, trunc);
+    for (int it = 0; it < sweeps; ++it) {
+        k_flags<<<g, 256, 0, s>>>(P.n, V.done, V.flags);
+        rc = scan_exclusive_i32(V.flags, V.off, P.n, V.scan_scratch, s);
+        if (rc) return rc;
+        k_compact<<<g, 256, 0, s>>>(P.n, V.flags, V.off, V.list);
+        if (it == 1) k_record_active<<<1, 1, 0, s>>>(list_count, P.n, st);
+        // the reference's update from the exact counts of the current h (Jacobi:
+        // every new h goes to hnew first)
+        k_vh_update<<<g, 256, 0, s>>>(V.list, list_count, noi, hnew, hnew, V.done, V.nit, target, tol, max_iter,
+                                      P.maxnb, T.hmax, T.leaf_node, T.parent, P.ord);
+        rc = sph_apply_h_changes(T, P, x, y, z, h, hnew, nbr, noi, V.list, list_count, B, trunc, st, s);
+        if (rc) return rc;
+        k_vh_commit<<<g, 256, 0, s>>>(V.list, list_count, hnew, h, B.ctr, rewalk);
+        k_frnn<2><<<(int)blocks, kBlock, 0, s>>>(T, P.n, P.maxnb, x, y, z, h, nullptr, nullptr, T.hmax, nbr, noi,
+                                                  st, rewalk, trunc);
+    }
+    k_flags<<<g, 256, 0, s>>>(P.n, V.done, V.flags);
+    rc = scan_exclusive_i32(V.flags, V.off, P.n, V.scan_scratch, s);
+    if (rc) return rc;
+    k_record_unconverged<<<1, 1, 0, s>>>(list_count, st);
+    rc = sph_sort_appended(P, nbr, noi, B.appended, s);
+    if (rc) return rc;
+    k_noi_stats<<<g, 256, 0, s>>>(P.n, P.maxnb, noi, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

@@ -118,7 +118,33 @@ struct BandBuffers {
     int cap_events;
     int* ctr;            // [4] events, overflow flag
     void* scan_scratch;
+    int* appended;       // [n] lists that received appends (zero outside the calls; cleared by the sort)
 };
+// Sort the lists marked in `appended` by neighbour index and clear the marks.
+int sph_sort_appended(const SphParams& P, int* nbr, const int* noi, int* appended, cudaStream_t s);
 int sph_band_fixup(const TreeDev& T, const SphParams& P, const double* x, const double* y, const double* z,
                    double* h, int* nbr, int* noi, const BandBuffers& B, int target, int tol, int rounds,
                    DevStatus* st, cudaStream_t s);
+
+// The pair changes of moving every particle of `list` from h to hnew, applied
+// to the lists and counts in place (events, removals, compaction, appends);
+// with `trunc` (variable-h iteration) nothing runs while *trunc is set, and a
+// list that would pass maxnb sets it.  ctr[0..1] are reset here; ctr[1]
+// reports an event-buffer overflow (no list edited).
+int sph_apply_h_changes(const TreeDev& T, const SphParams& P, const double* x, const double* y, const double* z,
+                        const double* h, const double* hnew, int* nbr, int* noi, const int* list,
+                        const int* list_count, const BandBuffers& B, int* trunc, DevStatus* st, cudaStream_t s);
+
+// The variable-h iteration of sph_variable_h (the same Jacobi sweeps, the same
+// update rule and stopping test) on neighbour lists instead of count walks:
+// one list walk with the starting h gives every count of the first sweep;
+// after each sweep the pairs changed by the new h are edited into the lists
+// (sph_apply_h_changes), so the next sweep's counts are exact without a walk,
+// and the lists at the end are those of the final h (the list walk of the
+// right-hand side is not needed).  Lists that pass maxnb during the
+// iteration, or an event-buffer overflow, fall back to a full list walk after
+// that sweep.  Uses B.hnew and B.ctr[0..3]; T.hmax stays an upper bound
+// (grow-only) of the current h.
+int sph_variable_h_lists(const TreeDev& T, const SphParams& P, const double* x, const double* y, const double* z,
+                         double* h, int* nbr, int* noi, const VhBuffers& V, const BandBuffers& B, int target,
+                         int tol, int max_iter, int sweeps, DevStatus* st, cudaStream_t s);

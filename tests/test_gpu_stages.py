@@ -402,6 +402,62 @@ def test_band_repair_matches_oracle(cuda):
     sim.close()
 
 
+@pytest.mark.parametrize("spread", [(0.7, 1.4), (2.0, 2.4)])
+def test_variable_h_on_lists_matches_oracle(spread, cuda):
+    """The variable-h iteration on neighbour lists: the final h equal to the
+    oracle's Jacobi iteration from the same start, and every list and count
+    equal to the brute-force set of the final h.  With h started 2-2.4x too
+    large the first counts pass max_num_interactions (180): the lists are
+    truncated and re-walked after each sweep, with the same result."""
+    S, C = _cloud_state(20_000, spread=spread)
+    n = len(S["x"])
+    mat = material(interactions=60, eos_type=0, K=C["cs2"], gamma=1.0)
+    sim = Miluphpc(sph_cfg(variable_sml=1, integrate_energy=0), S, materials=[mat], want_nnl=True)
+    sim.rhs(0)
+    h_gpu = sim.numpy("sml")
+    h_orc, _, _ = O.variable_h(S["x"], S["y"], S["z"], S["sml"], 60, tol=5, max_nb=180, max_iter=5)
+    assert (np.abs(h_gpu - h_orc) <= 1e-12 * h_orc).mean() > 0.999
+    off, nbr = O.frnn(S["x"], S["y"], S["z"], h_gpu)
+    noi = sim.numpy("noi")
+    assert np.array_equal(noi, np.diff(off))
+    nnl = sim.t["nnl"].cpu().numpy().reshape(n, 180)
+    for i in range(n):
+        assert np.array_equal(np.sort(nnl[i, :noi[i]]), nbr[off[i]:off[i + 1]]), i
+    st = sim.stats()
+    assert st["max_noi"] == noi.max() and st["mean_noi"] == pytest.approx(noi.mean())
+    sim.close()
+
+
+def test_variable_h_on_lists_after_steps(cuda):
+    """The common case of the list-based iteration: a few steps into a run
+    (band repair on), where most particles start in the band and the few
+    that move edit the lists pair by pair.  One more right-hand side, band
+    repair off, from the current state: h equal to the oracle's iteration from
+    the same h, lists and counts equal to the brute-force sets."""
+    S, C = _cloud_state(20_000)
+    n = len(S["x"])
+    mat = material(interactions=60, eos_type=0, K=C["cs2"], gamma=1.0)
+    cfg = sph_cfg(variable_sml=1, integrate_energy=0, sml_band_rounds=8, time_step=1e-3)
+    sim = Miluphpc(cfg, S, materials=[mat], want_nnl=True)
+    for k in range(3):
+        sim.integrate(k)
+    x, y, z, h0 = (sim.numpy(f) for f in ("x", "y", "z", "sml"))
+    cfg.sml_band_rounds = 0
+    sim.set_config(cfg)
+    sim.rhs(3)
+    h_gpu = sim.numpy("sml")
+    h_orc, _, _ = O.variable_h(x, y, z, h0, 60, tol=5, max_nb=180, max_iter=5)
+    assert (h_gpu != h0).sum() > 20  # some particles moved their h
+    assert (np.abs(h_gpu - h_orc) <= 1e-12 * h_orc).mean() > 0.999
+    off, nbr = O.frnn(x, y, z, h_gpu)
+    noi = sim.numpy("noi")
+    assert np.array_equal(noi, np.diff(off))
+    nnl = sim.t["nnl"].cpu().numpy().reshape(n, 180)
+    for i in range(n):
+        assert np.array_equal(np.sort(nnl[i, :noi[i]]), nbr[off[i]:off[i + 1]]), i
+    sim.close()
+
+
 def test_run_totals_equal_per_step_counters(cuda):
     """The device-side run totals (run_* of mhpc_stats) equal the sums and the
     maximum of the per-RHS counters read after every step, and restart at
