@@ -13,8 +13,8 @@
 // Kernels of one round: flags + scan + compaction (out-of-band list),
 // k_band_select (selection, one warp per particle: a tree walk below the band,
 // the particle's own list above it), k_band_events (one event per changed
-// pair, likewise), k_band_remove (tombstones),
-// k_band_compact, k_band_add, k_band_commit.  Every kernel after the
+// pair, likewise), k_band_mark + k_band_filter (removals: the marked lists
+// re-tested with the new h), k_band_add, k_band_commit.  Every kernel after the
 // compaction reads the list length on the device and returns at once when it
 // is zero, so the host enqueues all rounds without synchronising.
 #include "sph.cuh"
@@ -270,48 +270,65 @@ __global__ void __launch_bounds__(kBandBlock) k_band_events(TreeDev T, const dou
     }
 }
 
-__device__ __forceinline__ bool tombstone(int* nbr, const int* noi, int maxnb, int a, int b) {
-    const int k = min(noi[a], maxnb);
-    for (int q = 0; q < k; ++q) {
-        const size_t ix = nb_index(a, q, maxnb);
-        if (nbr[ix] == b) {
-            nbr[ix] = -1;
-            return true;
-        }
-    }
-    return false;
-}
-
-__global__ void k_band_remove(const int2* __restrict__ ev, const int* __restrict__ ctr, int cap, int* nbr,
-                              const int* __restrict__ noi, int maxnb, int* dirty, DevStatus* st,
-                              const int* skip = nullptr) {
+// Removals: both ends of every removal event are marked; each marked list is
+// then filtered with the pair test of the new h (d < min(h_i', h_j'), the list
+// walk's test), which drops exactly the pairs the events removed (every pair
+// in a list was present with the old h, and a pair whose status did not change
+// passes).  One warp per marked list, order kept (ballot compaction).
+__global__ void k_band_mark(const int2* __restrict__ ev, const int* __restrict__ ctr, int cap, int* dirty,
+                            const int* skip = nullptr) {
     if (ctr[1] || (skip && *skip)) return;
     const int m = min(ctr[0], cap);
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < m; e += gridDim.x * blockDim.x) {
         const int2 v = ev[e];
         if (v.x >= 0) continue;
-        const int i = ~v.x, j = v.y;
-        const bool a = tombstone(nbr, noi, maxnb, i, j);
-        const bool b = tombstone(nbr, noi, maxnb, j, i);
-        if (!a || !b) set_status(st, MHPC_ERR_NEIGHBOURS, i);  // lists and h disagree: cannot happen
-        dirty[i] = 1;
-        dirty[j] = 1;
+        dirty[~v.x] = 1;
+        dirty[v.y] = 1;
     }
 }
 
-__global__ void k_band_compact(int n, const int* __restrict__ ctr, int* nbr, int* noi, int maxnb, int* dirty,
-                               const int* skip = nullptr) {
+__global__ void k_band_filter(int n, const int* __restrict__ ctr, const double* __restrict__ sx,
+                              const double* __restrict__ sy, const double* __restrict__ sz,
+                              const double* __restrict__ hn, int* nbr, int* noi, int maxnb, int* dirty,
+                              const int* skip = nullptr) {
     if (ctr[1] || (skip && *skip)) return;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < n; a += gridDim.x * blockDim.x) {
-        if (!dirty[a]) continue;
-        dirty[a] = 0;
-        const int k = min(noi[a], maxnb);
-        int w = 0;
-        for (int q = 0; q < k; ++q) {
-            const int v = nbr[nb_index(a, q, maxnb)];
-            if (v >= 0) nbr[nb_index(a, w++, maxnb)] = v;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+    for (long base = warp * 32; base < n; base += nwarps * 32) {
+        const long me = base + lane;
+        const bool mark = me < n && dirty[me];
+        unsigned todo = __ballot_sync(MHPC_FULL, mark);
+        if (mark) dirty[me] = 0;
+        while (todo) {
+            const int b = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const long a = base + b;
+            const int k = min(noi[a], maxnb);
+            const double px = sx[a], py = sy[a], pz = sz[a], ha = hn[a];
+            const double ha2 = ha * ha;
+            int w = 0;
+            for (int q0 = 0; q0 < k; q0 += 32) {
+                const int q = q0 + lane;
+                int j = -1;
+                bool keep = false;
+                if (q < k) {
+                    j = nbr[nb_index(a, q, maxnb)];
+                    const double d2 = d2_exact(px - __ldg(sx + j), py - __ldg(sy + j), pz - __ldg(sz + j));
+                    const double hj = hn[j];
+                    keep = d2 < ha2 && d2 < hj * hj;
+                }
+                const unsigned bk = __ballot_sync(MHPC_FULL, keep);
+                // entries are only moved towards the front: slot w + rank <= q
+                __syncwarp();
+                if (keep) nbr[nb_index(a, w + __popc(bk & lt), maxnb)] = j;
+                w += __popc(bk);
+                __syncwarp();
+            }
+            if (lane == 0) noi[a] = w;
+            __syncwarp();
         }
-        noi[a] = w;
     }
 }
 
@@ -432,8 +449,8 @@ int sph_apply_h_changes(const TreeDev& T, const SphParams& P, const double* x, c
     k_reset_events<<<1, 1, 0, s>>>(B.ctr);
     k_band_events<<<148 * 8, kBandBlock, 0, s>>>(T, x, y, z, h, hnew, noi, nbr, P.maxnb, list, list_count, T.hmax,
                                                  B.events, B.cap_events, B.ctr, st, trunc);
-    k_band_remove<<<148 * 4, 256, 0, s>>>(B.events, B.ctr, B.cap_events, nbr, noi, P.maxnb, B.dirty, st, trunc);
-    k_band_compact<<<g, 256, 0, s>>>(P.n, B.ctr, nbr, noi, P.maxnb, B.dirty, trunc);
+    k_band_mark<<<148 * 4, 256, 0, s>>>(B.events, B.ctr, B.cap_events, B.dirty, trunc);
+    k_band_filter<<<148 * 8, 128, 0, s>>>(P.n, B.ctr, x, y, z, hnew, nbr, noi, P.maxnb, B.dirty, trunc);
     k_band_add<<<148 * 4, 256, 0, s>>>(B.events, B.ctr, B.cap_events, nbr, noi, P.maxnb, st, B.appended, trunc);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
@@ -459,8 +476,8 @@ int sph_band_fixup(const TreeDev& T, const SphParams& P, const double* x, const 
                                                      P.ord, B.hnew, T.hmax, st);
         k_band_events<<<148 * 8, kBandBlock, 0, s>>>(T, x, y, z, h, B.hnew, noi, nbr, P.maxnb, B.list, list_count,
                                                      T.hmax, B.events, B.cap_events, B.ctr, st);
-        k_band_remove<<<148 * 4, 256, 0, s>>>(B.events, B.ctr, B.cap_events, nbr, noi, P.maxnb, B.dirty, st);
-        k_band_compact<<<g, 256, 0, s>>>(n, B.ctr, nbr, noi, P.maxnb, B.dirty);
+        k_band_mark<<<148 * 4, 256, 0, s>>>(B.events, B.ctr, B.cap_events, B.dirty);
+        k_band_filter<<<148 * 8, 128, 0, s>>>(n, B.ctr, x, y, z, B.hnew, nbr, noi, P.maxnb, B.dirty);
         k_band_add<<<148 * 4, 256, 0, s>>>(B.events, B.ctr, B.cap_events, nbr, noi, P.maxnb, st, B.appended);
         k_band_commit<<<148 * 4, 256, 0, s>>>(B.list, list_count, B.ctr, h, B.hnew, st);
     }
