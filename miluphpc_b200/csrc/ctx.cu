@@ -71,6 +71,7 @@ struct mhpc_ctx {
     double* band_h0 = nullptr;
     int* nb_appended = nullptr;  // [n] lists with appended entries (zero between calls)
     bool band_ran = false;
+    bool dens_ready = false;  // the sorted rho, p, c_s are the density pass's of this tree
     // run totals of the per-RHS counters (SPH configurations); st_pending: *st
     // holds a finished RHS whose counters are not yet in *run
     RunTotals* run = nullptr;
@@ -201,9 +202,21 @@ int stage_tree_build(mhpc_ctx* c, const mhpc_particles* p) {
         L.src[L.count] = p->sml; L.dst[L.count++] = c->sh;
     }
     if (c->cfg.sph) {
-        const double* s2[] = {p->vx, p->vy, p->vz, p->e, p->rho, p->p, p->cs};
-        double* d2[] = {c->svx, c->svy, c->svz, c->se, c->srho, c->sp, c->scs};
-        for (int a = 0; a < 7; ++a) { L.src[L.count] = s2[a]; L.dst[L.count++] = d2[a]; }
+        const double* s2[] = {p->vx, p->vy, p->vz, p->e};
+        double* d2[] = {c->svx, c->svy, c->svz, c->se};
+        for (int a = 0; a < 4; ++a) { L.src[L.count] = s2[a]; L.dst[L.count++] = d2[a]; }
+        // rho, p and c_s are inputs of the density/EOS pass only where it reads
+        // them: rho when integrated, p for the ideal gas (its c_s uses the
+        // previous p), c_s for an EOS that does not set it; else they are outputs
+        bool need_p = false, need_cs = false;
+        for (int m = 0; m < c->nmat; ++m) {
+            const int t = c->mats[m].eos_type;
+            need_p = need_p || t == 9 || !(t == 0 || t == 1 || t == 3 || t == 12);
+            need_cs = need_cs || !(t == 0 || t == 1 || t == 3 || t == 9 || t == 12);
+        }
+        if (c->cfg.integrate_density) { L.src[L.count] = p->rho; L.dst[L.count++] = c->srho; }
+        if (need_p) { L.src[L.count] = p->p; L.dst[L.count++] = c->sp; }
+        if (need_cs) { L.src[L.count] = p->cs; L.dst[L.count++] = c->scs; }
         if (p->material_id) {
             // ids index the material table: out-of-range ids are an argument error
             L.isrc = p->material_id; L.idst = c->smat; L.imax = c->nmat; L.st = c->st;
@@ -215,6 +228,7 @@ int stage_tree_build(mhpc_ctx* c, const mhpc_particles* p) {
     record(c, EV_TREE);
     c->tree_n = n;
     c->com_ready = c->quad_ready = false;
+    c->dens_ready = false;
     return MHPC_OK;
 }
 
@@ -368,6 +382,7 @@ int stage_density_eos(mhpc_ctx* c, const mhpc_particles* p) {
     TRY(sph_density_eos(P, S, c->nbr, c->noi, c->perm, p->rho, p->p, p->cs, c->st, c->stream));
     if (c->cfg.balsara) TRY(sph_balsara(P, S, c->nbr, c->noi, c->st, c->stream));
     record(c, EV_DENS);
+    c->dens_ready = true;
     return MHPC_OK;
 }
 
@@ -743,6 +758,18 @@ int mhpc_forces(mhpc_ctx* c, const mhpc_particles* p) {
     TRY(check_particles(c, p));
     if (p->n == 0) return MHPC_OK;
     if (c->lists_n != p->n) return MHPC_ERR_ARG;
+    if (!c->dens_ready) {
+        // forces on the caller's rho, p and c_s (mhpc_density_eos did not run
+        // after this tree): their sorted copies, which the tree's gather leaves
+        // out where the density pass would compute them
+        GatherList L;
+        std::memset(&L, 0, sizeof(L));
+        const double* src[] = {p->rho, p->p, p->cs};
+        double* dst[] = {c->srho, c->sp, c->scs};
+        for (int a = 0; a < 3; ++a) { L.src[a] = src[a]; L.dst[a] = dst[a]; }
+        L.count = 3;
+        TRY(launch_gather(p->n, c->perm, L, c->stream));
+    }
     TRY(stage_forces(c, p));
     record(c, EV_END);
     return MHPC_OK;
