@@ -202,18 +202,22 @@ int stage_tree_build(mhpc_ctx* c, const mhpc_particles* p) {
         L.src[L.count] = p->sml; L.dst[L.count++] = c->sh;
     }
     if (c->cfg.sph) {
-        const double* s2[] = {p->vx, p->vy, p->vz, p->e};
-        double* d2[] = {c->svx, c->svy, c->svz, c->se};
-        for (int a = 0; a < 4; ++a) { L.src[L.count] = s2[a]; L.dst[L.count++] = d2[a]; }
-        // rho, p and c_s are inputs of the density/EOS pass only where it reads
-        // them: rho when integrated, p for the ideal gas (its c_s uses the
-        // previous p), c_s for an EOS that does not set it; else they are outputs
-        bool need_p = false, need_cs = false;
+        const double* s2[] = {p->vx, p->vy, p->vz};
+        double* d2[] = {c->svx, c->svy, c->svz};
+        for (int a = 0; a < 3; ++a) { L.src[L.count] = s2[a]; L.dst[L.count++] = d2[a]; }
+        // e, rho, p and c_s are inputs of the density/EOS pass only where it
+        // reads them: e and p for the ideal gas (p = (gamma - 1) rho e, its c_s
+        // uses the previous p), rho when integrated, c_s for an EOS that does not
+        // set it; else they are outputs or unused
+        bool need_p = false, need_cs = false, need_e = false;
         for (int m = 0; m < c->nmat; ++m) {
             const int t = c->mats[m].eos_type;
-            need_p = need_p || t == 9 || !(t == 0 || t == 1 || t == 3 || t == 12);
-            need_cs = need_cs || !(t == 0 || t == 1 || t == 3 || t == 9 || t == 12);
+            const bool known = t == 0 || t == 1 || t == 3 || t == 9 || t == 12;
+            need_e = need_e || t == 9 || !known;
+            need_p = need_p || t == 9 || !known;
+            need_cs = need_cs || !known;
         }
+        if (need_e) { L.src[L.count] = p->e; L.dst[L.count++] = c->se; }
         if (c->cfg.integrate_density) { L.src[L.count] = p->rho; L.dst[L.count++] = c->srho; }
         if (need_p) { L.src[L.count] = p->p; L.dst[L.count++] = c->sp; }
         if (need_cs) { L.src[L.count] = p->cs; L.dst[L.count++] = c->scs; }

@@ -549,7 +549,13 @@ __global__ void __launch_bounds__(kListBlock, MHPC_LISTS_MIN_BLOCKS) k_grav_list
         sl[k] = (int)(valid[k] ? s[k] : (long)P.n - 1);
         const double px = __ldg(sx + sl[k]), py = __ldg(sy + sl[k]), pz = __ldg(sz + sl[k]);
         double e = P.eps2;
-        if (P.h_factor > 0.0) { const double hh = P.h_factor * __ldg(sh + sl[k]); e += hh * hh; }
+        if (P.h_factor > 0.0) {
+            // softening tied to h: at least 1e-20 (h >= 2e-10 h_factor^-1 in
+            // practice), so that every r^2 >= eps^2 keeps 1/r^3 finite and the
+            // walk runs without the r^2 = 0 guard
+            const double hh = P.h_factor * __ldg(sh + sl[k]);
+            e = fmax(e + hh * hh, 1e-20);
+        }
         e2[k] = (float)e;
         lox = fmin(lox, px); loy = fmin(loy, py); loz = fmin(loz, pz);
         hix = fmax(hix, px); hiy = fmax(hiy, py); hiz = fmax(hiz, pz);
@@ -828,7 +834,7 @@ int gravity_lists(const TreeDev& T, const GravParams& P, const double* sx, const
     const long blocks = (groups * 32 + kListBlock - 1) / kListBlock;
     // the self-interaction has R = 0 and r^2 = eps2: 1/r^3 stays finite in
     // FP32 for eps2 >= 1e-20
-    const bool guard = !(P.eps2 >= 1e-20), rel = P.rel_alpha > 0.0;
+    const bool guard = !(P.eps2 >= 1e-20) && !(P.h_factor > 0.0), rel = P.rel_alpha > 0.0;
 #define MHPC_LISTS(G_, R_, P_) \
     k_grav_lists<G_, R_, P_><<<(int)blocks, kListBlock, 0, s>>>(T, P, sx, sy, sz, sh, perm, gax, gay, gaz, st)
     if (P.pot) {
