@@ -175,10 +175,13 @@ struct FrnnSmem {
     float4 plo[4], phi[4];                                // sub-group points boxes
 };
 
+#ifndef MHPC_FRNN_MIN_BLOCKS
+#define MHPC_FRNN_MIN_BLOCKS 6
+#endif
 template <int MODE>
 // 6 blocks per SM (the register cap costs a few spilled values, the extra
 // warps hide more of the walk's latency)
-__global__ void __launch_bounds__(kBlock, 6) k_frnn(TreeDev T, int n, int maxnb, const double* __restrict__ sx,
+__global__ void __launch_bounds__(kBlock, MHPC_FRNN_MIN_BLOCKS) k_frnn(TreeDev T, int n, int maxnb, const double* __restrict__ sx,
                                                  const double* __restrict__ sy, const double* __restrict__ sz,
                                                  const double* __restrict__ sh, const int* __restrict__ list,
                                                  const int* __restrict__ list_count,
