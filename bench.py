@@ -693,7 +693,7 @@ def refresh_launches(every_iters, step0, steps):
 
 
 def run_e2e(args, wl, sim, state, torch, step0):
-    """Same steps through mhpc_integrate_host: host (pinned) state copied in
+    """Same steps through mhpc_integrate_host_async (+ mhpc_host_wait): host (pinned) state copied in
     and the new state + accelerations copied out every step."""
     import ctypes
     from miluphpc_b200 import _lib
@@ -717,12 +717,15 @@ def run_e2e(args, wl, sim, state, torch, step0):
     L = _lib.load()
     dt = ctypes.c_double()
     steps = max(2, min(args.steps, 5))
-    # one untimed call allocates the context's device mirror
+    # one untimed call allocates the context's device mirror; the timed steps
+    # overlap each step's copy-out with the next step's copy-in
+    # (mhpc_integrate_host_async), the last wait inside the timed region
     _lib.check(L.mhpc_integrate_host(sim.ctx, ctypes.byref(hp), step0, ctypes.byref(dt)), "integrate_host")
     t0 = time.perf_counter()
     for k in range(steps):
-        _lib.check(L.mhpc_integrate_host(sim.ctx, ctypes.byref(hp), step0 + 1 + k, ctypes.byref(dt)),
-                   "integrate_host")
+        _lib.check(L.mhpc_integrate_host_async(sim.ctx, ctypes.byref(hp), step0 + 1 + k, ctypes.byref(dt)),
+                   "integrate_host_async")
+    _lib.check(L.mhpc_host_wait(sim.ctx), "host_wait")
     el = time.perf_counter() - t0
     h2d = n_in * 8 * n
     d2h = n_out * 8 * n

@@ -235,8 +235,20 @@ int mhpc_ctx_status(mhpc_ctx* ctx);
 int mhpc_integrate(mhpc_ctx* ctx, const mhpc_particles* p, int step, double* dt_out);
 /* The same step with HOST (pinned or pageable) state arrays: copies the state
  * in, runs the step, copies the state and accelerations out.  Uses the
- * context's device mirror (allocated on first use). */
+ * context's device mirror (allocated on first use).  Returns when the results
+ * are in the host arrays (mhpc_integrate_host_async + mhpc_host_wait). */
 int mhpc_integrate_host(mhpc_ctx* ctx, mhpc_particles* host, int step, double* dt_out);
+/* The host-state step without waiting: every field is copied in as soon as the
+ * previous step's compute has released the device mirror and the previous
+ * step's copy-out of that field has landed (the host arrays are read and
+ * written in place), and copied out after the compute, velocities first, so
+ * that successive calls overlap one step's copy-out with the next step's
+ * copy-in.  The host arrays must not be read or written until mhpc_host_wait
+ * returns. */
+int mhpc_integrate_host_async(mhpc_ctx* ctx, mhpc_particles* host, int step, double* dt_out);
+/* Wait until every copy of the host-state steps issued so far has finished;
+ * returns the device status. */
+int mhpc_host_wait(mhpc_ctx* ctx);
 
 /* Sub-stages, one per group of the reference's Launch:: wrappers (which
  * take the device Tree / Particles and return kernel milliseconds after a

@@ -120,6 +120,8 @@ def load():
     L.mhpc_ctx_status.argtypes = [c_void_p]
     L.mhpc_integrate.argtypes = [c_void_p, ctypes.POINTER(Particles), c_int, P_d]
     L.mhpc_integrate_host.argtypes = [c_void_p, ctypes.POINTER(Particles), c_int, P_d]
+    L.mhpc_integrate_host_async.argtypes = [c_void_p, ctypes.POINTER(Particles), c_int, P_d]
+    L.mhpc_host_wait.argtypes = [c_void_p]
     L.mhpc_stage_tree.argtypes = [c_void_p, ctypes.POINTER(Particles)]
     L.mhpc_stage_gravity.argtypes = [c_void_p, ctypes.POINTER(Particles)]
     L.mhpc_stage_sph.argtypes = [c_void_p, ctypes.POINTER(Particles)]
@@ -184,4 +186,5 @@ EXPORTS = [
     "mhpc_tree_build", "mhpc_com", "mhpc_gravity", "mhpc_frnn", "mhpc_density_eos", "mhpc_forces",
     "mhpc_integrate_leapfrog", "mhpc_integrate_euler", "mhpc_integrate_pc_step_size",
     "mhpc_integrate_pc_predictor", "mhpc_integrate_pc_corrector", "mhpc_stats_reset_run",
+    "mhpc_integrate_host_async", "mhpc_host_wait",
 ]

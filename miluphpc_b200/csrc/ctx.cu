@@ -97,6 +97,12 @@ struct mhpc_ctx {
     // copy_stream while the right-hand side runs (pos_out = host x, y, z)
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_drift = nullptr;
+    // host-state steps: copy-in / copy-out streams and their events (one per field)
+    cudaStream_t in_stream = nullptr, out_stream = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_computed = nullptr;
+    cudaEvent_t ev_out[18] = {};
+    bool out_pending[18] = {};
+    long long host_steps = 0;
     double* pos_out[3] = {nullptr, nullptr, nullptr};
     std::vector<void*> allocs;
     MlpState* mlp = nullptr;
@@ -644,6 +650,15 @@ int mhpc_ctx_destroy(mhpc_ctx* c) {
         cudaStreamDestroy(c->copy_stream);
     }
     if (c->ev_drift) cudaEventDestroy(c->ev_drift);
+    for (cudaStream_t q : {c->in_stream, c->out_stream})
+        if (q) {
+            cudaStreamSynchronize(q);
+            cudaStreamDestroy(q);
+        }
+    for (cudaEvent_t e : {c->ev_in, c->ev_computed})
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : c->ev_out)
+        if (e) cudaEventDestroy(e);
     if (c->mirror_ready) {
         double** ptrs[] = {&c->mirror.x, &c->mirror.y, &c->mirror.z, &c->mirror.mass, &c->mirror.vx, &c->mirror.vy,
                            &c->mirror.vz, &c->mirror.ax, &c->mirror.ay, &c->mirror.az, &c->mirror.g_ax,
@@ -914,7 +929,28 @@ int mhpc_integrate(mhpc_ctx* c, const mhpc_particles* p, int step, double* dt_ou
     return read_status(c);
 }
 
-int mhpc_integrate_host(mhpc_ctx* c, mhpc_particles* h, int step, double* dt_out) {
+// Host-state steps.  Every field moves on its own schedule: the inputs go in
+// on `in_stream` once the previous step's compute has released the device
+// mirror and the previous step's copy-out of the same field has landed in
+// the host buffer (the host state is read and written in place); the outputs
+// go out on `out_stream` after the compute, velocities first.  So the next
+// step's copy-in of the fields that are ready (masses, positions) runs while
+// this step's velocities and accelerations are still coming out (the bus is
+// full duplex), and mhpc_integrate_host_async returns without waiting.
+enum HostField { HF_X, HF_Y, HF_Z, HF_M, HF_VX, HF_VY, HF_VZ, HF_GX, HF_GY, HF_GZ, HF_H, HF_E, HF_RHO, HF_P,
+                 HF_CS, HF_AX, HF_AY, HF_AZ, HF_COUNT };
+
+int host_streams(mhpc_ctx* c) {
+    if (c->in_stream) return MHPC_OK;
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->in_stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->out_stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&c->ev_computed, cudaEventDisableTiming));
+    for (int f = 0; f < HF_COUNT; ++f) CUDA_TRY(cudaEventCreateWithFlags(&c->ev_out[f], cudaEventDisableTiming));
+    return MHPC_OK;
+}
+
+int mhpc_integrate_host_async(mhpc_ctx* c, mhpc_particles* h, int step, double* dt_out) {
     if (!c || !h) return MHPC_ERR_ARG;
     if (h->n > c->cap || h->n < 0) return MHPC_ERR_CAPACITY;
     const size_t n = c->cap;
@@ -930,23 +966,37 @@ int mhpc_integrate_host(mhpc_ctx* c, mhpc_particles* h, int step, double* dt_out
         }
         c->mirror_ready = true;
     }
+    TRY(host_streams(c));
     m.n = h->n;
     m.num_nodes = h->n;
     cudaStream_t s = c->stream;
     const size_t b = sizeof(double) * h->n;
-    // state in (positions, velocities, masses; leapfrog carries g_a between steps)
-    struct Pair { double* d; double* hh; };
-    std::vector<Pair> in = {{m.x, h->x}, {m.y, h->y}, {m.z, h->z}, {m.mass, h->mass},
-                            {m.vx, h->vx}, {m.vy, h->vy}, {m.vz, h->vz}};
+    struct Field { int id; double* d; double* hh; };
+    // state in (positions, velocities, masses; leapfrog carries g_a between
+    // steps), the fields whose host copy is ready earliest first
+    std::vector<Field> in = {{HF_M, m.mass, h->mass}, {HF_X, m.x, h->x}, {HF_Y, m.y, h->y}, {HF_Z, m.z, h->z},
+                             {HF_VX, m.vx, h->vx}, {HF_VY, m.vy, h->vy}, {HF_VZ, m.vz, h->vz}};
     if (c->cfg.integrator == 2) {
-        in.push_back({m.g_ax, h->g_ax}); in.push_back({m.g_ay, h->g_ay}); in.push_back({m.g_az, h->g_az});
+        in.push_back({HF_GX, m.g_ax, h->g_ax}); in.push_back({HF_GY, m.g_ay, h->g_ay});
+        in.push_back({HF_GZ, m.g_az, h->g_az});
     }
     if (c->cfg.sph) {
-        in.push_back({m.sml, h->sml}); in.push_back({m.e, h->e}); in.push_back({m.rho, h->rho});
-        in.push_back({m.p, h->p}); in.push_back({m.cs, h->cs});
+        in.push_back({HF_H, m.sml, h->sml}); in.push_back({HF_E, m.e, h->e}); in.push_back({HF_RHO, m.rho, h->rho});
+        in.push_back({HF_P, m.p, h->p}); in.push_back({HF_CS, m.cs, h->cs});
     }
-    for (auto& q : in)
-        if (q.hh) CUDA_TRY(cudaMemcpyAsync(q.d, q.hh, b, cudaMemcpyHostToDevice, s));
+    if (c->host_steps > 0) CUDA_TRY(cudaStreamWaitEvent(c->in_stream, c->ev_computed, 0));
+    for (auto& q : in) {
+        if (!q.hh) continue;
+        if (c->out_pending[q.id]) CUDA_TRY(cudaStreamWaitEvent(c->in_stream, c->ev_out[q.id], 0));
+        CUDA_TRY(cudaMemcpyAsync(q.d, q.hh, b, cudaMemcpyHostToDevice, c->in_stream));
+    }
+    CUDA_TRY(cudaEventRecord(c->ev_in, c->in_stream));
+    CUDA_TRY(cudaStreamWaitEvent(s, c->ev_in, 0));
+    // the compute overwrites every output field of the mirror: the previous
+    // step's copy-out of each must have finished (for the fields that are
+    // also inputs this is already implied by their copy-in)
+    for (int f = 0; f < HF_COUNT; ++f)
+        if (c->out_pending[f]) CUDA_TRY(cudaStreamWaitEvent(s, c->ev_out[f], 0));
     // leapfrog: step 0 computes the initial accelerations; later steps carry
     // the caller's g_a of the previous step
     if (c->cfg.integrator == 2) c->first_rhs_done = step != 0;
@@ -960,24 +1010,50 @@ int mhpc_integrate_host(mhpc_ctx* c, mhpc_particles* h, int step, double* dt_out
     }
     int rc = mhpc_integrate(c, &m, step, dt_out);
     c->pos_out[0] = c->pos_out[1] = c->pos_out[2] = nullptr;
-    if (overlap) CUDA_TRY(cudaStreamSynchronize(c->copy_stream));
     if (rc) return rc;
-    std::vector<Pair> outp = {{m.vx, h->vx}, {m.vy, h->vy}, {m.vz, h->vz}};
+    if (overlap) {
+        // the drifted positions went out on copy_stream during the RHS
+        for (int f = HF_X; f <= HF_Z; ++f) {
+            CUDA_TRY(cudaEventRecord(c->ev_out[f], c->copy_stream));
+            c->out_pending[f] = true;
+        }
+    }
+    CUDA_TRY(cudaEventRecord(c->ev_computed, s));
+    ++c->host_steps;
+    CUDA_TRY(cudaStreamWaitEvent(c->out_stream, c->ev_computed, 0));
+    std::vector<Field> outp = {{HF_VX, m.vx, h->vx}, {HF_VY, m.vy, h->vy}, {HF_VZ, m.vz, h->vz}};
     if (!overlap) {
-        outp.push_back({m.x, h->x}); outp.push_back({m.y, h->y}); outp.push_back({m.z, h->z});
+        outp.push_back({HF_X, m.x, h->x}); outp.push_back({HF_Y, m.y, h->y}); outp.push_back({HF_Z, m.z, h->z});
     }
     if (c->cfg.gravity) {
-        outp.push_back({m.g_ax, h->g_ax}); outp.push_back({m.g_ay, h->g_ay}); outp.push_back({m.g_az, h->g_az});
+        outp.push_back({HF_GX, m.g_ax, h->g_ax}); outp.push_back({HF_GY, m.g_ay, h->g_ay});
+        outp.push_back({HF_GZ, m.g_az, h->g_az});
     }
     if (c->cfg.sph) {
-        outp.push_back({m.sml, h->sml}); outp.push_back({m.e, h->e}); outp.push_back({m.rho, h->rho});
-        outp.push_back({m.p, h->p}); outp.push_back({m.cs, h->cs});
-        outp.push_back({m.ax, h->ax}); outp.push_back({m.ay, h->ay}); outp.push_back({m.az, h->az});
+        outp.push_back({HF_H, m.sml, h->sml}); outp.push_back({HF_E, m.e, h->e});
+        outp.push_back({HF_RHO, m.rho, h->rho}); outp.push_back({HF_P, m.p, h->p}); outp.push_back({HF_CS, m.cs, h->cs});
+        outp.push_back({HF_AX, m.ax, h->ax}); outp.push_back({HF_AY, m.ay, h->ay}); outp.push_back({HF_AZ, m.az, h->az});
     }
-    for (auto& q : outp)
-        if (q.hh) CUDA_TRY(cudaMemcpyAsync(q.hh, q.d, b, cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
+    for (auto& q : outp) {
+        if (!q.hh) continue;
+        CUDA_TRY(cudaMemcpyAsync(q.hh, q.d, b, cudaMemcpyDeviceToHost, c->out_stream));
+        CUDA_TRY(cudaEventRecord(c->ev_out[q.id], c->out_stream));
+        c->out_pending[q.id] = true;
+    }
     return MHPC_OK;
+}
+
+int mhpc_host_wait(mhpc_ctx* c) {
+    if (!c) return MHPC_ERR_ARG;
+    if (c->out_stream) CUDA_TRY(cudaStreamSynchronize(c->out_stream));
+    if (c->copy_stream) CUDA_TRY(cudaStreamSynchronize(c->copy_stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return read_status(c);
+}
+
+int mhpc_integrate_host(mhpc_ctx* c, mhpc_particles* h, int step, double* dt_out) {
+    TRY(mhpc_integrate_host_async(c, h, step, dt_out));
+    return mhpc_host_wait(c);
 }
 
 int mhpc_export_sorted(mhpc_ctx* c, uint64_t* keys_dev, int* perm_dev) {

@@ -496,10 +496,12 @@ def test_potential_matches_direct_sum(precision, cuda):
     sim.close()
 
 
-@pytest.mark.parametrize("pinned", [False, True])
-def test_integrate_host_matches_device(pinned, cuda):
+@pytest.mark.parametrize("pinned,pipelined", [(False, False), (True, False), (True, True)])
+def test_integrate_host_matches_device(pinned, pipelined, cuda):
     """mhpc_integrate_host (host arrays in and out, positions copied out while
-    the right-hand side runs) gives the device path's state bit for bit."""
+    the right-hand side runs) gives the device path's state bit for bit; so do
+    successive mhpc_integrate_host_async calls (each step's copy-out overlapping
+    the next step's copy-in) with one mhpc_host_wait at the end."""
     n = 20_000
     P = ics.plummer(n, seed=9)
     cfg = gravity_cfg(sfc=1, precision=1, theta_mixed=0.3, gravity_mac=1, mac_alpha=2e-3, time_step=0.01)
@@ -521,8 +523,51 @@ def test_integrate_host_matches_device(pinned, cuda):
     L = _lib.load()
     dt = ctypes.c_double()
     for k in range(3):
-        _lib.check(L.mhpc_integrate_host(hsim.ctx, ctypes.byref(hp), k, ctypes.byref(dt)), "integrate_host")
+        if pipelined:
+            _lib.check(L.mhpc_integrate_host_async(hsim.ctx, ctypes.byref(hp), k, ctypes.byref(dt)), "async")
+        else:
+            _lib.check(L.mhpc_integrate_host(hsim.ctx, ctypes.byref(hp), k, ctypes.byref(dt)), "integrate_host")
+    if pipelined:
+        _lib.check(L.mhpc_host_wait(hsim.ctx), "host_wait")
     for f in ["x", "y", "z", "vx", "vy", "vz", "g_ax", "g_ay", "g_az"]:
+        assert np.array_equal(host[f].numpy(), dev.numpy(f)), f
+    dev.close()
+    hsim.close()
+
+
+def test_integrate_host_async_sph_matches_device(cuda):
+    """Pipelined host-state steps of an SPH configuration (explicit Euler,
+    variable h): outputs that are not inputs (the SPH accelerations) are
+    copied out before the next step's compute overwrites them; three steps
+    equal the device path bit for bit."""
+    C = ics.rotating_cloud(20_000, seed=4)
+    n = len(C["x"])
+    S = dict(C)
+    S["p"] = np.zeros(n)
+    S["cs"] = np.zeros(n)
+    cfg = sph_cfg(variable_sml=1, integrate_energy=0, sml_band_rounds=4, time_step=1e-3)
+    mat = material(interactions=60, eos_type=0, K=C["cs2"], gamma=1.0)
+    dev = Miluphpc(cfg, S, materials=[mat])
+    for k in range(3):
+        dev.integrate(k)
+    hsim = Miluphpc(cfg, S, materials=[mat])
+    fields = ["x", "y", "z", "mass", "vx", "vy", "vz", "sml", "e", "rho", "p", "cs", "ax", "ay", "az"]
+    host = {}
+    for f in fields:
+        t = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        t.copy_(torch.as_tensor(np.asarray(S[f], dtype=np.float64)) if f in S else torch.zeros(n, dtype=torch.float64))
+        host[f] = t
+    hp = _lib.Particles()
+    hp.n = n
+    hp.num_nodes = n
+    for f in fields:
+        setattr(hp, f, ctypes.cast(ctypes.c_void_p(host[f].data_ptr()), _lib.P_d))
+    L = _lib.load()
+    dt = ctypes.c_double()
+    for k in range(3):
+        _lib.check(L.mhpc_integrate_host_async(hsim.ctx, ctypes.byref(hp), k, ctypes.byref(dt)), "async")
+    _lib.check(L.mhpc_host_wait(hsim.ctx), "host_wait")
+    for f in ["x", "y", "z", "vx", "vy", "vz", "sml", "rho", "p", "cs", "ax", "ay", "az"]:
         assert np.array_equal(host[f].numpy(), dev.numpy(f)), f
     dev.close()
     hsim.close()
