@@ -335,7 +335,14 @@ __global__ void __launch_bounds__(kWalkBlock) k_grav_mixed(const float4* __restr
 // limited to keep room for a depth-first descent (7 per level, 21 levels)
 // on top of the current stack; the stack never overflows, a check that cannot
 // fire reports MHPC_ERR_DEPTH instead of writing past it.
-constexpr int kListGroup = 64;
+// particles per lane (2: groups of 64; 4: groups of 128, build-time choice)
+#ifndef MHPC_LIST_PPL
+#define MHPC_LIST_PPL 2
+#endif
+constexpr int kPPL = MHPC_LIST_PPL;
+constexpr int kNP = kPPL / 2;  // particle pairs per lane (one paired FP32 instruction each)
+constexpr int kListGroup = 32 * kPPL;
+constexpr int kEvalUnroll = kPPL == 2 ? 8 : 4;
 constexpr int kListSub = 8;
 constexpr int kListStack = 1024;
 constexpr int kListReserve = 7 * 22 + 8;
@@ -373,73 +380,98 @@ __device__ __forceinline__ float2 rsqrt2(float2 r2) {
 }
 
 template <bool kGuard>
-__device__ __forceinline__ void eval_cells_x2(const ListSmem& S, int count, const float (&rx)[2],
-                                              const float (&ry)[2], const float (&rz)[2], const float (&e2)[2],
-                                              double (&ax)[2], double (&ay)[2], double (&az)[2]) {
-    const float2 PX = make_float2(rx[0], rx[1]), PY = make_float2(ry[0], ry[1]), PZ = make_float2(rz[0], rz[1]);
-    const float2 E2 = make_float2(e2[0], e2[1]);
-    float2 fx = bc2(0.f), fy = bc2(0.f), fz = bc2(0.f);
-#pragma unroll 8
-    for (int e = 0; e < count; ++e) {
-        const float4 c = S.cpos[e];
-        const float4 a0 = S.cq0[e];
-        const float2 a1 = S.cq1[e];
-        const float2 Rx = __fadd2_rn(PX, bc2(-c.x)), Ry = __fadd2_rn(PY, bc2(-c.y)), Rz = __fadd2_rn(PZ, bc2(-c.z));
-        const float2 r2 = __ffma2_rn(Rx, Rx, __ffma2_rn(Ry, Ry, __ffma2_rn(Rz, Rz, E2)));
-        const float2 ri = rsqrt2<kGuard>(r2);
-        const float2 ri2 = __fmul2_rn(ri, ri);
-        const float2 ri3 = __fmul2_rn(ri, ri2);
-        const float2 ri5 = __fmul2_rn(ri3, ri2);
-        const float2 qx = __ffma2_rn(bc2(a0.x), Rx, __ffma2_rn(bc2(a0.y), Ry, __fmul2_rn(bc2(a0.z), Rz)));
-        const float2 qy = __ffma2_rn(bc2(a0.y), Rx, __ffma2_rn(bc2(a0.w), Ry, __fmul2_rn(bc2(a1.x), Rz)));
-        const float2 qz = __ffma2_rn(bc2(a0.z), Rx, __ffma2_rn(bc2(a1.x), Ry, __fmul2_rn(bc2(a1.y), Rz)));
-        const float2 rqr = __ffma2_rn(qx, Rx, __ffma2_rn(qy, Ry, __fmul2_rn(qz, Rz)));
-        // -(m/r^3 + 5/2 RQR/r^7)
-        const float2 cc = __ffma2_rn(bc2(-c.w), ri3, __fmul2_rn(__fmul2_rn(__fmul2_rn(bc2(-2.5f), rqr), ri5), ri2));
-        fx = __ffma2_rn(cc, Rx, __ffma2_rn(qx, ri5, fx));
-        fy = __ffma2_rn(cc, Ry, __ffma2_rn(qy, ri5, fy));
-        fz = __ffma2_rn(cc, Rz, __ffma2_rn(qz, ri5, fz));
+__device__ __forceinline__ void eval_cells_x2(const ListSmem& S, int count, const float (&rx)[kPPL],
+                                              const float (&ry)[kPPL], const float (&rz)[kPPL],
+                                              const float (&e2)[kPPL], double (&ax)[kPPL], double (&ay)[kPPL],
+                                              double (&az)[kPPL]) {
+    float2 PX[kNP], PY[kNP], PZ[kNP], E2[kNP], fx[kNP], fy[kNP], fz[kNP];
+#pragma unroll
+    for (int q = 0; q < kNP; ++q) {
+        PX[q] = make_float2(rx[2 * q], rx[2 * q + 1]); PY[q] = make_float2(ry[2 * q], ry[2 * q + 1]);
+        PZ[q] = make_float2(rz[2 * q], rz[2 * q + 1]); E2[q] = make_float2(e2[2 * q], e2[2 * q + 1]);
+        fx[q] = bc2(0.f); fy[q] = bc2(0.f); fz[q] = bc2(0.f);
     }
-    ax[0] += fx.x; ay[0] += fy.x; az[0] += fz.x;
-    ax[1] += fx.y; ay[1] += fy.y; az[1] += fz.y;
-}
-
-template <bool kGuard>
-__device__ __forceinline__ void eval_leaves_x2(const ListSmem& S, int count, const float (&rx)[2],
-                                               const float (&ry)[2], const float (&rz)[2], const float (&e2)[2],
-                                               double (&ax)[2], double (&ay)[2], double (&az)[2]) {
-    const float2 PX = make_float2(rx[0], rx[1]), PY = make_float2(ry[0], ry[1]), PZ = make_float2(rz[0], rz[1]);
-    const float2 E2 = make_float2(e2[0], e2[1]);
-    float2 fx = bc2(0.f), fy = bc2(0.f), fz = bc2(0.f);
-#pragma unroll 8
-    for (int e = 0; e < count; ++e) {
-        const float4 c = S.lpos[e];
-        const float2 Rx = __fadd2_rn(PX, bc2(-c.x)), Ry = __fadd2_rn(PY, bc2(-c.y)), Rz = __fadd2_rn(PZ, bc2(-c.z));
-        const float2 r2 = __ffma2_rn(Rx, Rx, __ffma2_rn(Ry, Ry, __ffma2_rn(Rz, Rz, E2)));
-        const float2 ri = rsqrt2<kGuard>(r2);
-        const float2 nm = __fmul2_rn(bc2(-c.w), __fmul2_rn(__fmul2_rn(ri, ri), ri));  // -m / r^3
-        fx = __ffma2_rn(nm, Rx, fx);
-        fy = __ffma2_rn(nm, Ry, fy);
-        fz = __ffma2_rn(nm, Rz, fz);
-    }
-    ax[0] += fx.x; ay[0] += fy.x; az[0] += fz.x;
-    ax[1] += fx.y; ay[1] += fy.y; az[1] += fz.y;
-}
-
-// kPot: also the potential, -(m/r + RQR/(2 r^5)) per cell and -m/r per leaf,
-// leaving out the particle's own leaf (R = 0 exactly).
-template <bool kGuard, bool kPot>
-__device__ __forceinline__ void eval_cells(const ListSmem& S, int count, const float (&rx)[2], const float (&ry)[2],
-                                           const float (&rz)[2], const float (&e2)[2], double (&ax)[2],
-                                           double (&ay)[2], double (&az)[2], double (&ph)[2]) {
-    float fx[2] = {0.f, 0.f}, fy[2] = {0.f, 0.f}, fz[2] = {0.f, 0.f}, fp[2] = {0.f, 0.f};
-#pragma unroll 4
+#pragma unroll kEvalUnroll
     for (int e = 0; e < count; ++e) {
         const float4 c = S.cpos[e];
         const float4 a0 = S.cq0[e];
         const float2 a1 = S.cq1[e];
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
+        for (int q = 0; q < kNP; ++q) {
+            const float2 Rx = __fadd2_rn(PX[q], bc2(-c.x)), Ry = __fadd2_rn(PY[q], bc2(-c.y)),
+                         Rz = __fadd2_rn(PZ[q], bc2(-c.z));
+            const float2 r2 = __ffma2_rn(Rx, Rx, __ffma2_rn(Ry, Ry, __ffma2_rn(Rz, Rz, E2[q])));
+            const float2 ri = rsqrt2<kGuard>(r2);
+            const float2 ri2 = __fmul2_rn(ri, ri);
+            const float2 ri3 = __fmul2_rn(ri, ri2);
+            const float2 ri5 = __fmul2_rn(ri3, ri2);
+            const float2 qx = __ffma2_rn(bc2(a0.x), Rx, __ffma2_rn(bc2(a0.y), Ry, __fmul2_rn(bc2(a0.z), Rz)));
+            const float2 qy = __ffma2_rn(bc2(a0.y), Rx, __ffma2_rn(bc2(a0.w), Ry, __fmul2_rn(bc2(a1.x), Rz)));
+            const float2 qz = __ffma2_rn(bc2(a0.z), Rx, __ffma2_rn(bc2(a1.x), Ry, __fmul2_rn(bc2(a1.y), Rz)));
+            const float2 rqr = __ffma2_rn(qx, Rx, __ffma2_rn(qy, Ry, __fmul2_rn(qz, Rz)));
+            // -(m/r^3 + 5/2 RQR/r^7)
+            const float2 cc =
+                __ffma2_rn(bc2(-c.w), ri3, __fmul2_rn(__fmul2_rn(__fmul2_rn(bc2(-2.5f), rqr), ri5), ri2));
+            fx[q] = __ffma2_rn(cc, Rx, __ffma2_rn(qx, ri5, fx[q]));
+            fy[q] = __ffma2_rn(cc, Ry, __ffma2_rn(qy, ri5, fy[q]));
+            fz[q] = __ffma2_rn(cc, Rz, __ffma2_rn(qz, ri5, fz[q]));
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < kNP; ++q) {
+        ax[2 * q] += fx[q].x; ay[2 * q] += fy[q].x; az[2 * q] += fz[q].x;
+        ax[2 * q + 1] += fx[q].y; ay[2 * q + 1] += fy[q].y; az[2 * q + 1] += fz[q].y;
+    }
+}
+
+template <bool kGuard>
+__device__ __forceinline__ void eval_leaves_x2(const ListSmem& S, int count, const float (&rx)[kPPL],
+                                               const float (&ry)[kPPL], const float (&rz)[kPPL],
+                                               const float (&e2)[kPPL], double (&ax)[kPPL], double (&ay)[kPPL],
+                                               double (&az)[kPPL]) {
+    float2 PX[kNP], PY[kNP], PZ[kNP], E2[kNP], fx[kNP], fy[kNP], fz[kNP];
+#pragma unroll
+    for (int q = 0; q < kNP; ++q) {
+        PX[q] = make_float2(rx[2 * q], rx[2 * q + 1]); PY[q] = make_float2(ry[2 * q], ry[2 * q + 1]);
+        PZ[q] = make_float2(rz[2 * q], rz[2 * q + 1]); E2[q] = make_float2(e2[2 * q], e2[2 * q + 1]);
+        fx[q] = bc2(0.f); fy[q] = bc2(0.f); fz[q] = bc2(0.f);
+    }
+#pragma unroll kEvalUnroll
+    for (int e = 0; e < count; ++e) {
+        const float4 c = S.lpos[e];
+#pragma unroll
+        for (int q = 0; q < kNP; ++q) {
+            const float2 Rx = __fadd2_rn(PX[q], bc2(-c.x)), Ry = __fadd2_rn(PY[q], bc2(-c.y)),
+                         Rz = __fadd2_rn(PZ[q], bc2(-c.z));
+            const float2 r2 = __ffma2_rn(Rx, Rx, __ffma2_rn(Ry, Ry, __ffma2_rn(Rz, Rz, E2[q])));
+            const float2 ri = rsqrt2<kGuard>(r2);
+            const float2 nm = __fmul2_rn(bc2(-c.w), __fmul2_rn(__fmul2_rn(ri, ri), ri));  // -m / r^3
+            fx[q] = __ffma2_rn(nm, Rx, fx[q]);
+            fy[q] = __ffma2_rn(nm, Ry, fy[q]);
+            fz[q] = __ffma2_rn(nm, Rz, fz[q]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < kNP; ++q) {
+        ax[2 * q] += fx[q].x; ay[2 * q] += fy[q].x; az[2 * q] += fz[q].x;
+        ax[2 * q + 1] += fx[q].y; ay[2 * q + 1] += fy[q].y; az[2 * q + 1] += fz[q].y;
+    }
+}
+
+// kPot: also the potential, -(m/r + RQR/(2 r^5)) per cell and -m/r per leaf,
+// leaving out the particle's own leaf (R = 0 exactly).
+template <bool kGuard, bool kPot>
+__device__ __forceinline__ void eval_cells(const ListSmem& S, int count, const float (&rx)[kPPL], const float (&ry)[kPPL],
+                                           const float (&rz)[kPPL], const float (&e2)[kPPL], double (&ax)[kPPL],
+                                           double (&ay)[kPPL], double (&az)[kPPL], double (&ph)[kPPL]) {
+    float fx[kPPL] = {}, fy[kPPL] = {}, fz[kPPL] = {}, fp[kPPL] = {};
+#pragma unroll kEvalUnroll
+    for (int e = 0; e < count; ++e) {
+        const float4 c = S.cpos[e];
+        const float4 a0 = S.cq0[e];
+        const float2 a1 = S.cq1[e];
+#pragma unroll
+        for (int k = 0; k < kPPL; ++k) {
             const float Rx = rx[k] - c.x, Ry = ry[k] - c.y, Rz = rz[k] - c.z;
             const float r2 = fmaf(Rx, Rx, fmaf(Ry, Ry, fmaf(Rz, Rz, e2[k])));
             const float ri = kGuard ? (r2 > 0.f ? rsqrtf(r2) : 0.f) : rsqrtf(r2);
@@ -459,22 +491,22 @@ __device__ __forceinline__ void eval_cells(const ListSmem& S, int count, const f
         }
     }
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < kPPL; ++k) {
         ax[k] += fx[k]; ay[k] += fy[k]; az[k] += fz[k];
         if (kPot) ph[k] += fp[k];
     }
 }
 
 template <bool kGuard, bool kPot>
-__device__ __forceinline__ void eval_leaves(const ListSmem& S, int count, const float (&rx)[2], const float (&ry)[2],
-                                            const float (&rz)[2], const float (&e2)[2], double (&ax)[2],
-                                            double (&ay)[2], double (&az)[2], double (&ph)[2]) {
-    float fx[2] = {0.f, 0.f}, fy[2] = {0.f, 0.f}, fz[2] = {0.f, 0.f}, fp[2] = {0.f, 0.f};
-#pragma unroll 4
+__device__ __forceinline__ void eval_leaves(const ListSmem& S, int count, const float (&rx)[kPPL], const float (&ry)[kPPL],
+                                            const float (&rz)[kPPL], const float (&e2)[kPPL], double (&ax)[kPPL],
+                                            double (&ay)[kPPL], double (&az)[kPPL], double (&ph)[kPPL]) {
+    float fx[kPPL] = {}, fy[kPPL] = {}, fz[kPPL] = {}, fp[kPPL] = {};
+#pragma unroll kEvalUnroll
     for (int e = 0; e < count; ++e) {
         const float4 c = S.lpos[e];
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < kPPL; ++k) {
             const float Rx = rx[k] - c.x, Ry = ry[k] - c.y, Rz = rz[k] - c.z;
             const float r2 = fmaf(Rx, Rx, fmaf(Ry, Ry, fmaf(Rz, Rz, e2[k])));
             const float ri = kGuard ? (r2 > 0.f ? rsqrtf(r2) : 0.f) : rsqrtf(r2);
@@ -486,7 +518,7 @@ __device__ __forceinline__ void eval_leaves(const ListSmem& S, int count, const 
         }
     }
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < kPPL; ++k) {
         ax[k] += fx[k]; ay[k] += fy[k]; az[k] += fz[k];
         if (kPot) ph[k] += fp[k];
     }
@@ -495,16 +527,16 @@ __device__ __forceinline__ void eval_leaves(const ListSmem& S, int count, const 
 // the packed forms for the force walk, the scalar forms when the potential is wanted
 constexpr bool kPackedEval = true;
 template <bool kGuard, bool kPot>
-__device__ __forceinline__ void eval_cells_sel(const ListSmem& S, int count, const float (&rx)[2], const float (&ry)[2],
-                                               const float (&rz)[2], const float (&e2)[2], double (&ax)[2],
-                                               double (&ay)[2], double (&az)[2], double (&ph)[2]) {
+__device__ __forceinline__ void eval_cells_sel(const ListSmem& S, int count, const float (&rx)[kPPL], const float (&ry)[kPPL],
+                                               const float (&rz)[kPPL], const float (&e2)[kPPL], double (&ax)[kPPL],
+                                               double (&ay)[kPPL], double (&az)[kPPL], double (&ph)[kPPL]) {
     if (kPackedEval && !kPot) eval_cells_x2<kGuard>(S, count, rx, ry, rz, e2, ax, ay, az);
     else eval_cells<kGuard, kPot>(S, count, rx, ry, rz, e2, ax, ay, az, ph);
 }
 template <bool kGuard, bool kPot>
-__device__ __forceinline__ void eval_leaves_sel(const ListSmem& S, int count, const float (&rx)[2], const float (&ry)[2],
-                                                const float (&rz)[2], const float (&e2)[2], double (&ax)[2],
-                                                double (&ay)[2], double (&az)[2], double (&ph)[2]) {
+__device__ __forceinline__ void eval_leaves_sel(const ListSmem& S, int count, const float (&rx)[kPPL], const float (&ry)[kPPL],
+                                                const float (&rz)[kPPL], const float (&e2)[kPPL], double (&ax)[kPPL],
+                                                double (&ay)[kPPL], double (&az)[kPPL], double (&ph)[kPPL]) {
     if (kPackedEval && !kPot) eval_leaves_x2<kGuard>(S, count, rx, ry, rz, e2, ax, ay, az);
     else eval_leaves<kGuard, kPot>(S, count, rx, ry, rz, e2, ax, ay, az, ph);
 }
@@ -537,13 +569,13 @@ __global__ void __launch_bounds__(kListBlock, MHPC_LISTS_MIN_BLOCKS) k_grav_list
     const long ngroups = ((long)P.n + kListGroup - 1) / kListGroup;
     if (gwarp >= ngroups) return;
     const long s0 = gwarp * kListGroup;
-    long s[2];
-    bool valid[2];
-    int sl[2];
-    float e2[2];
+    long s[kPPL];
+    bool valid[kPPL];
+    int sl[kPPL];
+    float e2[kPPL];
     double lox = 1e300, loy = 1e300, loz = 1e300, hix = -1e300, hiy = -1e300, hiz = -1e300;
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < kPPL; ++k) {
         s[k] = s0 + k * 32 + lane;
         valid[k] = s[k] < P.n;
         sl[k] = (int)(valid[k] ? s[k] : (long)P.n - 1);
@@ -572,16 +604,16 @@ __global__ void __launch_bounds__(kListBlock, MHPC_LISTS_MIN_BLOCKS) k_grav_list
     const double cx = 0.5 * (lox + hix), cy = 0.5 * (loy + hiy), cz = 0.5 * (loz + hiz);
     const float chx = (float)cx, chy = (float)cy, chz = (float)cz;
     const float clx = (float)(cx - (double)chx), cly = (float)(cy - (double)chy), clz = (float)(cz - (double)chz);
-    float rx[2], ry[2], rz[2];
+    float rx[kPPL], ry[kPPL], rz[kPPL];
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < kPPL; ++k) {
         const int lf = __ldg(T.leaf_node + sl[k]);
         const float4 hp = __ldg(T.wrec + 4 * (size_t)lf);
         const float4 lp = __ldg(T.wrec + 4 * (size_t)lf + 1);
         rx[k] = (hp.x - chx) + (lp.x - clx);
         ry[k] = (hp.y - chy) + (lp.y - cly);
         rz[k] = (hp.z - chz) + (lp.z - clz);
-        // sub-box of members [8b, 8b + 8): 8-lane segments of member row k;
+        // sub-box of members [4 kPPL b, 4 kPPL (b + 1)): 4 kPPL-lane segments of member row k;
         // relative rule: alpha times the smallest previous |a| of the sub-box
         // (read before this walk overwrites the accelerations)
         float amin = 0.f;
@@ -593,7 +625,7 @@ __global__ void __launch_bounds__(kListBlock, MHPC_LISTS_MIN_BLOCKS) k_grav_list
         }
         float bx0 = rx[k], by0 = ry[k], bz0 = rz[k], bx1 = rx[k], by1 = ry[k], bz1 = rz[k];
 #pragma unroll
-        for (int o = 4; o > 0; o >>= 1) {
+        for (int o = 2 * kPPL; o > 0; o >>= 1) {
             bx0 = fminf(bx0, __shfl_xor_sync(MHPC_FULL, bx0, o));
             by0 = fminf(by0, __shfl_xor_sync(MHPC_FULL, by0, o));
             bz0 = fminf(bz0, __shfl_xor_sync(MHPC_FULL, bz0, o));
@@ -602,8 +634,8 @@ __global__ void __launch_bounds__(kListBlock, MHPC_LISTS_MIN_BLOCKS) k_grav_list
             if (kRel) amin = fminf(amin, __shfl_xor_sync(MHPC_FULL, amin, o));
             bz1 = fmaxf(bz1, __shfl_xor_sync(MHPC_FULL, bz1, o));
         }
-        if ((lane & 7) == 0) {
-            const int b = 4 * k + (lane >> 3);
+        if ((lane & (4 * kPPL - 1)) == 0) {
+            const int b = k * (8 / kPPL) + lane / (4 * kPPL);
             S.bx0[b] = bx0; S.by0[b] = by0; S.bz0[b] = bz0; S.bw0[b] = amin;
             // bhi.w: quad_alpha |a|_min of the sub-box (monopole threshold)
             S.nbx1[b] = -bx1; S.nby1[b] = -by1; S.nbz1[b] = -bz1; S.bw1[b] = kRel ? amin * qratio : 0.f;
@@ -620,7 +652,7 @@ __global__ void __launch_bounds__(kListBlock, MHPC_LISTS_MIN_BLOCKS) k_grav_list
     }
     top = __shfl_sync(MHPC_FULL, top, 0);
     __syncwarp();
-    double ax[2] = {0.0, 0.0}, ay[2] = {0.0, 0.0}, az[2] = {0.0, 0.0}, ph[2] = {0.0, 0.0};
+    double ax[kPPL] = {}, ay[kPPL] = {}, az[kPPL] = {}, ph[kPPL] = {};
     int ncell = 0, nleaf = 0;
     unsigned long long tested = 0, ncell_tot = 0, nleaf_tot = 0;
     while (top > 0) {
@@ -776,7 +808,7 @@ __global__ void __launch_bounds__(kListBlock, MHPC_LISTS_MIN_BLOCKS) k_grav_list
     nleaf_tot += nleaf;
     unsigned nv = 0;
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
+    for (int k = 0; k < kPPL; ++k) {
         if (valid[k]) {
             const int o = __ldg(perm + s[k]);
             gax[o] = P.G * ax[k]; gay[o] = P.G * ay[k]; gaz[o] = P.G * az[k];
