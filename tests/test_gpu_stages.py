@@ -428,6 +428,28 @@ def test_variable_h_on_lists_matches_oracle(spread, cuda):
     sim.close()
 
 
+@pytest.mark.parametrize("n", [1, 7, 100, 1000])
+def test_variable_h_on_lists_small_n(n, cuda):
+    """The list-based variable-h iteration and the band repair on a handful of
+    particles (partial warps, a single tree leaf, counts far below the target):
+    h equal to the oracle's iteration, lists equal to the brute-force sets."""
+    S, C = _cloud_state(max(n, 2), seed=11)
+    S = {k: (v[:n].copy() if isinstance(v, np.ndarray) and v.shape[:1] == (max(n, 2),) else v) for k, v in S.items()}
+    mat = material(interactions=60, eos_type=0, K=C["cs2"], gamma=1.0)
+    sim = Miluphpc(sph_cfg(variable_sml=1, integrate_energy=0), S, materials=[mat], want_nnl=True)
+    sim.rhs(0)
+    h_gpu = sim.numpy("sml")
+    h_orc, _, _ = O.variable_h(S["x"], S["y"], S["z"], S["sml"], 60, tol=5, max_nb=180, max_iter=5)
+    assert (np.abs(h_gpu - h_orc) <= 1e-12 * h_orc).mean() > 0.99
+    off, nbr = O.frnn(S["x"], S["y"], S["z"], h_gpu)
+    noi = sim.numpy("noi")
+    assert np.array_equal(noi, np.diff(off))
+    nnl = sim.t["nnl"].cpu().numpy().reshape(n, 180)
+    for i in range(n):
+        assert np.array_equal(np.sort(nnl[i, :noi[i]]), nbr[off[i]:off[i + 1]]), i
+    sim.close()
+
+
 def test_variable_h_on_lists_after_steps(cuda):
     """The common case of the list-based iteration: a few steps into a run
     (band repair on), where most particles start in the band and the few
