@@ -665,15 +665,16 @@ def launches_per_step(variant, kind="gravity", band_rounds=8):
     grav = tree + 1  # + the walk
     if kind == "cloud":
         # variable h on lists: copy of h, largest-h bounds (leaves + 21 levels), the
-        # list walk of the starting h, 7 sweeps x (flags, 4 scan, compact, update,
-        # event reset, events, removals, compaction, appends, commit, gated re-walk),
-        # record after the first sweep, final flags + 4 scan + record, sort of the
-        # appended lists, list statistics, scatter of h; band repair: 2 copies,
+        # list walk of the starting h, the first sweep's list (flags, 4 scan,
+        # compact), 7 sweeps x (update, event reset, events, marks, filter, appends,
+        # commit, gated re-walk), the next list of each later sweep (6), record after
+        # the first sweep, final list + record, sort of the appended lists, list
+        # statistics, scatter of h; band repair: 2 copies,
         # rounds x (flags, 4 scan, compact, select, events, remove, compact, add,
         # commit), sort of the appended lists, scatter of h; (mixed: position pack)
         # density, forces, noi export, band statistics; learned h: apply, collect,
         # features; explicit Euler update
-        vh = 1 + 22 + 1 + 7 * 14 + 1 + 5 + 1 + 1 + 1 + 1
+        vh = 1 + 22 + 1 + 6 + 7 * 8 + 6 + 1 + 2 + 1 + 1 + 1
         band = (2 + 12 * band_rounds + 1 + 1) if band_rounds > 0 else 0
         sphk = band + (1 if mixed else 0) + 4
         learned = 3 if mixed else 0

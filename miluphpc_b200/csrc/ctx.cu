@@ -51,6 +51,7 @@ struct mhpc_ctx {
     double* hold = nullptr;
     int *vh_done = nullptr, *vh_nit = nullptr, *vh_count = nullptr;
     int *vh_flags = nullptr, *vh_off = nullptr, *vh_list = nullptr;
+    int *vh_list2 = nullptr, *vh_cnt = nullptr;  // alternating sweep lists and their lengths
     double* h_start = nullptr;  // sorted h the variable-h iteration started from
     double last_dt = 0.0;
     double* diag_part = nullptr;
@@ -332,6 +333,7 @@ int stage_frnn(mhpc_ctx* c, const mhpc_particles* p, bool variable_h, bool learn
         VhBuffers B;
         B.hold = c->hold; B.done = c->vh_done; B.nit = c->vh_nit; B.count = c->vh_count;
         B.flags = c->vh_flags; B.off = c->vh_off; B.list = c->vh_list; B.scan_scratch = c->scan_scratch;
+        B.list2 = c->vh_list2; B.cnt = c->vh_cnt;
         if (MHPC_VH_LISTS) {
             // the iteration on lists: its lists are the right-hand side's
             BandBuffers E;
@@ -593,6 +595,7 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
         A(c->noi, n);
         A(c->hold, n); A(c->vh_done, n); A(c->vh_nit, n); A(c->vh_count, n);
         A(c->vh_flags, n); A(c->vh_off, n + 1); A(c->vh_list, n); A(c->h_start, n);
+        A(c->vh_list2, n); A(c->vh_cnt, 2);
         // band repair events: a round changes a few pairs per out-of-band particle
         // (room for 4 per particle: a round that needs more is skipped and counted)
         c->band_cap = (int)std::min<size_t>(2147483000, std::max<size_t>(4096, 4 * n));

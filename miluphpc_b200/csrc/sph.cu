@@ -538,6 +538,18 @@ __global__ void k_copy(int n, const double* __restrict__ a, double* b) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) b[i] = a[i];
 }
 
+// The particles of `in` that have not stopped, appended to `out` (order
+// irrelevant: every particle's update and pair edits depend on it alone, and
+// the appended lists are sorted at the end); *out_count must be zero.
+__global__ void k_next_list(const int* __restrict__ in, const int* __restrict__ in_count,
+                            const int* __restrict__ done, int* out, int* out_count) {
+    const int m = *in_count;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < m; q += gridDim.x * blockDim.x) {
+        const int i = in[q];
+        if (!done[i]) out[atomicAdd(out_count, 1)] = i;
+    }
+}
+
 // End of a sweep on lists: every iterating particle takes its new h; the
 // lists are re-walked when they are truncated (a count above maxnb) or when
 // the sweep's pair changes overflowed the event buffer (nothing was edited).
@@ -950,26 +962,41 @@ int sph_variable_h_lists(const TreeDev& T, const SphParams& P, const double* x, 
     // the lists and counts of the starting h: the counts of the first sweep
     k_frnn<2><<<(int)blocks, kBlock, 0, s>>>(T, P.n, P.maxnb, x, y, z, h, nullptr, nullptr, T.hmax, nbr, noi, st,
                                               rewalk, trunc);
-    for (int it = 0; it < sweeps; ++it) {
-        k_flags<<<g, 256, 0, s>>>(P.n, V.done, V.flags);
-        rc = scan_exclusive_i32(V.flags, V.off, P.n, V.scan_scratch, s);
-        if (rc) return rc;
-        k_compact<<<g, 256, 0, s>>>(P.n, V.flags, V.off, V.list);
-        if (it == 1) k_record_active<<<1, 1, 0, s>>>(list_count, P.n, st);
-        // the reference's update from the exact counts of the current h (Jacobi:
-        // every new h goes to hnew first)
-        k_vh_update<<<g, 256, 0, s>>>(V.list, list_count, noi, hnew, hnew, V.done, V.nit, target, tol, max_iter,
-                                      P.maxnb, T.hmax, T.leaf_node, T.parent, P.ord);
-        rc = sph_apply_h_changes(T, P, x, y, z, h, hnew, nbr, noi, V.list, list_count, B, trunc, st, s);
-        if (rc) return rc;
-        k_vh_commit<<<g, 256, 0, s>>>(V.list, list_count, hnew, h, B.ctr, rewalk);
-        k_frnn<2><<<(int)blocks, kBlock, 0, s>>>(T, P.n, P.maxnb, x, y, z, h, nullptr, nullptr, T.hmax, nbr, noi,
-                                                  st, rewalk, trunc);
-    }
+    // the first sweep lists every particle (ordered, by a scan); later sweeps
+    // keep the particles of the previous list that have not stopped
     k_flags<<<g, 256, 0, s>>>(P.n, V.done, V.flags);
     rc = scan_exclusive_i32(V.flags, V.off, P.n, V.scan_scratch, s);
     if (rc) return rc;
-    k_record_unconverged<<<1, 1, 0, s>>>(list_count, st);
+    k_compact<<<g, 256, 0, s>>>(P.n, V.flags, V.off, V.list);
+    const int* cur = V.list;
+    const int* cur_count = list_count;
+    for (int it = 0; it < sweeps; ++it) {
+        if (it > 0) {
+            int* out = (it & 1) ? V.list2 : V.list;
+            int* out_count = V.cnt + (it & 1);
+            CUDA_TRY(cudaMemsetAsync(out_count, 0, sizeof(int), s));
+            k_next_list<<<g, 256, 0, s>>>(cur, cur_count, V.done, out, out_count);
+            cur = out;
+            cur_count = out_count;
+        }
+        if (it == 1) k_record_active<<<1, 1, 0, s>>>(cur_count, P.n, st);
+        // the reference's update from the exact counts of the current h (Jacobi:
+        // every new h goes to hnew first)
+        k_vh_update<<<g, 256, 0, s>>>(cur, cur_count, noi, hnew, hnew, V.done, V.nit, target, tol, max_iter,
+                                      P.maxnb, T.hmax, T.leaf_node, T.parent, P.ord);
+        rc = sph_apply_h_changes(T, P, x, y, z, h, hnew, nbr, noi, cur, cur_count, B, trunc, st, s);
+        if (rc) return rc;
+        k_vh_commit<<<g, 256, 0, s>>>(cur, cur_count, hnew, h, B.ctr, rewalk);
+        k_frnn<2><<<(int)blocks, kBlock, 0, s>>>(T, P.n, P.maxnb, x, y, z, h, nullptr, nullptr, T.hmax, nbr, noi,
+                                                  st, rewalk, trunc);
+    }
+    {
+        int* out = (sweeps & 1) ? V.list2 : V.list;
+        int* out_count = V.cnt + (sweeps & 1);
+        CUDA_TRY(cudaMemsetAsync(out_count, 0, sizeof(int), s));
+        k_next_list<<<g, 256, 0, s>>>(cur, cur_count, V.done, out, out_count);
+        k_record_unconverged<<<1, 1, 0, s>>>(out_count, st);
+    }
     rc = sph_sort_appended(P, nbr, noi, B.appended, s);
     if (rc) return rc;
     k_noi_stats<<<g, 256, 0, s>>>(P.n, P.maxnb, noi, st);

@@ -65,6 +65,8 @@ struct VhBuffers {
     int* off;            // [n+1] scratch (scan); off[n] = particles still iterating
     int* list;           // [n] particles still iterating
     void* scan_scratch;
+    int* list2;          // [n] second list (list-based form: sweeps after the first alternate lists)
+    int* cnt;            // [2] lengths of the alternating lists
 };
 // Plain variable-h iteration (Jacobi form of fixedRadiusNN_variableSML):
 // updates h (sorted, in place) for `sweeps` sweeps; every sweep walks only the
