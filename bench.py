@@ -652,9 +652,8 @@ def launches_per_step(variant, kind="gravity", band_rounds=8):
     """This library's kernel launches in one timed step (counted from the
     launch sequence; the ncu launch lists in profiles/ show the same)."""
     # every RHS: bbox, bbox_finish, keys, hist, hist_scan, 8 onesweep (13), gather (1),
-    # tree: lcp, count, 4 scan, copy_total, zero_cells, nodes, 3 level-list kernels (12),
-    # upward pass: leaves + 21 levels (22)
-    tree = 13 + 1 + 12 + 22
+    # tree: lcp, count, 4 scan, copy_total, zero_cells, nodes (9), upward pass (1)
+    tree = 13 + 1 + 9 + 1
     mixed = variant == "mixed"
     if kind == "sph":
         # frnn, (mixed: position pack), density+EOS, forces; noi export on the
@@ -664,7 +663,7 @@ def launches_per_step(variant, kind="gravity", band_rounds=8):
         return (rhs + 1) + rhs + 3 + 2
     grav = tree + 1  # + the walk
     if kind == "cloud":
-        # variable h on lists: copy of h, largest-h bounds (leaves + 21 levels), the
+        # variable h on lists: copy of h, largest-h bounds (one upward pass), the
         # list walk of the starting h, the first sweep's list (flags, 4 scan,
         # compact), 7 sweeps x (update, event reset, events, marks, filter, appends,
         # commit, gated re-walk), the next list of each later sweep (6), record after
@@ -674,7 +673,7 @@ def launches_per_step(variant, kind="gravity", band_rounds=8):
         # commit), sort of the appended lists, scatter of h; (mixed: position pack)
         # density, forces, noi export, band statistics; learned h: apply, collect,
         # features; explicit Euler update
-        vh = 1 + 22 + 1 + 6 + 7 * 8 + 6 + 1 + 2 + 1 + 1 + 1
+        vh = 1 + 1 + 1 + 6 + 7 * 8 + 6 + 1 + 2 + 1 + 1 + 1
         band = (2 + 12 * band_rounds + 1 + 1) if band_rounds > 0 else 0
         sphk = band + (1 if mixed else 0) + 4
         learned = 3 if mixed else 0

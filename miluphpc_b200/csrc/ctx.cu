@@ -579,11 +579,10 @@ int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg, const 
     A(T.dl, n); A(T.cnt, n); A(T.off, n + 1); A(T.leaf_node, n);
     A(T.link, M); A(T.first, M); A(T.last, M); A(T.parent, M);
     A(T.kids, 8 * M); A(T.kmask, M);
-    A(T.com, M); A(T.bmin, M); A(T.bmax, M); A(T.hmax, M);
-    A(T.level_cells, M); A(T.level_off, 64);
+    A(T.com, M); A(T.bmin, M); A(T.bmax, M); A(T.hmax, M); A(T.arrive, M);
     A(T.nodes, 1);
     if (cfg->gravity) {
-        A(T.quad0, M); A(T.quad1, M); A(T.wrec, 4 * M);
+        A(T.wrec, 4 * M);
     }
     if (cfg->sph) {
         A(c->svx, n); A(c->svy, n); A(c->svz, n); A(c->se, n); A(c->srho, n); A(c->sp, n); A(c->scs, n);

@@ -6,11 +6,13 @@
 // follow calculateCentersOfMass (tree.cu:1416-1497): m = sum of child masses,
 // x = sum(x_c m_c) / m over the children in curve order, computed with
 // explicitly rounded FP64 multiplies and adds (the reference builds with
-// -fmad=false) so that Lebesgue-ordered results match it bit for bit.  Like
-// the reference (21 launches, miluphpc.cpp:1205-1210) the pass runs one
-// launch per level, deepest first, each over a dense list of that level's
-// cells built once per tree from the sorted keys' common-digit counts; no
-// atomics or fences are involved.
+// -fmad=false) so that Lebesgue-ordered results match it bit for bit.  The
+// reference runs one launch per level (21 launches, miluphpc.cpp:1205-1210);
+// here one launch does the whole pass: each block completes the subtrees
+// inside its range of sorted particles level by level between block
+// barriers, and the few cells that cross a range boundary by counted
+// hand-offs (k_upward below).  The level-L cell starting at sorted position
+// a exists iff dl[a-1] < L <= dl[a]; its id is off[a] + L - dl[a-1] - 1.
 #include "tree.cuh"
 
 namespace {
@@ -143,75 +145,16 @@ __global__ void k_zero_cells(TreeDev T) {
     // are the non-leaf nodes, whose ids are unknown before the scan, so clear all.
     int total = *T.nodes;
     if (total > T.cap_nodes) total = T.cap_nodes;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) T.kmask[i] = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        T.kmask[i] = 0;
+        T.arrive[i] = 0;
+    }
 }
 
 __global__ void k_copy_total(TreeDev T) { *T.nodes = T.off[T.n]; }
 
 __device__ __forceinline__ float rd(double v) { return __double2float_rd(v); }
 __device__ __forceinline__ float ru(double v) { return __double2float_ru(v); }
-
-// Cell lists per level.  The level-L cell starting at sorted position a
-// exists iff dl[a-1] < L <= dl[a] (its id is off[a] + L - dl[a-1] - 1);
-// k_level_count histograms them per block in shared memory, k_level_offsets
-// scans the 21 counts, k_level_fill reserves one range per (block, level) and
-// scatters the cell ids.  A block takes a fixed chunk of sorted positions, so
-// both passes see the same cells; the order inside a level is irrelevant.
-constexpr int kLevelChunk = 2048;
-
-__global__ void __launch_bounds__(256) k_level_count(TreeDev T, const DevStatus* st) {
-    if (st->code) return;
-    __shared__ int h[32];
-    if (threadIdx.x < 32) h[threadIdx.x] = 0;
-    __syncthreads();
-    const int a0 = blockIdx.x * kLevelChunk;
-    const int a1 = min(a0 + kLevelChunk, T.n);
-    for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
-        const int dp = dl_at(T.dl, a - 1), dc = T.dl[a];
-        for (int L = dp + 1; L <= dc; ++L) atomicAdd(&h[L], 1);
-    }
-    __syncthreads();
-    if (threadIdx.x >= 1 && threadIdx.x <= MHPC_MAX_LEVEL && h[threadIdx.x])
-        atomicAdd(&T.level_off[32 + threadIdx.x], h[threadIdx.x]);
-}
-
-__global__ void k_level_offsets(TreeDev T) {
-    int acc = 0;
-    for (int L = 0; L <= MHPC_MAX_LEVEL + 1; ++L) {
-        const int c = (L >= 1 && L <= MHPC_MAX_LEVEL) ? T.level_off[32 + L] : 0;
-        T.level_off[L] = acc;
-        T.level_off[32 + L] = acc;  // fill cursor of level L
-        acc += c;
-    }
-}
-
-__global__ void __launch_bounds__(256) k_level_fill(TreeDev T, const DevStatus* st) {
-    if (st->code) return;
-    __shared__ int h[32], base[32];
-    if (threadIdx.x < 32) h[threadIdx.x] = 0;
-    __syncthreads();
-    const int a0 = blockIdx.x * kLevelChunk;
-    const int a1 = min(a0 + kLevelChunk, T.n);
-    for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
-        const int dp = dl_at(T.dl, a - 1), dc = T.dl[a];
-        for (int L = dp + 1; L <= dc; ++L) atomicAdd(&h[L], 1);
-    }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-        const int L = threadIdx.x;
-        base[L] = (L >= 1 && L <= MHPC_MAX_LEVEL && h[L]) ? atomicAdd(&T.level_off[32 + L], h[L]) : 0;
-        h[L] = 0;
-    }
-    __syncthreads();
-    for (int a = a0 + threadIdx.x; a < a1; a += blockDim.x) {
-        const int dp = dl_at(T.dl, a - 1), dc = T.dl[a];
-        const int o = T.off[a];
-        for (int L = dp + 1; L <= dc; ++L) {
-            const int i = base[L] + atomicAdd(&h[L], 1);
-            if (i < T.cap_nodes) T.level_cells[i] = o + (L - dp - 1);
-        }
-    }
-}
 
 // Children of cell p by key digit: slot d holds a child where bit d of the
 // mask is set, so visiting d = 0..7 gives the summation order of the
@@ -251,137 +194,333 @@ __device__ __forceinline__ void put_wrec(const TreeDev& T, int i, double x, doub
     w[3] = make_float4(q1.x, q1.y, __int_as_float((info & 0x1ff) | (mask << 9)), ml3);
 }
 
-// Leaves: centre of mass = the particle; with want_quad (mixed walk) the walk
-// record as well (a leaf's quadrupole is zero and never read from quad0/1).
-__global__ void __launch_bounds__(256) k_upward_leaves(TreeDev T, const double* __restrict__ sx,
-                                                       const double* __restrict__ sy, const double* __restrict__ sz,
-                                                       const double* __restrict__ sm, int want_quad,
-                                                       int want_box, const long long* __restrict__ ord,
-                                                       double inv_theta, const DevStatus* st) {
-    if (st->code) return;
-    const double edge0 = want_quad ? ord_to_dbl(ord[1]) - ord_to_dbl(ord[0]) : 0.0;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < T.n; a += gridDim.x * blockDim.x) {
-        const int leaf = T.leaf_node[a];
-        const double px = __ldg(sx + a), py = __ldg(sy + a), pz = __ldg(sz + a), pm = __ldg(sm + a);
-        T.com[leaf] = make_double4(px, py, pz, pm);
-        if (want_box) {
-            T.bmin[leaf] = make_float4(rd(px), rd(py), rd(pz), 0.f);
-            T.bmax[leaf] = make_float4(ru(px), ru(py), ru(pz), 0.f);
-        }
-        if (want_quad)
-            put_wrec(T, leaf, px, py, pz, pm, __ldg(&T.link[leaf].y), 0, make_float4(0.f, 0.f, 0.f, 0.f),
-                     make_float2(0.f, 0.f), edge0, inv_theta);
+// Loads of values that the running upward pass itself writes, never through
+// the non-coherent read-only path: written by this block (`local`), cached
+// in L1, which sees the block's own stores; written by another block,
+// through L2 (ld.global.cg).
+template <typename V>
+__device__ __forceinline__ V ld_up(const V* p, bool local) {
+    return local ? *p : __ldcg(p);
+}
+__device__ __forceinline__ double4 ld_up_d4(const double4* p, bool local) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    const double2 a = ld_up(q, local), b = ld_up(q + 1, local);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// Leaf: centre of mass = the particle; with want_quad (mixed walk) the walk
+// record as well (a leaf's quadrupole is zero; its record's leaf flag says so).
+__device__ __forceinline__ void leaf_moments(const TreeDev& T, int a, int leaf, const double* __restrict__ sx,
+                                             const double* __restrict__ sy, const double* __restrict__ sz,
+                                             const double* __restrict__ sm, int want_quad, int want_box,
+                                             double edge0, double inv_theta) {
+    const double px = __ldg(sx + a), py = __ldg(sy + a), pz = __ldg(sz + a), pm = __ldg(sm + a);
+    T.com[leaf] = make_double4(px, py, pz, pm);
+    if (want_box) {
+        T.bmin[leaf] = make_float4(rd(px), rd(py), rd(pz), 0.f);
+        T.bmax[leaf] = make_float4(ru(px), ru(py), ru(pz), 0.f);
     }
+    if (want_quad)
+        put_wrec(T, leaf, px, py, pz, pm, __ldg(&T.link[leaf].y), 0, make_float4(0.f, 0.f, 0.f, 0.f),
+                 make_float2(0.f, 0.f), edge0, inv_theta);
 }
 
-// One level of the upward pass: every cell of level L combines its children,
-// which the previous launches (deeper levels, leaves) completed.  Centres of
-// mass use explicitly rounded products and sums in slot order, so the result
-// is bit-identical to the level-wise sums of the reference.
-__global__ void __launch_bounds__(256) k_upward_level(TreeDev T, int L, int want_quad, int want_box,
-                                                      const long long* __restrict__ ord, double inv_theta,
-                                                      const DevStatus* st) {
-    if (st->code) return;
-    const double edge0 = want_quad ? ord_to_dbl(ord[1]) - ord_to_dbl(ord[0]) : 0.0;
-    const int i0 = T.level_off[L], i1 = min(T.level_off[L + 1], T.cap_nodes);
-    for (int i = i0 + blockIdx.x * blockDim.x + threadIdx.x; i < i1; i += gridDim.x * blockDim.x) {
-        const int p = T.level_cells[i];
-        const Kids K = cell_kids(T, p);
-        double m = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
-        float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
-        float4 hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
-        auto add_com = [&](int c) {
-            const double4 cc = ldg_d4(&T.com[c]);
-            mx = __dadd_rn(mx, __dmul_rn(cc.x, cc.w));
-            my = __dadd_rn(my, __dmul_rn(cc.y, cc.w));
-            mz = __dadd_rn(mz, __dmul_rn(cc.z, cc.w));
-            m = __dadd_rn(m, cc.w);
-            if (want_box) {
-                const float4 bl = __ldg(&T.bmin[c]), bh = __ldg(&T.bmax[c]);
-                lo.x = fminf(lo.x, bl.x); lo.y = fminf(lo.y, bl.y); lo.z = fminf(lo.z, bl.z);
-                hi.x = fmaxf(hi.x, bh.x); hi.y = fmaxf(hi.y, bh.y); hi.z = fmaxf(hi.z, bh.z);
+// Cell p from its completed children.  Centres of mass use explicitly
+// rounded products and sums in slot order, so the result is bit-identical to
+// the level-wise sums of the reference.  With `local` the first pass over the
+// children also brings their quadrupoles into L1 for the second.
+__device__ __forceinline__ void cell_moments(const TreeDev& T, int p, const Kids& K, int want_quad, int want_box,
+                                             double edge0, double inv_theta, bool local) {
+    double m = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+    float4 lo = make_float4(INFINITY, INFINITY, INFINITY, 0.f);
+    float4 hi = make_float4(-INFINITY, -INFINITY, -INFINITY, 0.f);
+    auto add_com = [&](int c) {
+        const double4 cc = ld_up_d4(&T.com[c], local);
+        if (local && want_quad) prefetch_l1(T.wrec + 4 * (size_t)c + 2);
+        mx = __dadd_rn(mx, __dmul_rn(cc.x, cc.w));
+        my = __dadd_rn(my, __dmul_rn(cc.y, cc.w));
+        mz = __dadd_rn(mz, __dmul_rn(cc.z, cc.w));
+        m = __dadd_rn(m, cc.w);
+        if (want_box) {
+            const float4 bl = ld_up(&T.bmin[c], local), bh = ld_up(&T.bmax[c], local);
+            lo.x = fminf(lo.x, bl.x); lo.y = fminf(lo.y, bl.y); lo.z = fminf(lo.z, bl.z);
+            hi.x = fmaxf(hi.x, bh.x); hi.y = fmaxf(hi.y, bh.y); hi.z = fmaxf(hi.z, bh.z);
+        }
+    };
+    const int2 lkp = __ldg(&T.link[p]);
+    const int end = lkp.x;
+    if (K.mask & 0x100) {
+        for (int c = p + 1; c < end; c = __ldg(&T.link[c].x)) add_com(c);
+    } else {
+#pragma unroll
+        for (int d = 0; d < 8; ++d)
+            if ((K.mask >> d) & 1) add_com(K.id[d]);
+    }
+    if (m > 0.0) {
+        mx = __ddiv_rn(mx, m);
+        my = __ddiv_rn(my, m);
+        mz = __ddiv_rn(mz, m);
+    }
+    T.com[p] = make_double4(mx, my, mz, m);
+    if (want_box) {
+        T.bmin[p] = lo;
+        T.bmax[p] = hi;
+    }
+    if (want_quad) {
+        double q[6] = {0, 0, 0, 0, 0, 0};
+        auto add_quad = [&](int c) {
+            const double4 cc = ld_up_d4(&T.com[c], local);
+            const double s0 = cc.x - mx, s1 = cc.y - my, s2 = cc.z - mz;
+            const double ss = s0 * s0 + s1 * s1 + s2 * s2;
+            const double w = cc.w;
+            q[0] += w * (3.0 * s0 * s0 - ss);
+            q[1] += w * 3.0 * s0 * s1;
+            q[2] += w * 3.0 * s0 * s2;
+            q[3] += w * (3.0 * s1 * s1 - ss);
+            q[4] += w * 3.0 * s1 * s2;
+            q[5] += w * (3.0 * s2 * s2 - ss);
+            // the child's quadrupole from its walk record (one 32-byte sector)
+            const float4 a0 = ld_up(T.wrec + 4 * (size_t)c + 2, local);
+            const float4 a1 = ld_up(T.wrec + 4 * (size_t)c + 3, local);
+            if (!(__float_as_int(a1.z) & ND_LEAF)) {
+                q[0] += a0.x; q[1] += a0.y; q[2] += a0.z; q[3] += a0.w; q[4] += a1.x; q[5] += a1.y;
             }
         };
-        const int2 lkp = __ldg(&T.link[p]);
-        const int end = lkp.x;
         if (K.mask & 0x100) {
-            for (int c = p + 1; c < end; c = __ldg(&T.link[c].x)) add_com(c);
+            for (int c = p + 1; c < end; c = __ldg(&T.link[c].x)) add_quad(c);
         } else {
 #pragma unroll
             for (int d = 0; d < 8; ++d)
-                if ((K.mask >> d) & 1) add_com(K.id[d]);
+                if ((K.mask >> d) & 1) add_quad(K.id[d]);
         }
-        if (m > 0.0) {
-            mx = __ddiv_rn(mx, m);
-            my = __ddiv_rn(my, m);
-            mz = __ddiv_rn(mz, m);
+        const float4 q0 = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+        const float2 q1 = make_float2((float)q[4], (float)q[5]);
+        put_wrec(T, p, mx, my, mz, m, lkp.y, K.mask, q0, q1, edge0, inv_theta);
+    }
+}
+
+// The upward pass in one launch.  Block b owns the sorted particles
+// [a0, a1) = [b C, (b + 1) C): it completes their leaves, then, deepest level
+// first with a block barrier between levels, every cell that starts and ends
+// inside the range (cells starting at position a are levels dl[a-1]+1 ..
+// dl[a]); their children are its own leaves and cells, so no other block is
+// involved and their loads go through L1, which holds the block's own
+// stores.  Whether a cell ends inside the range, and whether a parent crosses
+// a range boundary, follows from the block's prefix and suffix minima of dl
+// in shared memory, without a load.  Each warp queues its cells of the level
+// in shared memory and spreads them over its lanes, so a level costs one
+// combine per lane, not one per owned position.  A cell that crosses a range
+// boundary collects its
+// children by a count instead: the block's completed nodes whose parent
+// crosses are queued and handed off after the last level (every thread
+// fences its own writes, then one barrier), and each hand-off adds one to the
+// parent's count; the thread that adds the last combines the parent and
+// hands it off in turn (fence, count, fence, combine).  The combining thread
+// clears the count for the next pass over the same tree.  Crossing cells are
+// the common ancestors of the two particles at a range boundary, at most 21
+// per boundary, so counted hand-offs are rare.
+// 256 threads x 8 positions; 4 resident blocks per SM (64 registers) measured
+// faster than 2 (86 registers); 16 positions per thread measured slower
+constexpr int kUpBlock = 256;
+constexpr int kUpPer = 8;  // positions per thread
+constexpr int kUpChunk = kUpPer * kUpBlock;
+constexpr int kUpHand = 1024;
+
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// children of cell p: digit slots, or for a shared-key bucket its particles (all leaves)
+__device__ __forceinline__ int cell_nkids(const TreeDev& T, int p) {
+    const int mask = __ldg(T.kmask + p);
+    return (mask & 0x100) ? __ldg(T.last + p) - __ldg(T.first + p) + 1 : __popc(mask & 0xff);
+}
+
+// one completed child of p counted (after the caller's release fence)
+template <typename Combine>
+__device__ __forceinline__ void hand_off(const TreeDev& T, int p, Combine&& combine) {
+    while (p >= 0) {
+        const int need = cell_nkids(T, p);
+        if (atomicAdd(T.arrive + p, 1) != need - 1) return;
+        fence_acq_rel();
+        T.arrive[p] = 0;
+        combine(p, false);
+        fence_acq_rel();
+        p = __ldg(T.parent + p);
+    }
+}
+
+// Minimum over the block of per-thread aggregates, exclusive, from the left
+// (prefix) or from the right (suffix); identity 255.
+__device__ __forceinline__ void block_min_scans(int agg, int* wtot, int& pre, int& suf) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int p = agg, q = agg;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(MHPC_FULL, p, o);
+        const int w = __shfl_down_sync(MHPC_FULL, q, o);
+        if (lane >= o) p = min(p, v);
+        if (lane + o < 32) q = min(q, w);
+    }
+    // p, q: inclusive within the warp; totals per warp to shared memory
+    if (lane == 31) wtot[warp] = p;
+    __syncthreads();
+    int left = 255, right = 255;
+    for (int w = 0; w < kUpBlock / 32; ++w) {
+        if (w < warp) left = min(left, wtot[w]);
+        if (w > warp) right = min(right, wtot[w]);
+    }
+    const int pe = __shfl_up_sync(MHPC_FULL, p, 1), qe = __shfl_down_sync(MHPC_FULL, q, 1);
+    pre = min(left, lane > 0 ? pe : 255);
+    suf = min(right, lane < 31 ? qe : 255);
+}
+
+template <typename Leaf, typename Combine>
+__device__ __forceinline__ void upward_chunk(const TreeDev& T, Leaf&& leaf_fn, Combine&& combine) {
+    __shared__ int queue[kUpBlock / 32][32 * kUpPer];             // cell
+    __shared__ unsigned short qpos[kUpBlock / 32][32 * kUpPer];   // its first position - a0
+    __shared__ int hand[kUpHand];
+    // dls[i + 1] = dl[a0 + i], dls[0] = dl[a0 - 1]; pre[i] = min dl[a0 - 1 .. a - 1],
+    // suf[i] = min dl[a .. a1 - 1] for a = a0 + i: the run of common digits >= L
+    // through position a leaves the range to the left iff pre[i] >= L, to the
+    // right iff suf[i] >= L
+    __shared__ unsigned char dls[kUpChunk + 1], pre[kUpChunk], suf[kUpChunk];
+    __shared__ int wtot[kUpBlock / 32];
+    __shared__ int nhand, smax;
+    const int a0 = blockIdx.x * kUpChunk, a1 = min(a0 + kUpChunk, T.n), na = a1 - a0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) { nhand = 0; smax = 0; dls[0] = (unsigned char)dl_at(T.dl, a0 - 1); }
+    {
+        // thread t: positions kUpPer t .. kUpPer t + kUpPer - 1
+        int v[kUpPer], agg = 255, mx = 0;
+#pragma unroll
+        for (int k = 0; k < kUpPer; ++k) {
+            const int i = kUpPer * threadIdx.x + k;
+            v[k] = i < na ? (int)T.dl[a0 + i] : 255;
+            agg = min(agg, v[k]);
+            if (i < na) mx = max(mx, v[k]);
         }
-        T.com[p] = make_double4(mx, my, mz, m);
-        if (want_box) {
-            T.bmin[p] = lo;
-            T.bmax[p] = hi;
+        int el, er;
+        block_min_scans(agg, wtot, el, er);  // (contains a barrier: nhand, smax, dls[0] are set)
+        el = min(el, (int)dls[0]);
+        int run = el;
+#pragma unroll
+        for (int k = 0; k < kUpPer; ++k) {
+            const int i = kUpPer * threadIdx.x + k;
+            if (i < na) { pre[i] = (unsigned char)run; dls[i + 1] = (unsigned char)v[k]; }
+            run = min(run, v[k]);
         }
-        if (want_quad) {
-            double q[6] = {0, 0, 0, 0, 0, 0};
-            auto add_quad = [&](int c) {
-                const double4 cc = ldg_d4(&T.com[c]);
-                const double s0 = cc.x - mx, s1 = cc.y - my, s2 = cc.z - mz;
-                const double ss = s0 * s0 + s1 * s1 + s2 * s2;
-                const double w = cc.w;
-                q[0] += w * (3.0 * s0 * s0 - ss);
-                q[1] += w * 3.0 * s0 * s1;
-                q[2] += w * 3.0 * s0 * s2;
-                q[3] += w * (3.0 * s1 * s1 - ss);
-                q[4] += w * 3.0 * s1 * s2;
-                q[5] += w * (3.0 * s2 * s2 - ss);
-                if (!(__ldg(&T.link[c].y) & ND_LEAF)) {
-                    const float4 a0 = __ldg(&T.quad0[c]);
-                    const float2 a1 = __ldg(&T.quad1[c]);
-                    q[0] += a0.x; q[1] += a0.y; q[2] += a0.z; q[3] += a0.w; q[4] += a1.x; q[5] += a1.y;
-                }
-            };
-            if (K.mask & 0x100) {
-                for (int c = p + 1; c < end; c = __ldg(&T.link[c].x)) add_quad(c);
+        run = er;
+#pragma unroll
+        for (int k = kUpPer - 1; k >= 0; --k) {
+            const int i = kUpPer * threadIdx.x + k;
+            run = min(run, v[k]);
+            if (i < na) suf[i] = (unsigned char)run;
+        }
+        mx = __reduce_max_sync(MHPC_FULL, mx);
+        if (lane == 0) atomicMax(&smax, mx);
+    }
+    __syncthreads();
+    auto queue_parent = [&](int node) {
+        const int p = __ldg(T.parent + node);
+        const int i = atomicAdd(&nhand, 1);
+        if (i < kUpHand) {
+            hand[i] = p;
+        } else {  // queue full (not reached for kUpChunk particles): hand off at once
+            fence_acq_rel();
+            hand_off(T, p, combine);
+        }
+    };
+#pragma unroll 2
+    for (int j = 0; j < kUpPer; ++j) {
+        const int i = j * kUpBlock + threadIdx.x;
+        if (i >= na) break;
+        const int leaf = T.leaf_node[a0 + i];
+        leaf_fn(a0 + i, leaf);
+        // parent: the cell of level P = max(dl[a-1], dl[a]) (none for P = 0)
+        const int P = max((int)dls[i], (int)dls[i + 1]);
+        if (P > 0 && (pre[i] >= P || suf[i] >= P)) queue_parent(leaf);
+    }
+    int* q = queue[warp];
+    unsigned short* qi = qpos[warp];
+    for (int L = MHPC_MAX_LEVEL; L >= 1; --L) {
+        __syncthreads();
+        if (L > smax) continue;  // uniform
+        // this lane's local cells of level L (start in the range, end inside it), queued for the warp
+        unsigned sel = 0;
+#pragma unroll
+        for (int j = 0; j < kUpPer; ++j) {
+            const int i = j * kUpBlock + threadIdx.x;
+            if (i < na && dls[i] < L && L <= dls[i + 1] && suf[i] < L) sel |= 1u << j;
+        }
+        const int c = __popc(sel);
+        int incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(MHPC_FULL, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(MHPC_FULL, incl, 31);
+        int w = incl - c;
+        while (sel) {
+            const int j = __ffs(sel) - 1;
+            sel &= sel - 1;
+            const int i = j * kUpBlock + threadIdx.x;
+            q[w] = T.off[a0 + i] + (L - dls[i] - 1);
+            qi[w++] = (unsigned short)i;
+        }
+        __syncwarp();
+        for (int k = lane; k < total; k += 32) {
+            const int p = q[k];
+            combine(p, true);
+            // parent of level L - 1 crossing a range boundary: queued for the hand-off
+            const int i = qi[k];
+            if (L > 1 && (pre[i] >= L - 1 || suf[i] >= L - 1)) queue_parent(p);
+        }
+        __syncwarp();
+    }
+    // hand-offs: every thread releases its own writes, then the queued parents are counted
+    fence_acq_rel();
+    __syncthreads();
+    const int nh = min(nhand, kUpHand);
+    for (int k = threadIdx.x; k < nh; k += kUpBlock) hand_off(T, hand[k], combine);
+}
+
+__global__ void __launch_bounds__(kUpBlock, 4) k_upward(TreeDev T, const double* __restrict__ sx,
+                                                     const double* __restrict__ sy, const double* __restrict__ sz,
+                                                     const double* __restrict__ sm, int want_quad, int want_box,
+                                                     const long long* __restrict__ ord, double inv_theta,
+                                                     const DevStatus* st) {
+    if (st->code) return;
+    const double edge0 = want_quad ? ord_to_dbl(ord[1]) - ord_to_dbl(ord[0]) : 0.0;
+    upward_chunk(
+        T, [&](int a, int leaf) { leaf_moments(T, a, leaf, sx, sy, sz, sm, want_quad, want_box, edge0, inv_theta); },
+        [&](int p, bool local) {
+            cell_moments(T, p, cell_kids(T, p), want_quad, want_box, edge0, inv_theta, local);
+        });
+}
+
+
+// Bottom-up maximum of the smoothing lengths, in one launch like the moments.
+__global__ void __launch_bounds__(kUpBlock, 4) k_hmax(TreeDev T, const double* __restrict__ h, const DevStatus* st) {
+    if (st->code) return;
+    upward_chunk(
+        T, [&](int a, int leaf) { T.hmax[leaf] = __double2float_ru(h[a]); },
+        [&](int p, bool local) {
+            const int km = __ldg(T.kmask + p);
+            float m = 0.f;
+            if (km & 0x100) {
+                const int end = __ldg(&T.link[p].x);
+                for (int c = p + 1; c < end; c = __ldg(&T.link[c].x)) m = fmaxf(m, ld_up(&T.hmax[c], local));
             } else {
+                const Kids K = cell_kids(T, p);
 #pragma unroll
                 for (int d = 0; d < 8; ++d)
-                    if ((K.mask >> d) & 1) add_quad(K.id[d]);
+                    if ((K.mask >> d) & 1) m = fmaxf(m, ld_up(&T.hmax[K.id[d]], local));
             }
-            const float4 q0 = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
-            const float2 q1 = make_float2((float)q[4], (float)q[5]);
-            T.quad0[p] = q0;
-            T.quad1[p] = q1;
-            put_wrec(T, p, mx, my, mz, m, lkp.y, K.mask, q0, q1, edge0, inv_theta);
-        }
-    }
+            T.hmax[p] = m;
+        });
 }
 
-// Bottom-up maximum of the smoothing lengths, level by level like the
-// centres of mass.
-__global__ void __launch_bounds__(256) k_hmax_leaves(TreeDev T, const double* __restrict__ h, const DevStatus* st) {
-    if (st->code) return;
-    for (int a = blockIdx.x * blockDim.x + threadIdx.x; a < T.n; a += gridDim.x * blockDim.x)
-        T.hmax[T.leaf_node[a]] = __double2float_ru(h[a]);
-}
-
-__global__ void __launch_bounds__(256) k_hmax_level(TreeDev T, int L, const DevStatus* st) {
-    if (st->code) return;
-    const int i0 = T.level_off[L], i1 = min(T.level_off[L + 1], T.cap_nodes);
-    for (int i = i0 + blockIdx.x * blockDim.x + threadIdx.x; i < i1; i += gridDim.x * blockDim.x) {
-        const int p = T.level_cells[i];
-        const Kids K = cell_kids(T, p);
-        float m = 0.f;
-        if (K.mask & 0x100) {
-            const int end = __ldg(&T.link[p].x);
-            for (int c = p + 1; c < end; c = __ldg(&T.link[c].x)) m = fmaxf(m, __ldg(&T.hmax[c]));
-        } else {
-#pragma unroll
-            for (int d = 0; d < 8; ++d)
-                if ((K.mask >> d) & 1) m = fmaxf(m, __ldg(&T.hmax[K.id[d]]));
-        }
-        T.hmax[p] = m;
-    }
-}
 
 }  // namespace
 
@@ -397,11 +536,6 @@ int tree_build(TreeDev& T, const uint64_t* skey, void* scan_scratch, DevStatus* 
     k_copy_total<<<1, 1, 0, s>>>(T);
     k_zero_cells<<<148 * 8, 256, 0, s>>>(T);
     k_nodes<<<g, 256, 0, s>>>(T, skey, st);
-    CUDA_TRY(cudaMemsetAsync(T.level_off, 0, 64 * sizeof(int), s));
-    const int chunks = (n + kLevelChunk - 1) / kLevelChunk;
-    k_level_count<<<chunks, 256, 0, s>>>(T, st);
-    k_level_offsets<<<1, 1, 0, s>>>(T);
-    k_level_fill<<<chunks, 256, 0, s>>>(T, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }
@@ -409,19 +543,14 @@ int tree_build(TreeDev& T, const uint64_t* skey, void* scan_scratch, DevStatus* 
 int tree_upward(TreeDev& T, const double* sx, const double* sy, const double* sz, const double* sm,
                 int want_quad, int want_box, const long long* ord, double theta, DevStatus* st, cudaStream_t s) {
     const double inv_theta = want_quad ? 1.0 / theta : 0.0;
-    k_upward_leaves<<<grid_for(T.n, 256, 148 * 16), 256, 0, s>>>(T, sx, sy, sz, sm, want_quad, want_box, ord,
+    k_upward<<<(T.n + kUpChunk - 1) / kUpChunk, kUpBlock, 0, s>>>(T, sx, sy, sz, sm, want_quad, want_box, ord,
                                                                   inv_theta, st);
-    const int gl = grid_for(T.n / 2 + 1, 256, 148 * 16);
-    for (int L = MHPC_MAX_LEVEL; L >= 1; --L)
-        k_upward_level<<<gl, 256, 0, s>>>(T, L, want_quad, want_box, ord, inv_theta, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }
 
 int tree_node_hmax(const TreeDev& T, const double* h, const DevStatus* st, cudaStream_t s) {
-    k_hmax_leaves<<<grid_for(T.n, 256, 148 * 16), 256, 0, s>>>(T, h, st);
-    const int gl = grid_for(T.n / 2 + 1, 256, 148 * 16);
-    for (int L = MHPC_MAX_LEVEL; L >= 1; --L) k_hmax_level<<<gl, 256, 0, s>>>(T, L, st);
+    k_hmax<<<(T.n + kUpChunk - 1) / kUpChunk, kUpBlock, 0, s>>>(T, h, st);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

@@ -32,18 +32,15 @@ struct TreeDev {
     double4* com;       // [cap] centre of mass (x, y, z, m)
     float4* bmin;       // [cap] particle bounding box min (rounded down)
     float4* bmax;       // [cap] particle bounding box max (rounded up)
-    float4* quad0;      // [cap] traceless quadrupole Qxx Qxy Qxz Qyy (about com)
-    float2* quad1;      // [cap] Qyz Qzz
     // [4 * cap] mixed-path walk record, one 64-byte line per node:
     //   [0] float(x), float(y), float(z), m   (FP32 hi part of the centre of mass)
     //   [1] x - float(x), ..., opening criterion edge^2/theta (-1 for leaves)
-    //   [2] Qxx Qxy Qxz Qyy
+    //   [2] Qxx Qxy Qxz Qyy  (traceless quadrupole about the centre of mass; 0 for leaves)
     //   [3] Qyz Qzz, bits (link info & 0x1ff) | kmask << 9, M l^3 (cells; l = edge)
     float4* wrec;
     float* hmax;        // [cap] largest smoothing length below the node (rounded up)
-    int* level_cells;   // [cap] cell ids grouped by level (any order within a level)
-    int* level_off;     // [64] level_off[L] = start of level L's cells (L = 1..21, [22] = end);
-                        // [32 + L] = fill cursors while the lists are built
+    int* arrive;        // [cap] completed children counted for cells that cross a block's
+                        // range in the upward pass (0 between passes)
     int* nodes;         // [1] total nodes (= off[n]), device copy
 };
 
@@ -51,7 +48,7 @@ int tree_build(TreeDev& T, const uint64_t* skey, void* scan_scratch, DevStatus* 
 // Centres of mass (FP64), quadrupoles and walk records (want_quad, mixed
 // walk: every node's wrec, whose geometric criterion uses theta and the root
 // edge from the device bounding box `ord`) and particle bounding boxes
-// (want_box, used by the neighbour search) of every cell, level by level.
+// (want_box, used by the neighbour search) of every cell, in one launch.
 int tree_upward(TreeDev& T, const double* sx, const double* sy, const double* sz, const double* sm,
                 int want_quad, int want_box, const long long* ord, double theta, DevStatus* st, cudaStream_t s);
 // T.hmax[node] = max h over the node's particles (h sorted, n entries).
