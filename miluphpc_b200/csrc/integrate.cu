@@ -5,11 +5,19 @@
 
 namespace {
 
+// Every field's load is issued before the first store: the destination
+// arrays may alias the sources as far as the compiler knows, so a load after
+// a store would wait for the previous load's value (one round trip per field).
 __global__ void __launch_bounds__(256) k_gather(int n, const int* __restrict__ perm, GatherList L) {
     for (long s = blockIdx.x * (long)blockDim.x + threadIdx.x; s < n; s += (long)gridDim.x * blockDim.x) {
         const int o = __ldg(perm + s);
-#pragma unroll 4
-        for (int a = 0; a < L.count; ++a) L.dst[a][s] = __ldg(L.src[a] + o);
+        double v[MHPC_GATHER_MAX];
+#pragma unroll
+        for (int a = 0; a < MHPC_GATHER_MAX; ++a)
+            if (a < L.count) v[a] = __ldg(L.src[a] + o);
+#pragma unroll
+        for (int a = 0; a < MHPC_GATHER_MAX; ++a)
+            if (a < L.count) L.dst[a][s] = v[a];
         if (L.isrc) {
             int v = __ldg(L.isrc + o);
             if (L.imax > 0 && (v < 0 || v >= L.imax)) {
@@ -24,8 +32,13 @@ __global__ void __launch_bounds__(256) k_gather(int n, const int* __restrict__ p
 __global__ void __launch_bounds__(256) k_scatter(int n, const int* __restrict__ perm, GatherList L) {
     for (long s = blockIdx.x * (long)blockDim.x + threadIdx.x; s < n; s += (long)gridDim.x * blockDim.x) {
         const int o = __ldg(perm + s);
-#pragma unroll 4
-        for (int a = 0; a < L.count; ++a) L.dst[a][o] = L.src[a][s];
+        double v[MHPC_GATHER_MAX];
+#pragma unroll
+        for (int a = 0; a < MHPC_GATHER_MAX; ++a)
+            if (a < L.count) v[a] = L.src[a][s];
+#pragma unroll
+        for (int a = 0; a < MHPC_GATHER_MAX; ++a)
+            if (a < L.count) L.dst[a][o] = v[a];
     }
 }
 

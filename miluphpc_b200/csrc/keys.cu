@@ -91,10 +91,17 @@ __global__ void __launch_bounds__(256) k_keys(const double* __restrict__ x, cons
                                               const double* __restrict__ z, int n,
                                               const long long* __restrict__ ord, const double* __restrict__ bb,
                                               int curve, uint64_t* __restrict__ keys, int* __restrict__ iota) {
-    __shared__ unsigned char sdir[12][8], shil[12][8];
-    if (curve == 1 && threadIdx.x < 96) {
-        (&sdir[0][0])[threadIdx.x] = (&c_dir[0][0])[threadIdx.x];
-        (&shil[0][0])[threadIdx.x] = (&c_hil[0][0])[threadIdx.x];
+    // two levels per lookup: state s and the octants (c1, c2) of two
+    // consecutive levels -> (Hilbert digits h1 h2 as 6 bits) | (state after both) << 6,
+    // composed from the one-level tables, so the result is the same
+    __shared__ unsigned short s2[12 * 64];
+    if (curve == 1) {
+        for (int e = threadIdx.x; e < 12 * 64; e += blockDim.x) {
+            const int st = e >> 6, c1 = (e >> 3) & 7, c2 = e & 7;
+            const int h1 = c_hil[st][c1], st1 = c_dir[st][c1];
+            const int h2 = c_hil[st1][c2], st2 = c_dir[st1][c2];
+            s2[e] = (unsigned short)((h1 << 3) | h2 | (st2 << 6));
+        }
     }
     __syncthreads();
     const double lo = bb ? bb[0] : ord_to_dbl(ord[0]), hi = bb ? bb[1] : ord_to_dbl(ord[1]);
@@ -104,15 +111,17 @@ __global__ void __launch_bounds__(256) k_keys(const double* __restrict__ x, cons
         uint32_t bz = axis_bits(__ldg(z + i), lo, hi);
         uint64_t key = spread3(bx) | (spread3(by) << 1) | (spread3(bz) << 2);
         if (curve == 1) {
+            // levels 21..2 in pairs, then level 1
             uint64_t h = 0;
             int dir = 0;
 #pragma unroll
-            for (int lvl = 21; lvl > 0; --lvl) {
-                int cell = (int)((key >> (3 * (lvl - 1))) & 7ULL);
-                h = (h << 3) + shil[dir][cell];
-                dir = sdir[dir][cell];
+            for (int lvl = 21; lvl > 1; lvl -= 2) {
+                const int e = s2[(dir << 6) | (int)((key >> (3 * (lvl - 2))) & 63ULL)];
+                h = (h << 6) | (uint64_t)(e & 63);
+                dir = e >> 6;
             }
-            key = h;
+            const int e = s2[(dir << 6) | (int)((key & 7ULL) << 3)];  // (c1, c2 = 0): h1 in bits 3-5
+            key = (h << 3) | (uint64_t)((e >> 3) & 7);
         }
         keys[i] = key;
         if (iota) iota[i] = i;
