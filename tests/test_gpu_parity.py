@@ -668,6 +668,44 @@ def test_coincident_particles(cuda):
     sim.close()
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_upward_pass_long_shared_key_runs(precision, cuda):
+    """Three runs of 2600 identical positions: each shared-key bucket spans more
+    than one block's range of 2048 sorted particles, so the one-launch upward
+    pass completes it by counted hand-offs from several blocks, and a block
+    inside the run queues more hand-offs than its shared-memory queue holds.
+    Every cell's mass and centre of mass equal the sums over its particles
+    (contiguous in sorted order: the keys with the cell's prefix)."""
+    n = 24_000
+    P = ics.plummer(n, seed=31)
+    for a, b, src in [(2000, 4600, 100), (9000, 11600, 7000), (15000, 17600, 20000)]:
+        for k in ("x", "y", "z"):
+            P[k][a:b] = P[k][src]
+    sim = Miluphpc(gravity_cfg(sfc=0, precision=precision, theta_mixed=0.3), P)
+    sim.rhs(0)
+    assert sim.stats()["key_collisions"] >= 3 * 2599
+    keys, perm = sim.export_sorted()
+    tr = sim.export_tree()
+    gmap = _node_map(tr["child"], n)
+    ms = P["mass"][perm]
+    cm = np.concatenate([[0.0], np.cumsum(ms)])
+    cx = [np.concatenate([[0.0], np.cumsum(ms * P[k][perm])]) for k in ("x", "y", "z")]
+    big = 0
+    for (pre, lev), gid in gmap.items():
+        sh = np.uint64(3 * (21 - lev))
+        lo = np.searchsorted(keys, np.uint64(pre) << sh, side="left")
+        hi = np.searchsorted(keys, np.uint64(pre + 1) << sh, side="left") if pre + 1 < (1 << (3 * lev)) else n
+        m = cm[hi] - cm[lo]
+        big += hi - lo > 2048
+        np.testing.assert_allclose(tr["m"][gid], m, rtol=1e-10)  # (prefix-sum differences)
+        for c, k in zip(cx, ("x", "y", "z")):
+            np.testing.assert_allclose(tr[k][gid], (c[hi] - c[lo]) / m, rtol=1e-9, atol=1e-12)
+    assert big > 0
+    ax = sim.numpy("g_ax")
+    assert np.isfinite(ax).all() and np.isfinite(sim.numpy("g_az")).all()
+    sim.close()
+
+
 @pytest.mark.parametrize("criterion,d", [(0, 2.0), (1, 1.5)])
 def test_remove_particles(criterion, d, cuda):
     """Miluphpc::removeParticles: the survivors keep their order in every
