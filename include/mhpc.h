@@ -203,7 +203,7 @@ typedef struct mhpc_ctx mhpc_ctx;
  * (replaces the handlers' cudaMalloc, src/particle_handler.cpp:148+ and
  * src/subdomain_key_tree/tree_handler.cpp:6-36).  No call below allocates
  * device memory, with two stated exceptions: mhpc_integrate_host allocates its
- * device mirror of the state on its first call, and mhpc_fp32_peak allocates
+ * two device mirrors of the state on its first call, and mhpc_fp32_peak allocates
  * and frees a small buffer.  A gravity context also holds 4 * capacity
  * doubles for mhpc_potential. */
 int mhpc_ctx_create(mhpc_ctx** out, int capacity, const mhpc_config* cfg,
@@ -223,7 +223,10 @@ int mhpc_ctx_set_config(mhpc_ctx* ctx, const mhpc_config* cfg);
  * summed kernel milliseconds). */
 int mhpc_rhs(mhpc_ctx* ctx, const mhpc_particles* p, int step, int self_gravity, void* stream, float* ms_out);
 /* Same without the final synchronisation: the status is read by
- * mhpc_ctx_status().  Capturable into a CUDA graph. */
+ * mhpc_ctx_status().  Capturable into a CUDA graph.  A right-hand side that
+ * starts before the host has read the status of the previous one keeps that
+ * one's error code (its kernels then do nothing), so the first error of a
+ * queued sequence is the one reported. */
 int mhpc_rhs_async(mhpc_ctx* ctx, const mhpc_particles* p, int step, int self_gravity);
 int mhpc_ctx_status(mhpc_ctx* ctx);
 
@@ -234,17 +237,21 @@ int mhpc_ctx_status(mhpc_ctx* ctx);
  * step size used. */
 int mhpc_integrate(mhpc_ctx* ctx, const mhpc_particles* p, int step, double* dt_out);
 /* The same step with HOST (pinned or pageable) state arrays: copies the state
- * in, runs the step, copies the state and accelerations out.  Uses the
- * context's device mirror (allocated on first use).  Returns when the results
- * are in the host arrays (mhpc_integrate_host_async + mhpc_host_wait). */
+ * in, runs the step, copies the state and accelerations out.  Uses one of the
+ * context's two device mirrors (allocated on first use, each the state fields
+ * of `capacity` particles).  Returns when the results are in the host arrays
+ * (mhpc_integrate_host_async + mhpc_host_wait). */
 int mhpc_integrate_host(mhpc_ctx* ctx, mhpc_particles* host, int step, double* dt_out);
-/* The host-state step without waiting: every field is copied in as soon as the
- * previous step's compute has released the device mirror and the previous
- * step's copy-out of that field has landed (the host arrays are read and
- * written in place), and copied out after the compute, velocities first, so
- * that successive calls overlap one step's copy-out with the next step's
- * copy-in.  The host arrays must not be read or written until mhpc_host_wait
- * returns. */
+/* The host-state step without waiting (the leapfrog's step 0 and the
+ * predictor-corrector read a device value and wait for it): successive calls
+ * use the two device mirrors in turn; every field is copied in as soon as its
+ * mirror is free and the previous step's copy-out of that field has landed
+ * (the host arrays are read and written in place), and copied out after the
+ * compute, velocities first.  So one step's masses and (leapfrog) drifted
+ * positions go in while the previous step computes, and its other fields as
+ * soon as the previous step's copies of them are out.  The host arrays must
+ * not be read or written until mhpc_host_wait returns; an error of any queued
+ * step is reported there. */
 int mhpc_integrate_host_async(mhpc_ctx* ctx, mhpc_particles* host, int step, double* dt_out);
 /* Wait until every copy of the host-state steps issued so far has finished;
  * returns the device status. */

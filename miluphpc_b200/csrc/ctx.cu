@@ -77,6 +77,8 @@ struct mhpc_ctx {
     // holds a finished RHS whose counters are not yet in *run
     RunTotals* run = nullptr;
     bool st_pending = false;
+    // a right-hand side ran since the host last read *st
+    bool status_unread = false;
     long long learned_rhs = 0;  // right-hand sides that ran the learned feature pass
     // particle count of the last gravity walk, -1 before the first: the
     // relative opening rule reads that walk's accelerations from g_ax/g_ay/g_az
@@ -87,8 +89,9 @@ struct mhpc_ctx {
     double* dt_dev = nullptr;
     double* dt_part = nullptr;
     double time = 0.0;
-    // device mirror for mhpc_integrate_host
-    mhpc_particles mirror;
+    // device mirrors for mhpc_integrate_host, used by alternate steps so that
+    // one step's copy-in can run while the previous step computes
+    mhpc_particles mirror[2];
     bool mirror_ready = false;
     // mhpc_potential: the tree gets walk records whatever the precision; scratch
     // for the potential and the walk's accelerations (allocated on first use)
@@ -98,11 +101,13 @@ struct mhpc_ctx {
     // copy_stream while the right-hand side runs (pos_out = host x, y, z)
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_drift = nullptr;
-    // host-state steps: copy-in / copy-out streams and their events (one per field)
+    // host-state steps: copy-in / copy-out streams and their events (per
+    // mirror: compute done, and per field: copy-out done)
     cudaStream_t in_stream = nullptr, out_stream = nullptr;
-    cudaEvent_t ev_in = nullptr, ev_computed = nullptr;
-    cudaEvent_t ev_out[18] = {};
-    bool out_pending[18] = {};
+    cudaEvent_t ev_in = nullptr, ev_computed[2] = {};
+    cudaEvent_t ev_out[2][18] = {};
+    bool out_pending[2][18] = {};
+    bool computed_pending[2] = {};
     long long host_steps = 0;
     double* pos_out[3] = {nullptr, nullptr, nullptr};
     std::vector<void*> allocs;
@@ -440,9 +445,13 @@ int stage_sph(mhpc_ctx* c, const mhpc_particles* p) {
 
 // Zero the status word on the stream; with SPH the counters of a finished
 // right-hand side are first added to the run totals (one small kernel).
+// Start of a right-hand side.  A status the host has not read since the
+// previous right-hand side (queued host-state steps, the predictor-corrector's
+// second RHS) keeps its error code, so no error is lost between reads.
 int reset_status(mhpc_ctx* c, cudaStream_t s) {
-    if (c->cfg.sph) {
-        TRY(launch_status_fold(c->st, c->run, c->st_pending ? 1 : 0, c->band_ran ? 1 : 0, s));
+    const int keep = c->status_unread ? 1 : 0;
+    if (c->cfg.sph || keep) {
+        TRY(launch_status_fold(c->st, c->run, c->st_pending ? 1 : 0, c->band_ran ? 1 : 0, keep, s));
     } else {
         CUDA_TRY(cudaMemsetAsync(c->st, 0, sizeof(DevStatus), s));
     }
@@ -463,12 +472,14 @@ int rhs_async(mhpc_ctx* c, const mhpc_particles* p, int self_gravity) {
     record(c, EV_END);
     c->first_rhs_done = true;
     c->st_pending = c->cfg.sph != 0;
+    c->status_unread = true;
     return MHPC_OK;
 }
 
 int read_status(mhpc_ctx* c) {
     CUDA_TRY(cudaMemcpyAsync(c->h_st, c->st, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->status_unread = false;
     return c->h_st->code;
 }
 
@@ -657,18 +668,19 @@ int mhpc_ctx_destroy(mhpc_ctx* c) {
             cudaStreamSynchronize(q);
             cudaStreamDestroy(q);
         }
-    for (cudaEvent_t e : {c->ev_in, c->ev_computed})
+    for (cudaEvent_t e : {c->ev_in, c->ev_computed[0], c->ev_computed[1]})
         if (e) cudaEventDestroy(e);
-    for (cudaEvent_t e : c->ev_out)
-        if (e) cudaEventDestroy(e);
+    for (auto& row : c->ev_out)
+        for (cudaEvent_t e : row)
+            if (e) cudaEventDestroy(e);
     if (c->mirror_ready) {
-        double** ptrs[] = {&c->mirror.x, &c->mirror.y, &c->mirror.z, &c->mirror.mass, &c->mirror.vx, &c->mirror.vy,
-                           &c->mirror.vz, &c->mirror.ax, &c->mirror.ay, &c->mirror.az, &c->mirror.g_ax,
-                           &c->mirror.g_ay, &c->mirror.g_az, &c->mirror.g_ax_old, &c->mirror.g_ay_old,
-                           &c->mirror.g_az_old, &c->mirror.sml, &c->mirror.rho, &c->mirror.p, &c->mirror.cs,
-                           &c->mirror.e, &c->mirror.drhodt, &c->mirror.dedt, &c->mirror.dsmldt};
-        for (auto pp : ptrs)
-            if (*pp) cudaFree(*pp);
+        for (mhpc_particles& m : c->mirror) {
+            double** ptrs[] = {&m.x, &m.y, &m.z, &m.mass, &m.vx, &m.vy, &m.vz, &m.ax, &m.ay, &m.az, &m.g_ax,
+                               &m.g_ay, &m.g_az, &m.g_ax_old, &m.g_ay_old, &m.g_az_old, &m.sml, &m.rho, &m.p,
+                               &m.cs, &m.e, &m.drhodt, &m.dedt, &m.dsmldt};
+            for (auto pp : ptrs)
+                if (*pp) cudaFree(*pp);
+        }
     }
     delete c;
     return MHPC_OK;
@@ -857,7 +869,26 @@ int mhpc_stage_sph(mhpc_ctx* c, const mhpc_particles* p) {
     return stage_sph(c, p);
 }
 
+}  // extern "C"
+
+namespace {
+// One integrator step; with `sync` false (host-state steps) it returns after
+// queueing the work, without reading the status word, except where the host
+// needs a device value (the predictor-corrector's step size, the status after
+// the leapfrog's initial right-hand side).
+int integrate_step(mhpc_ctx* c, const mhpc_particles* p, int step, double* dt_out, bool sync);
+}  // namespace
+
+extern "C" {
+
 int mhpc_integrate(mhpc_ctx* c, const mhpc_particles* p, int step, double* dt_out) {
+    return integrate_step(c, p, step, dt_out, true);
+}
+
+}  // extern "C"
+
+namespace {
+int integrate_step(mhpc_ctx* c, const mhpc_particles* p, int step, double* dt_out, bool sync) {
     if (!c) return MHPC_ERR_ARG;
     TRY(check_particles(c, p));
     const double dt = c->cfg.time_step;
@@ -928,17 +959,23 @@ int mhpc_integrate(mhpc_ctx* c, const mhpc_particles* p, int step, double* dt_ou
     }
     c->time += dt;
     c->last_dt = dt;
-    return read_status(c);
+    return sync ? read_status(c) : MHPC_OK;
 }
+}  // namespace
 
-// Host-state steps.  Every field moves on its own schedule: the inputs go in
-// on `in_stream` once the previous step's compute has released the device
-// mirror and the previous step's copy-out of the same field has landed in
-// the host buffer (the host state is read and written in place); the outputs
-// go out on `out_stream` after the compute, velocities first.  So the next
-// step's copy-in of the fields that are ready (masses, positions) runs while
-// this step's velocities and accelerations are still coming out (the bus is
-// full duplex), and mhpc_integrate_host_async returns without waiting.
+extern "C" {
+
+// Host-state steps.  Successive steps use the two device mirrors in turn,
+// and every field moves on its own schedule: a field goes in on `in_stream`
+// once its mirror is free (the compute and the copy-out of the step before
+// the previous one are done) and the host buffer holds the previous step's
+// value (that step's copy-out of the field has landed; the host state is read
+// and written in place); the outputs go out on `out_stream` after the
+// compute, velocities first.  Steps are queued without waiting, so the next
+// step's masses and (leapfrog) drifted positions go in while this step still
+// computes, and its velocities and accelerations go in as soon as they are
+// out (the bus is full duplex); the compute of a step starts when its inputs
+// are in.
 enum HostField { HF_X, HF_Y, HF_Z, HF_M, HF_VX, HF_VY, HF_VZ, HF_GX, HF_GY, HF_GZ, HF_H, HF_E, HF_RHO, HF_P,
                  HF_CS, HF_AX, HF_AY, HF_AZ, HF_COUNT };
 
@@ -947,8 +984,10 @@ int host_streams(mhpc_ctx* c) {
     CUDA_TRY(cudaStreamCreateWithFlags(&c->in_stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaStreamCreateWithFlags(&c->out_stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
-    CUDA_TRY(cudaEventCreateWithFlags(&c->ev_computed, cudaEventDisableTiming));
-    for (int f = 0; f < HF_COUNT; ++f) CUDA_TRY(cudaEventCreateWithFlags(&c->ev_out[f], cudaEventDisableTiming));
+    for (int k = 0; k < 2; ++k) {
+        CUDA_TRY(cudaEventCreateWithFlags(&c->ev_computed[k], cudaEventDisableTiming));
+        for (int f = 0; f < HF_COUNT; ++f) CUDA_TRY(cudaEventCreateWithFlags(&c->ev_out[k][f], cudaEventDisableTiming));
+    }
     return MHPC_OK;
 }
 
@@ -956,19 +995,23 @@ int mhpc_integrate_host_async(mhpc_ctx* c, mhpc_particles* h, int step, double* 
     if (!c || !h) return MHPC_ERR_ARG;
     if (h->n > c->cap || h->n < 0) return MHPC_ERR_CAPACITY;
     const size_t n = c->cap;
-    mhpc_particles& m = c->mirror;
     if (!c->mirror_ready) {
-        std::memset(&m, 0, sizeof(m));
-        double** ptrs[] = {&m.x, &m.y, &m.z, &m.mass, &m.vx, &m.vy, &m.vz, &m.g_ax, &m.g_ay, &m.g_az,
-                           &m.g_ax_old, &m.g_ay_old, &m.g_az_old};
-        for (auto pp : ptrs) CUDA_TRY(cudaMalloc(pp, sizeof(double) * n));
-        if (c->cfg.sph) {
-            double** p2[] = {&m.ax, &m.ay, &m.az, &m.sml, &m.rho, &m.p, &m.cs, &m.e, &m.drhodt, &m.dedt, &m.dsmldt};
-            for (auto pp : p2) CUDA_TRY(cudaMalloc(pp, sizeof(double) * n));
+        for (mhpc_particles& m : c->mirror) {
+            std::memset(&m, 0, sizeof(m));
+            double** ptrs[] = {&m.x, &m.y, &m.z, &m.mass, &m.vx, &m.vy, &m.vz, &m.g_ax, &m.g_ay, &m.g_az,
+                               &m.g_ax_old, &m.g_ay_old, &m.g_az_old};
+            for (auto pp : ptrs) CUDA_TRY(cudaMalloc(pp, sizeof(double) * n));
+            if (c->cfg.sph) {
+                double** p2[] = {&m.ax, &m.ay, &m.az, &m.sml, &m.rho, &m.p, &m.cs, &m.e, &m.drhodt, &m.dedt,
+                                 &m.dsmldt};
+                for (auto pp : p2) CUDA_TRY(cudaMalloc(pp, sizeof(double) * n));
+            }
         }
         c->mirror_ready = true;
     }
     TRY(host_streams(c));
+    const int k = (int)(c->host_steps & 1), j = 1 - k;  // this step's mirror, the previous step's
+    mhpc_particles& m = c->mirror[k];
     m.n = h->n;
     m.num_nodes = h->n;
     cudaStream_t s = c->stream;
@@ -986,19 +1029,23 @@ int mhpc_integrate_host_async(mhpc_ctx* c, mhpc_particles* h, int step, double* 
         in.push_back({HF_H, m.sml, h->sml}); in.push_back({HF_E, m.e, h->e}); in.push_back({HF_RHO, m.rho, h->rho});
         in.push_back({HF_P, m.p, h->p}); in.push_back({HF_CS, m.cs, h->cs});
     }
-    if (c->host_steps > 0) CUDA_TRY(cudaStreamWaitEvent(c->in_stream, c->ev_computed, 0));
+    // mirror k is free once the compute of its last step is done
+    if (c->computed_pending[k]) CUDA_TRY(cudaStreamWaitEvent(c->in_stream, c->ev_computed[k], 0));
     for (auto& q : in) {
         if (!q.hh) continue;
-        if (c->out_pending[q.id]) CUDA_TRY(cudaStreamWaitEvent(c->in_stream, c->ev_out[q.id], 0));
+        // mirror k's copy-out of this field (two steps back) and the host
+        // buffer's latest write (the previous step's copy-out from mirror j)
+        if (c->out_pending[k][q.id]) CUDA_TRY(cudaStreamWaitEvent(c->in_stream, c->ev_out[k][q.id], 0));
+        if (c->out_pending[j][q.id]) CUDA_TRY(cudaStreamWaitEvent(c->in_stream, c->ev_out[j][q.id], 0));
         CUDA_TRY(cudaMemcpyAsync(q.d, q.hh, b, cudaMemcpyHostToDevice, c->in_stream));
     }
     CUDA_TRY(cudaEventRecord(c->ev_in, c->in_stream));
     CUDA_TRY(cudaStreamWaitEvent(s, c->ev_in, 0));
-    // the compute overwrites every output field of the mirror: the previous
-    // step's copy-out of each must have finished (for the fields that are
-    // also inputs this is already implied by their copy-in)
+    // the compute overwrites every output field of mirror k: its copy-out two
+    // steps back must have finished (for the fields that are also inputs this
+    // is already implied by their copy-in)
     for (int f = 0; f < HF_COUNT; ++f)
-        if (c->out_pending[f]) CUDA_TRY(cudaStreamWaitEvent(s, c->ev_out[f], 0));
+        if (c->out_pending[k][f]) CUDA_TRY(cudaStreamWaitEvent(s, c->ev_out[k][f], 0));
     // leapfrog: step 0 computes the initial accelerations; later steps carry
     // the caller's g_a of the previous step
     if (c->cfg.integrator == 2) c->first_rhs_done = step != 0;
@@ -1008,21 +1055,24 @@ int mhpc_integrate_host_async(mhpc_ctx* c, mhpc_particles* h, int step, double* 
             CUDA_TRY(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
             CUDA_TRY(cudaEventCreateWithFlags(&c->ev_drift, cudaEventDisableTiming));
         }
+        // the drifted positions are written to the host during this step's
+        // right-hand side, after this step's copy-in has read them
         c->pos_out[0] = h->x; c->pos_out[1] = h->y; c->pos_out[2] = h->z;
     }
-    int rc = mhpc_integrate(c, &m, step, dt_out);
+    int rc = integrate_step(c, &m, step, dt_out, false);
     c->pos_out[0] = c->pos_out[1] = c->pos_out[2] = nullptr;
     if (rc) return rc;
     if (overlap) {
         // the drifted positions went out on copy_stream during the RHS
         for (int f = HF_X; f <= HF_Z; ++f) {
-            CUDA_TRY(cudaEventRecord(c->ev_out[f], c->copy_stream));
-            c->out_pending[f] = true;
+            CUDA_TRY(cudaEventRecord(c->ev_out[k][f], c->copy_stream));
+            c->out_pending[k][f] = true;
         }
     }
-    CUDA_TRY(cudaEventRecord(c->ev_computed, s));
+    CUDA_TRY(cudaEventRecord(c->ev_computed[k], s));
+    c->computed_pending[k] = true;
     ++c->host_steps;
-    CUDA_TRY(cudaStreamWaitEvent(c->out_stream, c->ev_computed, 0));
+    CUDA_TRY(cudaStreamWaitEvent(c->out_stream, c->ev_computed[k], 0));
     std::vector<Field> outp = {{HF_VX, m.vx, h->vx}, {HF_VY, m.vy, h->vy}, {HF_VZ, m.vz, h->vz}};
     if (!overlap) {
         outp.push_back({HF_X, m.x, h->x}); outp.push_back({HF_Y, m.y, h->y}); outp.push_back({HF_Z, m.z, h->z});
@@ -1039,14 +1089,15 @@ int mhpc_integrate_host_async(mhpc_ctx* c, mhpc_particles* h, int step, double* 
     for (auto& q : outp) {
         if (!q.hh) continue;
         CUDA_TRY(cudaMemcpyAsync(q.hh, q.d, b, cudaMemcpyDeviceToHost, c->out_stream));
-        CUDA_TRY(cudaEventRecord(c->ev_out[q.id], c->out_stream));
-        c->out_pending[q.id] = true;
+        CUDA_TRY(cudaEventRecord(c->ev_out[k][q.id], c->out_stream));
+        c->out_pending[k][q.id] = true;
     }
     return MHPC_OK;
 }
 
 int mhpc_host_wait(mhpc_ctx* c) {
     if (!c) return MHPC_ERR_ARG;
+    if (c->in_stream) CUDA_TRY(cudaStreamSynchronize(c->in_stream));
     if (c->out_stream) CUDA_TRY(cudaStreamSynchronize(c->out_stream));
     if (c->copy_stream) CUDA_TRY(cudaStreamSynchronize(c->copy_stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));

@@ -418,7 +418,11 @@ extern "C" int mhpc_fp32_peak(double* tflops) {
     return cudaGetLastError() == cudaSuccess ? MHPC_OK : MHPC_ERR_CUDA;
 }
 
-__global__ void k_status_fold(DevStatus* st, RunTotals* run, int fold, int band) {
+__global__ void k_status_fold(DevStatus* st, RunTotals* run, int fold, int band, int keep) {
+    // keep: an error of a right-hand side the host has not read yet stays
+    // (code, detail, site), so that the kernels of the next one skip and the
+    // host sees the first error when it reads the status
+    const int code = st->code, detail = st->detail, site = st->timeout_site;
     if (fold && threadIdx.x == 0) {
         const unsigned long long oob = (unsigned long long)max(st->sml_out_of_band, 0);
         run->rhs += 1;
@@ -434,10 +438,16 @@ __global__ void k_status_fold(DevStatus* st, RunTotals* run, int fold, int band)
     __syncthreads();
     int* w = reinterpret_cast<int*>(st);
     for (int i = threadIdx.x; i < (int)(sizeof(DevStatus) / sizeof(int)); i += blockDim.x) w[i] = 0;
+    __syncthreads();
+    if (keep && code && threadIdx.x == 0) {
+        st->code = code;
+        st->detail = detail;
+        st->timeout_site = site;
+    }
 }
 
-int launch_status_fold(DevStatus* st, RunTotals* run, int fold, int band, cudaStream_t s) {
-    k_status_fold<<<1, 32, 0, s>>>(st, run, fold, band);
+int launch_status_fold(DevStatus* st, RunTotals* run, int fold, int band, int keep, cudaStream_t s) {
+    k_status_fold<<<1, 32, 0, s>>>(st, run, fold, band, keep);
     CUDA_TRY(cudaGetLastError());
     return MHPC_OK;
 }

@@ -35,8 +35,9 @@ int launch_compact_d(int n, const int* keep, const int* rank, const double* src,
 int launch_compact_i(int n, const int* keep, const int* rank, const int* src, int* dst, cudaStream_t s);
 int launch_diagnostics(const mhpc_particles& p, int sph, double* part, double* out, cudaStream_t s);
 // Start of a right-hand side: when `fold`, add the finished RHS's counters in
-// *st to the run totals (its band counter only when `band`); then zero *st.
-int launch_status_fold(DevStatus* st, RunTotals* run, int fold, int band, cudaStream_t s);
+// *st to the run totals (its band counter only when `band`); then zero *st,
+// keeping an error code (with its detail and site) when `keep`.
+int launch_status_fold(DevStatus* st, RunTotals* run, int fold, int band, int keep, cudaStream_t s);
 size_t diagnostics_scratch_doubles();
 // W = 1/2 sum m_i phi_i into out[0] (part: diagnostics scratch).
 int launch_potential_energy(int n, const double* m, const double* pot, double* part, double* out, cudaStream_t s);

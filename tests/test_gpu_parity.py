@@ -496,17 +496,18 @@ def test_potential_matches_direct_sum(precision, cuda):
     sim.close()
 
 
-@pytest.mark.parametrize("pinned,pipelined", [(False, False), (True, False), (True, True)])
-def test_integrate_host_matches_device(pinned, pipelined, cuda):
+@pytest.mark.parametrize("pinned,pipelined,n,steps", [(False, False, 20_000, 3), (True, False, 20_000, 3),
+                                                       (True, True, 20_000, 3), (True, True, 400_000, 6)])
+def test_integrate_host_matches_device(pinned, pipelined, n, steps, cuda):
     """mhpc_integrate_host (host arrays in and out, positions copied out while
     the right-hand side runs) gives the device path's state bit for bit; so do
-    successive mhpc_integrate_host_async calls (each step's copy-out overlapping
-    the next step's copy-in) with one mhpc_host_wait at the end."""
-    n = 20_000
+    successive mhpc_integrate_host_async calls (alternate device mirrors, each
+    step's copy-in overlapping the previous step's compute and copy-out) with
+    one mhpc_host_wait at the end."""
     P = ics.plummer(n, seed=9)
     cfg = gravity_cfg(sfc=1, precision=1, theta_mixed=0.3, gravity_mac=1, mac_alpha=2e-3, time_step=0.01)
     dev = Miluphpc(cfg, P)
-    for k in range(3):
+    for k in range(steps):
         dev.integrate(k)
     hsim = Miluphpc(cfg, P)
     fields = ["x", "y", "z", "mass", "vx", "vy", "vz", "g_ax", "g_ay", "g_az"]
@@ -522,7 +523,7 @@ def test_integrate_host_matches_device(pinned, pipelined, cuda):
         setattr(hp, f, ctypes.cast(ctypes.c_void_p(host[f].data_ptr()), _lib.P_d))
     L = _lib.load()
     dt = ctypes.c_double()
-    for k in range(3):
+    for k in range(steps):
         if pipelined:
             _lib.check(L.mhpc_integrate_host_async(hsim.ctx, ctypes.byref(hp), k, ctypes.byref(dt)), "async")
         else:
@@ -570,6 +571,33 @@ def test_integrate_host_async_sph_matches_device(cuda):
     for f in ["x", "y", "z", "vx", "vy", "vz", "sml", "rho", "p", "cs", "ax", "ay", "az"]:
         assert np.array_equal(host[f].numpy(), dev.numpy(f)), f
     dev.close()
+    hsim.close()
+
+
+def test_integrate_host_async_keeps_first_error(cuda):
+    """Queued host-state steps do not read the status between steps: an error
+    of the first step (neighbour lists past max_num_interactions) stays in the
+    status word through the later steps' starts and mhpc_host_wait reports it."""
+    S = _sedov_state(16)
+    n = len(S["x"])
+    cfg = sph_cfg(max_num_interactions=8)
+    hsim = Miluphpc(cfg, S, materials=[material()])
+    fields = ["x", "y", "z", "mass", "vx", "vy", "vz", "sml", "e", "rho", "p", "cs", "ax", "ay", "az"]
+    host = {}
+    for f in fields:
+        t = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        t.copy_(torch.as_tensor(np.asarray(S[f], dtype=np.float64)) if f in S else torch.zeros(n, dtype=torch.float64))
+        host[f] = t
+    hp = _lib.Particles()
+    hp.n = n
+    hp.num_nodes = n
+    for f in fields:
+        setattr(hp, f, ctypes.cast(ctypes.c_void_p(host[f].data_ptr()), _lib.P_d))
+    L = _lib.load()
+    dt = ctypes.c_double()
+    for k in range(3):
+        _lib.check(L.mhpc_integrate_host_async(hsim.ctx, ctypes.byref(hp), k, ctypes.byref(dt)), "async")
+    assert L.mhpc_host_wait(hsim.ctx) == 6
     hsim.close()
 
 
