@@ -105,8 +105,8 @@ struct mhpc_ctx {
     // mirror: compute done, and per field: copy-out done)
     cudaStream_t in_stream = nullptr, out_stream = nullptr;
     cudaEvent_t ev_in = nullptr, ev_computed[2] = {};
-    cudaEvent_t ev_out[2][18] = {};
-    bool out_pending[2][18] = {};
+    cudaEvent_t ev_out[2][18 * 4] = {};  // [mirror][field * kHostChunks + chunk]
+    bool out_pending[2][18 * 4] = {};
     bool computed_pending[2] = {};
     long long host_steps = 0;
     double* pos_out[3] = {nullptr, nullptr, nullptr};
@@ -974,10 +974,15 @@ extern "C" {
 // compute, velocities first.  Steps are queued without waiting, so the next
 // step's masses and (leapfrog) drifted positions go in while this step still
 // computes, and its velocities and accelerations go in as soon as they are
-// out (the bus is full duplex); the compute of a step starts when its inputs
-// are in.
+// out (the bus is full duplex), piece by piece; the compute of a step starts
+// when its inputs are in.
 enum HostField { HF_X, HF_Y, HF_Z, HF_M, HF_VX, HF_VY, HF_VZ, HF_GX, HF_GY, HF_GZ, HF_H, HF_E, HF_RHO, HF_P,
                  HF_CS, HF_AX, HF_AY, HF_AZ, HF_COUNT };
+// Each field moves in this many pieces, each with its own copy-out event, so
+// that the next step's copy-in of a piece follows the copy-out of the same
+// piece rather than of the whole field.
+constexpr int kHostChunks = 4;
+static_assert(HF_COUNT * kHostChunks <= 18 * 4, "host-step event arrays too small");
 
 int host_streams(mhpc_ctx* c) {
     if (c->in_stream) return MHPC_OK;
@@ -986,7 +991,8 @@ int host_streams(mhpc_ctx* c) {
     CUDA_TRY(cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming));
     for (int k = 0; k < 2; ++k) {
         CUDA_TRY(cudaEventCreateWithFlags(&c->ev_computed[k], cudaEventDisableTiming));
-        for (int f = 0; f < HF_COUNT; ++f) CUDA_TRY(cudaEventCreateWithFlags(&c->ev_out[k][f], cudaEventDisableTiming));
+        for (int f = 0; f < HF_COUNT * kHostChunks; ++f)
+            CUDA_TRY(cudaEventCreateWithFlags(&c->ev_out[k][f], cudaEventDisableTiming));
     }
     return MHPC_OK;
 }
@@ -1015,7 +1021,7 @@ int mhpc_integrate_host_async(mhpc_ctx* c, mhpc_particles* h, int step, double* 
     m.n = h->n;
     m.num_nodes = h->n;
     cudaStream_t s = c->stream;
-    const size_t b = sizeof(double) * h->n;
+    auto piece = [&](int i) { return (size_t)h->n * i / kHostChunks; };  // first element of piece i
     struct Field { int id; double* d; double* hh; };
     // state in (positions, velocities, masses; leapfrog carries g_a between
     // steps), the fields whose host copy is ready earliest first
@@ -1033,18 +1039,24 @@ int mhpc_integrate_host_async(mhpc_ctx* c, mhpc_particles* h, int step, double* 
     if (c->computed_pending[k]) CUDA_TRY(cudaStreamWaitEvent(c->in_stream, c->ev_computed[k], 0));
     for (auto& q : in) {
         if (!q.hh) continue;
-        // mirror k's copy-out of this field (two steps back) and the host
-        // buffer's latest write (the previous step's copy-out from mirror j)
-        if (c->out_pending[k][q.id]) CUDA_TRY(cudaStreamWaitEvent(c->in_stream, c->ev_out[k][q.id], 0));
-        if (c->out_pending[j][q.id]) CUDA_TRY(cudaStreamWaitEvent(c->in_stream, c->ev_out[j][q.id], 0));
-        CUDA_TRY(cudaMemcpyAsync(q.d, q.hh, b, cudaMemcpyHostToDevice, c->in_stream));
+        for (int i = 0; i < kHostChunks; ++i) {
+            // mirror k's copy-out of this piece (two steps back) and the host
+            // buffer's latest write (the previous step's copy-out from mirror j)
+            const int e = q.id * kHostChunks + i;
+            if (c->out_pending[k][e]) CUDA_TRY(cudaStreamWaitEvent(c->in_stream, c->ev_out[k][e], 0));
+            if (c->out_pending[j][e]) CUDA_TRY(cudaStreamWaitEvent(c->in_stream, c->ev_out[j][e], 0));
+            const size_t a0 = piece(i), a1 = piece(i + 1);
+            if (a1 > a0)
+                CUDA_TRY(cudaMemcpyAsync(q.d + a0, q.hh + a0, sizeof(double) * (a1 - a0), cudaMemcpyHostToDevice,
+                                         c->in_stream));
+        }
     }
     CUDA_TRY(cudaEventRecord(c->ev_in, c->in_stream));
     CUDA_TRY(cudaStreamWaitEvent(s, c->ev_in, 0));
     // the compute overwrites every output field of mirror k: its copy-out two
     // steps back must have finished (for the fields that are also inputs this
     // is already implied by their copy-in)
-    for (int f = 0; f < HF_COUNT; ++f)
+    for (int f = 0; f < HF_COUNT * kHostChunks; ++f)
         if (c->out_pending[k][f]) CUDA_TRY(cudaStreamWaitEvent(s, c->ev_out[k][f], 0));
     // leapfrog: step 0 computes the initial accelerations; later steps carry
     // the caller's g_a of the previous step
@@ -1064,7 +1076,7 @@ int mhpc_integrate_host_async(mhpc_ctx* c, mhpc_particles* h, int step, double* 
     if (rc) return rc;
     if (overlap) {
         // the drifted positions went out on copy_stream during the RHS
-        for (int f = HF_X; f <= HF_Z; ++f) {
+        for (int f = HF_X * kHostChunks; f < (HF_Z + 1) * kHostChunks; ++f) {
             CUDA_TRY(cudaEventRecord(c->ev_out[k][f], c->copy_stream));
             c->out_pending[k][f] = true;
         }
@@ -1088,9 +1100,15 @@ int mhpc_integrate_host_async(mhpc_ctx* c, mhpc_particles* h, int step, double* 
     }
     for (auto& q : outp) {
         if (!q.hh) continue;
-        CUDA_TRY(cudaMemcpyAsync(q.hh, q.d, b, cudaMemcpyDeviceToHost, c->out_stream));
-        CUDA_TRY(cudaEventRecord(c->ev_out[k][q.id], c->out_stream));
-        c->out_pending[k][q.id] = true;
+        for (int i = 0; i < kHostChunks; ++i) {
+            const size_t a0 = piece(i), a1 = piece(i + 1);
+            if (a1 > a0)
+                CUDA_TRY(cudaMemcpyAsync(q.hh + a0, q.d + a0, sizeof(double) * (a1 - a0), cudaMemcpyDeviceToHost,
+                                         c->out_stream));
+            const int e = q.id * kHostChunks + i;
+            CUDA_TRY(cudaEventRecord(c->ev_out[k][e], c->out_stream));
+            c->out_pending[k][e] = true;
+        }
     }
     return MHPC_OK;
 }

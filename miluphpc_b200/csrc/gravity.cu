@@ -542,6 +542,9 @@ __device__ __forceinline__ void eval_leaves_sel(const ListSmem& S, int count, co
 }
 
 constexpr int kListBlock = 128;
+// relative rule: a sub-box's smallest previous |a| is taken as at least this
+// fraction of its largest (the oracle's statement uses the same floor)
+constexpr float kRelFloor = 0.1f;
 // Resident blocks per SM the list walk is compiled for: 5 (96 registers, no
 // spills in the force walk) measured 3 % faster at 16.7 M than the
 // unconstrained 116 registers (4 blocks); 6 blocks (80 registers) spill and
@@ -615,13 +618,16 @@ __global__ void __launch_bounds__(kListBlock, MHPC_LISTS_MIN_BLOCKS) k_grav_list
         rz[k] = (hp.z - chz) + (lp.z - clz);
         // sub-box of members [4 kPPL b, 4 kPPL (b + 1)): 4 kPPL-lane segments of member row k;
         // relative rule: alpha times the smallest previous |a| of the sub-box
-        // (read before this walk overwrites the accelerations)
-        float amin = 0.f;
+        // (read before this walk overwrites the accelerations), floored at
+        // kRelFloor times the largest: near a potential minimum |a| tends to
+        // zero, and without the floor such a group would open the whole tree
+        float amin = 0.f, amax = 0.f;
         const float qratio = kRel ? (float)(P.quad_alpha / P.rel_alpha) : 0.f;
         if (kRel) {
             const int o = __ldg(perm + sl[k]);
             const double gx = gax[o], gy = gay[o], gz = gaz[o];
             amin = (float)(P.rel_alpha * sqrt(gx * gx + gy * gy + gz * gz));
+            amax = amin;
         }
         float bx0 = rx[k], by0 = ry[k], bz0 = rz[k], bx1 = rx[k], by1 = ry[k], bz1 = rz[k];
 #pragma unroll
@@ -632,8 +638,10 @@ __global__ void __launch_bounds__(kListBlock, MHPC_LISTS_MIN_BLOCKS) k_grav_list
             bx1 = fmaxf(bx1, __shfl_xor_sync(MHPC_FULL, bx1, o));
             by1 = fmaxf(by1, __shfl_xor_sync(MHPC_FULL, by1, o));
             if (kRel) amin = fminf(amin, __shfl_xor_sync(MHPC_FULL, amin, o));
+            if (kRel) amax = fmaxf(amax, __shfl_xor_sync(MHPC_FULL, amax, o));
             bz1 = fmaxf(bz1, __shfl_xor_sync(MHPC_FULL, bz1, o));
         }
+        if (kRel) amin = fmaxf(amin, kRelFloor * amax);
         if ((lane & (4 * kPPL - 1)) == 0) {
             const int b = k * (8 / kPPL) + lane / (4 * kPPL);
             S.bx0[b] = bx0; S.by0[b] = by0; S.bz0[b] = bz0; S.bw0[b] = amin;

@@ -520,7 +520,12 @@ void orc_gravity_group_crit(const double* x, const double* y, const double* z, c
 //   M l^lpow <= alpha a_b dist(com, box_b)^(lpow + 2),
 // i.e. the first neglected multipole term stays below alpha times the
 // particle's own acceleration; the geometric condition with theta stays as a
-// safety bound.  amag is indexed like x (original order).
+// safety bound.  a_b is floored at kRelFloor times the largest previous |a| of
+// the sub-box: near a potential minimum |a| tends to zero and the unfloored
+// rule would open the whole tree for that group (the device kernel applies
+// the same floor).  amag is indexed like x (original order).
+static const double kRelFloor = 0.1;
+
 static void gravity_boxes_impl(const double* x, const double* y, const double* z, const double* mass,
                                const double* q, const int* child, const int* level, const int* sorted,
                                int n, int gsize, int nsub, double radius, double theta, double eps2,
@@ -535,17 +540,19 @@ static void gravity_boxes_impl(const double* x, const double* y, const double* z
         const int lanes = std::min(gsize, n - base);
         // sub-box b covers group members [b*w, (b+1)*w); members past n
         // repeat the last particle (as the device kernel loads them)
-        std::vector<double> lo(3 * nsub, 1e300), hi(3 * nsub, -1e300), amin(nsub, 1e300);
+        std::vector<double> lo(3 * nsub, 1e300), hi(3 * nsub, -1e300), amin(nsub, 1e300), amax(nsub, 0.0);
         for (int j = 0; j < gsize; ++j) {
             const int s = sorted[std::min(base + j, n - 1)];
             const int b = j / w;
-            if (amag) amin[b] = std::min(amin[b], amag[s]);
+            if (amag) { amin[b] = std::min(amin[b], amag[s]); amax[b] = std::max(amax[b], amag[s]); }
             const double p[3] = {x[s], y[s], z[s]};
             for (int d = 0; d < 3; ++d) {
                 lo[3 * b + d] = std::min(lo[3 * b + d], p[d]);
                 hi[3 * b + d] = std::max(hi[3 * b + d], p[d]);
             }
         }
+        if (amag)
+            for (int b = 0; b < nsub; ++b) amin[b] = std::max(amin[b], kRelFloor * amax[b]);
         std::vector<int> stack;
         for (int i = 0; i < 8; ++i) if (child[i] != -1) stack.push_back(child[i]);
         std::vector<int> acc_nodes;
