@@ -136,6 +136,32 @@ def test_walk_small_theta_is_direct_sum():
     np.testing.assert_allclose(bx, dx, rtol=1e-9, atol=1e-12)
 
 
+def test_relative_rule_floor_bounds_a_vanishing_acceleration():
+    """Relative opening rule: a particle whose previous |a| is zero (the
+    potential minimum) does not make its group open the whole tree; the
+    sub-box's smallest |a| is floored at a tenth of its largest, so the
+    group's interactions grow by a bounded factor and no other group changes."""
+    n = 65_536
+    P = ics.plummer(n, seed=2)
+    bb = O.bbox(P["x"], P["y"], P["z"])
+    radius = 0.5 * (bb[1] - bb[0])
+    _, perm = O.sort(O.keys(P["x"], P["y"], P["z"], bb, 1))
+    T = O.Tree(P["x"], P["y"], P["z"], P["mass"], bb)
+    q = O.quad(T)
+    ax, ay, az, _, _ = O.gravity_boxes(T, perm, radius, 0.28, 1e-4, q)
+    amag = np.sqrt(ax ** 2 + ay ** 2 + az ** 2)
+    _, _, _, c0, _ = O.gravity_boxes_rel(T, perm, radius, 1.0, 1e-4, q, amag, 1.8e-3)
+    s = int(perm[1000])  # sorted position 1000: group 15, sub-box 5
+    a2 = amag.copy()
+    a2[s] = 0.0
+    _, _, _, c1, _ = O.gravity_boxes_rel(T, perm, radius, 1.0, 1e-4, q, a2, 1.8e-3)
+    grp = perm[960:1024]
+    others = np.setdiff1d(np.arange(n), grp)
+    assert np.array_equal(c1[others], c0[others])
+    assert c1[s] >= c0[s] and c1[s] < 6 * c0[s], (c0[s], c1[s])
+    assert c1[s] < n // 4
+
+
 def test_frnn_equals_bruteforce():
     rng = np.random.default_rng(3)
     n = 1500
